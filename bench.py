@@ -1,0 +1,339 @@
+"""Benchmark: photons/s of the photon-propagation path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload bilayer_rgd_mie] [--photons P] [--precision fp32|fp64]
+
+One step = one transport pass over P photons of the workload (default: the
+two-layer RGD-over-Mie slab with FarFieldCBS 200x8, PlanarFluence 200x200x64 and
+FarFieldFluence 90x36 detectors, 1e8 photons per step).  `value` is photons/s of
+the whole job with tallies resident in HBM, timed with CUDA events on the
+launching stream; `e2e` is the same metric through the public API
+(run_simulation_parallel with host tally arrays, host<->device copies inside).
+Under torchrun each rank transports its own photon range (weak scaling) and rank
+0 prints one JSON line with the max-over-ranks time.  `--impl reference` times
+the reference's own CPU implementation (built from its sources into oracle/_ref)
+on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "luminis-mc_b200"))
+sys.path.insert(0, REPO)
+
+FLOP_PER_EVENT = 300        # FP32 flops per scattering event (add/mul = 1, FMA = 2)
+METRIC = "photons/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="bilayer_rgd_mie")
+    ap.add_argument("--photons", type=int, default=None)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="CPU work per reference sample (bounded)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_spec(name, photons):
+    from luminis_mc_b200 import workloads as W
+    spec = W.WORKLOADS[name]()
+    if photons is not None:
+        spec["n_photons"] = int(photons)
+    return spec
+
+
+def config_block(spec, args, n_gpus):
+    return {"workload": spec["name"], "photons_per_step_per_gpu": int(spec["n_photons"]),
+            "sensors": [s["kind"] for s in spec["sensors"]], "layers": len(spec["layers"]),
+            "max_events": spec.get("max_events", 1000), "precision": args.precision,
+            "l2": "flushed between steps (256 MiB write)", "parallelism": f"photon-range x{n_gpus}",
+            "seed": spec["seed"]}
+
+
+# ------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if sm:
+            out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(mx), samples=len(sm))
+        out["reasons"] = sorted(reasons)
+        os.unlink(self.path)
+        return out
+
+
+# ------------------------------------------------------------------ reference (CPU)
+def reference_module():
+    from oracle import pyoracle as O
+    lm = O.reference_module("perf")
+    lm.set_log_level(lm.LogLevel.off)
+    return lm
+
+
+def reference_sample(spec, seconds, threads):
+    """Time the reference's run_simulation_parallel on a bounded photon sample sized
+    for about `seconds` of work; returns (photons/s, photons, wall)."""
+    from luminis_mc_b200 import workloads as W
+    lm = reference_module()
+
+    def run(n, seed):
+        cfg, _, keep = W.build(lm, spec, n_photons=n, seed=seed, n_threads=threads)
+        cfg.pin_threads_to_cores = True
+        t0 = time.perf_counter()
+        lm.run_simulation_parallel(cfg)
+        return time.perf_counter() - t0
+
+    n = max(threads * 50, 2000)
+    dt = run(n, 1)
+    while dt < 1.0 and n < 10 ** 9:
+        n *= 4
+        dt = run(n, 2)
+    n = max(n, int(n * seconds / dt))
+    dt = run(n, 3)
+    return n / dt, n, dt
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    spec = workload_spec(args.workload, args.photons)
+    threads = os.cpu_count() or 1
+    from luminis_mc_b200 import workloads as W
+    lm = reference_module()
+    # size one step to a bounded sample (~cpu_seconds of work)
+    rate, n, _ = reference_sample(spec, args.cpu_seconds / 2, threads)
+    n_step = max(1000, int(rate * args.cpu_seconds / 2))
+    times = []
+    for i in range(args.warmup + args.steps):
+        cfg, _, keep = W.build(lm, spec, n_photons=n_step, seed=1000 + i, n_threads=threads)
+        cfg.pin_threads_to_cores = True
+        t0 = time.perf_counter()
+        lm.run_simulation_parallel(cfg)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = n_step * len(times) / total
+    line = {"metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded media of the workload)", "impl": "reference",
+            "config": config_block(spec, args, 1) | {"photons_per_step_per_gpu": n_step,
+                                                      "precision": "fp64"},
+            "cpu_baseline": {"value": value, "unit": "photons/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": f"{n_step} photons per step of {spec['name']}, "
+                                       f"run_simulation_parallel with n_threads={threads}"},
+            "e2e": {"value": value, "unit": "photons/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- ours
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import luminis_mc_b200 as lm
+    from luminis_mc_b200 import _native as N
+    from luminis_mc_b200 import workloads as W
+    from luminis_mc_b200.device import DeviceRun
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    spec = workload_spec(args.workload, args.photons)
+    P = int(spec["n_photons"])
+    cfg, handles, keep = W.build(lm, spec)
+    run = DeviceRun(cfg, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    seed = int(spec["seed"])
+    base = rank * P                       # this rank's photon range, per step
+
+    def step(k):
+        flush.zero_()
+        st, _ = run.run(P, seed, begin=(k * world * P) + base, precision=args.precision,
+                        stream=stream.cuda_stream)
+        return st
+
+    for k in range(args.warmup):
+        step(k)
+    barrier()
+    stats = []
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            stats.append(step(args.warmup + k))
+        barrier()
+    clocks = clk.summary()
+    kernel_ms = sum(s["kernel_ms"] for s in stats)
+    t = torch.tensor([kernel_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    photons_all = P * world * args.steps
+    value = photons_all / (total_ms * 1e-3)
+    events = sum(s["events"] for s in stats)
+    steps_ = sum(s["steps"] for s in stats)
+    photons_done = sum(s["photons"] for s in stats)
+    assert photons_done == P * args.steps, (photons_done, P * args.steps)
+
+    # roofline: the transport kernel is FP32/SFU issue-bound; measured FMA peak
+    peak_tflops, _ = N.probe_fp32_peak(200000)
+    achieved_tflops = events * FLOP_PER_EVENT / (kernel_ms * 1e-3) / 1e12
+    launches = 0
+    nb = max(1, math.ceil(P / (8 << 20)))
+    launches = args.steps * nb * 2        # one transport + one tally kernel per batch
+
+    # end-to-end through the public API: host tally arrays, copies inside
+    e2e = None
+    if not args.no_e2e:
+        e2e_ms = []
+        cfg2, h2, keep2 = W.build(lm, spec)
+        tally_bytes = run.transport.tally_size * 8
+        table_bytes = 0
+        for layer in cfg2.sample.layers:
+            m = layer.medium
+            table_bytes += m._s1.nbytes + m._s2.nbytes
+            v, c = m.phase_function._table()
+            if v is not None:
+                table_bytes += 2 * v.nbytes
+        for k in range(2):
+            barrier()
+            t0 = time.perf_counter()
+            cfg2.seed = seed + 77 + k
+            lm.run_simulation_parallel(cfg2, precision=args.precision)
+            torch.cuda.synchronize()
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        worst = torch.tensor([max(e2e_ms)], dtype=torch.float64, device=f"cuda:{local}")
+        if dist is not None:
+            dist.all_reduce(worst, op=dist.ReduceOp.MAX)
+        e2e = {"value": P * world / (float(worst.item()) * 1e-3), "unit": "photons/s",
+               "h2d_bytes_per_step": int(tally_bytes + table_bytes),
+               "d2h_bytes_per_step": int(tally_bytes + 256),
+               "path": "luminis_mc_b200.run_simulation_parallel(config) with numpy tallies"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            rate, n, dt = reference_sample(spec, args.cpu_seconds, threads)
+            cpu = {"value": rate, "unit": "photons/s", "cores": threads, "kind": "reference",
+                   "sample": f"{n} photons of {spec['name']} in {dt:.1f} s, reference "
+                             f"run_simulation_parallel (oracle/_ref/perf) with n_threads={threads}"}
+        except Exception as exc:          # the reference build is optional on a GPU box
+            cpu = {"value": None, "unit": "photons/s", "cores": os.cpu_count(),
+                   "kind": "reference", "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if args.precision == "fp32" else "f64",
+                "data": "synthetic (seeded media of the workload)",
+                "config": config_block(spec, args, world),
+                "events_per_s": events * world / (total_ms * 1e-3),
+                "steps_per_s": steps_ * world / (total_ms * 1e-3),
+                "events_per_photon": events / max(1, photons_done),
+                "roofline": {"bound": "fp32-issue", "achieved": achieved_tflops,
+                             "peak": peak_tflops, "unit": "TFLOP/s",
+                             "frac": achieved_tflops / peak_tflops,
+                             "peak_source": "measured: FFMA probe (lmc_probe_fp32_peak) on this GPU",
+                             "flop_per_event": FLOP_PER_EVENT, "traffic": None},
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    run.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,262 @@
+/*
+ * luminis_b200.h -- C ABI of the B200 photon-propagation library
+ * (luminis-mc_b200/luminis_mc_b200/lib/libluminis_b200.so).
+ *
+ * This is the drop-in boundary for luminis-mc's photon-propagation path.  It
+ * replaces the work behind the reference's Python entry point
+ *   luminis_mc.run_simulation_parallel(config)   (python/python_module.cpp:664-673)
+ * i.e. run_simulation_parallel(const SimConfig&)  (include/luminis/core/simulation.hpp:127,
+ *                                                  src/simulation.cpp:105-249)
+ * with one persistent CUDA kernel on an sm_100a GPU.  All signatures use plain C
+ * types, pointers and sizes; nothing here depends on PyTorch.
+ *
+ * Lifecycle: lmc_create (uploads the scene and its tables, allocates the
+ * handle's device scratch) -> lmc_run / lmc_run_host (any number of times) ->
+ * lmc_destroy.  A handle owns one CUDA stream; calls on one handle must not
+ * overlap (the same rule as the reference, which is not re-entrant on one
+ * SensorsGroup).  Different handles may be used from different threads.
+ *
+ * Errors: every call returns lmc_status; LMC_ERR_INVALID corresponds to the
+ * reference's std::invalid_argument (ValueError in Python), and the message is
+ * available from lmc_last_error (thread-local).
+ *
+ * Random stream contract (shared with the CPU replay oracle): Philox4x32-10,
+ * key = (seed lo, seed hi), counter = (block, 0, photon lo, photon hi).
+ * LMC_PRECISION_FP64 draws "u53" values (2 per block, u = (2*(w>>12)+1)*2^-53 for
+ * the 64-bit words x1:x0 and x3:x2); LMC_PRECISION_FP32 draws "u24" values
+ * (4 per block, u = (2*(x_i>>9)+1)*2^-24).  Draw j of photon i uses block j/2
+ * (u53) or j/4 (u24), in the reference's draw order (src/simulation.cpp:305-598,
+ * src/phase.cpp:27-49, src/laser.cpp:11-99).
+ */
+#ifndef LUMINIS_B200_H
+#define LUMINIS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LMC_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define LMC_API __attribute__((visibility("default")))
+#else
+#define LMC_API
+#endif
+#define LMC_MAX_LAYERS 16
+#define LMC_MAX_MEDIA 16
+#define LMC_MAX_SENSORS 8
+
+typedef enum lmc_status {
+  LMC_OK = 0,
+  LMC_ERR_INVALID = 1,      /* bad scene / options (reference: std::invalid_argument) */
+  LMC_ERR_CUDA = 2,         /* a CUDA runtime call failed                           */
+  LMC_ERR_NOMEM = 3,        /* device or host allocation failed                     */
+  LMC_ERR_KERNEL = 4,       /* the kernel raised its device error word              */
+  LMC_ERR_UNSUPPORTED = 5   /* valid for the reference but outside this library     */
+} lmc_status;
+
+/* How a medium's phase function turns a uniform u into theta
+ * (PhaseFunction::sample_theta, src/phase.cpp:78-304). */
+typedef enum lmc_theta_kind {
+  LMC_THETA_TABLE = 0,      /* inverse-CDF table over theta (RD, RD-EMC, Mie)        */
+  LMC_THETA_TABLE_COS = 1,  /* inverse-CDF table over cos(theta) (Rayleigh, Draine)  */
+  LMC_THETA_HG = 2,         /* Henyey-Greenstein closed form                         */
+  LMC_THETA_UNIFORM = 3     /* acos(2u - 1)                                          */
+} lmc_theta_kind;
+
+/* One scattering medium (ScatteringMedium + its PhaseFunction,
+ * include/luminis/core/medium.hpp:71-345).  Tables are host arrays copied by
+ * lmc_create; the caller may free them afterwards. */
+typedef struct lmc_medium_desc {
+  int theta_kind;               /* lmc_theta_kind                                      */
+  double hg_g;                  /* LMC_THETA_HG                                        */
+  int theta_n;                  /* SamplingTable nodes (nDiv + 1)                      */
+  const double *theta_values;   /* SamplingTable::values (src/table.cpp:27-31)         */
+  const double *theta_cdf;      /* SamplingTable::cdf    (src/table.cpp:38-47)         */
+  int amp_n;                    /* DataTable nodes, uniform in theta from 0            */
+  double amp_dtheta;            /* DataTable spacing (pi / (amp_n - 1))                */
+  const double *amp_s1;         /* S1(theta_i), interleaved re, im (amp_n complex)     */
+  const double *amp_s2;         /* S2(theta_i), interleaved re, im                     */
+  double mu_a, mu_s;            /* 1/mm; mu_t = mu_a + mu_s (src/medium.cpp:61-71)     */
+  double mean_free_path;        /* mm; free paths are -mfp*ln(u) (src/medium.cpp:123)  */
+} lmc_medium_desc;
+
+/* HomogeneousLayer z in [z_min, z_max) (include/luminis/core/sample.hpp:120-147). */
+typedef struct lmc_layer_desc {
+  double z_min, z_max;          /* z_max may be +inf for the last layer                */
+  int medium;
+} lmc_layer_desc;
+
+/* Laser (include/luminis/core/laser.hpp:24-96). */
+typedef struct lmc_laser_desc {
+  double position[3], direction[3], local_m[3], local_n[3];
+  double jones[4];              /* m.re, m.im, n.re, n.im                              */
+  double wavelength;            /* vacuum wavelength; photon k = 2 pi / wavelength     */
+  double sigma;
+  int source;                   /* 0 Point, 1 Uniform disk, 2 Gaussian                 */
+  int temporal;                 /* 0 Delta, 1 Gaussian, 2 TopHat, 3 Exponential,
+                                   4 PulseTrain, 5 CW                                  */
+  double pulse_duration, repetition_rate, time_offset;
+} lmc_laser_desc;
+
+typedef enum lmc_sensor_kind {
+  LMC_SENSOR_FARFIELD_CBS = 0,      /* FarFieldCBSSensor (src/detector.cpp:851-1310)  */
+  LMC_SENSOR_PLANAR_FLUENCE = 1,    /* PlanarFluenceSensor (src/detector.cpp:704-841) */
+  LMC_SENSOR_PLANAR_FIELD = 2,      /* PlanarFieldSensor (src/detector.cpp:490-568)   */
+  LMC_SENSOR_FARFIELD_FLUENCE = 3   /* far-field |E_f|^2 Stokes on (theta, phi); no
+                                       counterpart in the reference's sources         */
+} lmc_sensor_kind;
+
+/* One sensor (Sensor + subclass fields, include/luminis/core/detector.hpp:95-562).
+ * Filters follow Sensor::check_conditions (src/detector.cpp:374-417). */
+typedef struct lmc_sensor_desc {
+  int kind;
+  double z;
+  int absorb, estimator;
+  int f_theta; double theta_min, theta_max;
+  int f_phi; double phi_min, phi_max;
+  int f_pos; double x_min, x_max, y_min, y_max;
+  int f_dir; int direction;         /* 0 Forward, 1 Backward, 2 Both                  */
+  int f_events; int events_min, events_max;
+  double len_x, len_y, len_t, dx, dy, dt;              /* planar sensors            */
+  double theta_max_grid, phi_max_grid, dtheta, dphi;   /* far-field sensors         */
+} lmc_sensor_desc;
+
+/* The scene: Sample + Laser + SensorsGroup of a SimConfig
+ * (include/luminis/core/simulation.hpp:67-90). */
+typedef struct lmc_scene {
+  double n_host;                /* Sample(n_medium): light_speed = 1 / n_host          */
+  int n_media;
+  lmc_medium_desc media[LMC_MAX_MEDIA];
+  int n_layers;
+  lmc_layer_desc layers[LMC_MAX_LAYERS];
+  lmc_laser_desc laser;
+  int n_sensors;
+  lmc_sensor_desc sensors[LMC_MAX_SENSORS];
+} lmc_scene;
+
+typedef enum lmc_precision {
+  LMC_PRECISION_FP32 = 0,       /* fp32 transport, fp64 CBS phase, fp64 tallies        */
+  LMC_PRECISION_FP64 = 1        /* fp64 throughout (strict per-photon replay)          */
+} lmc_precision;
+
+typedef struct lmc_run_opts {
+  int precision;                /* lmc_precision                                       */
+  int max_events;               /* SimConfig::MAX_EVENTS                               */
+  int track_reverse_paths;      /* SimConfig::track_reverse_paths                      */
+  int block_size;               /* 0: default                                          */
+  int blocks_per_sm;            /* 0: as many as fit                                   */
+  void *records;                /* optional device array of n_photons lmc_record       */
+  void *stream;                 /* cudaStream_t to launch on; NULL: the handle's own   */
+  uint64_t batch_photons;       /* photons per transport batch (hit-queue mode); 0: 8M */
+} lmc_run_opts;
+
+/* Final state of one photon, written when opts.records is set (the same layout as
+ * the oracle's per-photon record). */
+typedef struct lmc_record {
+  uint64_t photon;
+  uint32_t events, draws;
+  int32_t fate, layer;          /* fate: 1 detected, 2 escaped, 3 left the stack at an
+                                   interface, 4 roulette, 5 event cap                  */
+  double weight, opticalpath, penetration_depth, launch_time;
+  double pos[3], dir[3], m[3], n[3];
+  double E[4];
+  double r1[3], rn[3];
+  double Er[4];
+  double hit[3];
+  int32_t n_hits, pad;
+} lmc_record;
+
+typedef struct lmc_stats {
+  uint64_t photons, events, steps, detected, escaped, stack, roulette, cap, draws;
+  uint64_t hits[LMC_MAX_SENSORS];   /* Sensor::hits increments                         */
+  uint32_t error_flags;             /* device error word (0 = none)                    */
+  float kernel_ms;                  /* transport kernel time, CUDA events              */
+} lmc_stats;
+
+typedef struct lmc_handle lmc_handle;
+
+/* Validate a scene, upload its tables and allocate the handle's device scratch.
+ * Replaces the set-up half of run_simulation_parallel (validate_sim_config,
+ * per-thread sensor clones; src/simulation.cpp:95-143). */
+LMC_API lmc_status lmc_create(const lmc_scene *scene, lmc_handle **out);
+
+/* Release everything lmc_create allocated. */
+LMC_API void lmc_destroy(lmc_handle *h);
+
+/* Tally layout of sensor `sensor` inside the handle's tally buffer (doubles).
+ * sensor = -1 returns the total size in *count.  dims as in the oracle:
+ *  FARFIELD_CBS [8][N_t][N_theta][N_phi], PLANAR_FLUENCE [4][N_t][N_x][N_y],
+ *  PLANAR_FIELD [2][N_x][N_y][2], FARFIELD_FLUENCE [4][N_t][N_theta][N_phi]. */
+LMC_API lmc_status lmc_tally_layout(const lmc_handle *h, int sensor, size_t *offset, size_t *count,
+                            int dims[4]);
+
+/* Transport photons [photon_begin, photon_begin + n_photons) under `seed` and ADD
+ * their contributions into the device tally buffer d_tallies (size from
+ * lmc_tally_layout(-1)).  Replaces the worker loop and merge of
+ * run_simulation_parallel (src/simulation.cpp:157-243) and run_photon
+ * (src/simulation.cpp:255-617).  Asynchronous on the handle's stream except for
+ * the statistics read-back when `stats` is non-NULL. */
+LMC_API lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
+                   const lmc_run_opts *opts, double *d_tallies, lmc_stats *stats);
+
+/* lmc_run with HOST tallies: copies h_tallies to the device, runs, and copies the
+ * sum back (the whole call is synchronous).  This is the path a reference-side
+ * binding uses when it owns plain host arrays. */
+LMC_API lmc_status lmc_run_host(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
+                        const lmc_run_opts *opts, double *h_tallies, lmc_stats *stats);
+
+/* Copy of the last error message on this thread; returns its length. */
+LMC_API size_t lmc_last_error(char *buf, size_t len);
+
+/* ---- set-up physics (host), the constructors' work -------------------------------- */
+
+/* Mie amplitudes S1, S2 (interleaved re/im) at the n cosines mu for size parameter x
+ * and relative index m; efficiencies and g.  Replaces miev/mievinfo
+ * (src/mie/dmiev.cpp:45-76, src/mie/MIEV0noP.f). */
+LMC_API lmc_status lmc_mie(double x, double m_re, double m_im, int n, const double *mu, double *s1,
+                   double *s2, double *qext, double *qsca, double *g);
+
+typedef enum lmc_pdf_kind {
+  LMC_PDF_RAYLEIGH = 1, LMC_PDF_RD = 3, LMC_PDF_RDEMC = 4, LMC_PDF_DRAINE = 5, LMC_PDF_MIE = 6
+} lmc_pdf_kind;
+
+/* Phase-function parameters for lmc_sampling_table / lmc_phase_cross_section. */
+typedef struct lmc_phase_params {
+  int kind;                     /* lmc_pdf_kind                                        */
+  double g, a;                  /* Draine                                              */
+  double wavelength, radius, n_particle, n_medium;
+} lmc_phase_params;
+
+/* SamplingTable of a tabulated phase function: values and cdf (n_div + 1 each).
+ * Replaces SamplingTable::initialize with the phase functions' PDFs
+ * (src/table.cpp:6-48, src/phase.cpp:87-304). */
+LMC_API lmc_status lmc_sampling_table(const lmc_phase_params *p, int n_div, double min_val,
+                              double max_val, double *values, double *cdf);
+
+/* Single-particle scattering cross-section sigma_s (RD-EMC, Mie;
+ * src/phase.cpp:168-200, :270-284). */
+LMC_API lmc_status lmc_phase_cross_section(const lmc_phase_params *p, double *sigma_s);
+
+typedef enum lmc_amp_kind { LMC_AMP_RGD = 0, LMC_AMP_MIE = 1 } lmc_amp_kind;
+
+/* Amplitude tables S1(theta_i), S2(theta_i), theta_i = i*pi/(n-1): RGDMedium uses
+ * n = 2000 (src/medium.cpp:77-120), MieMedium n = 1000 with x = 2 pi r / lambda
+ * (src/medium.cpp:160-236). */
+LMC_API lmc_status lmc_amplitude_table(int kind, double radius, double n_particle, double n_medium,
+                               double wavelength, int n, double *s1, double *s2);
+
+/* ---- measurement --------------------------------------------------------------------- */
+
+/* Measured FP32 FMA issue rate of the current GPU (TFLOP/s, 2 flops per FMA): the
+ * roofline denominator of the transport kernel, which is FP32/SFU-issue bound.
+ * No counterpart in the reference (it has no GPU code). */
+LMC_API lmc_status lmc_probe_fp32_peak(int iters, double *tflops, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,124 @@
+// lmc_device.cuh -- device-side data layout and math of the transport kernel.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "luminis_b200.h"
+
+namespace lmc {
+namespace dev {
+
+constexpr int kGuideBuckets = 4096;     // inverse-CDF guide table size (power of two)
+
+// One medium as the kernel sees it.  Tables live in the handle's device arena.
+struct Medium {
+  int theta_kind, theta_n, amp_n, pad;
+  double hg_g;
+  double amp_inv_dx;
+  double mu_t, mfp, albedo;             // albedo = mu_s / mu_t (1 if mu_t == 0: no split)
+  float hg_g_f, amp_inv_dx_f, mu_t_f, mfp_f, albedo_f, pad_f;
+  const double *th_val_d, *th_cdf_d;
+  const double2 *th_cs;                  // (cdf[i], slope into node i) for the fp32 path
+  const int *guide_d;                    // kGuideBuckets + 1 entries
+  const double4 *amp_d;                  // (s1.re, s1.im, s2.re, s2.im) per node
+  const float4 *amp_f;
+};
+
+struct Layer {
+  double z_min, z_max;
+  int medium, pad;
+};
+
+struct Sensor {
+  int kind, plane, absorb, estimator;
+  int f_theta, f_phi, f_pos, f_dir, f_events, direction, events_min, events_max;
+  double cos_min, cos_max, phi_min, phi_max, x_min, x_max, y_min, y_max;
+  double len_x, len_y, len_t, dx, dy, dt, dtheta, dphi;
+  int N_t, N_x, N_y, N_theta, N_phi, pad;
+  unsigned long long tally_off;          // offset in doubles into the tally buffer
+  unsigned long long plane_stride;       // doubles between Stokes planes
+};
+
+struct Laser {
+  double pos[3], dir[3], m[3], n[3];
+  double E[4];
+  double k;                              // 2 pi / vacuum wavelength
+  double sigma;
+  int source, temporal;
+  double pulse_duration, repetition_rate, time_offset;
+};
+
+// Everything the kernel needs except the per-run options; copied to shared
+// memory by every block at start-up.
+struct __align__(16) Scene {
+  int n_layers, n_interfaces, n_media, n_sensors, n_planes, top_is_inf;
+  int need_phase;                        // a PlanarField sensor needs exp(i k L)
+  int pad;
+  double top;                            // z_max of the last layer
+  double n_step;                         // 1 / light_speed = 1 / (1 / n_host)
+  double interfaces[LMC_MAX_LAYERS];
+  double plane_z[LMC_MAX_SENSORS];
+  float interfaces_f[LMC_MAX_LAYERS];
+  float plane_z_f[LMC_MAX_SENSORS];
+  float top_f, pad_f;
+  Layer layers[LMC_MAX_LAYERS];
+  Medium media[LMC_MAX_MEDIA];
+  Sensor sensors[LMC_MAX_SENSORS];
+  Laser laser;
+};
+
+// Device scratch of one run: photon work counter, statistics, error word.
+struct Scratch {
+  unsigned long long next_photon;        // reset per batch
+  unsigned long long queue_count;        // reset per batch
+  unsigned long long photons, events, steps, detected, escaped, stack, roulette, cap, draws;
+  unsigned long long hits[LMC_MAX_SENSORS];
+  unsigned int error_flags;
+  unsigned int pad;
+};
+
+// Hit queue: one entry per (photon, crossed sensor plane) whose sensors pass their
+// filters, written by the transport kernel and consumed by the tally kernel.
+// Struct-of-arrays, `cap` entries per field.
+enum QueueU32 { kQPhotonLo = 0, kQPhotonHi, kQEvents, kQMask, kQMedia, kQU32Fields };
+enum QueueF64 { kQWeight = 0, kQOpath, kQF64Fields };
+enum QueueR {
+  kQHit = 0,                  // 3: hit point
+  kQP = 3,                    // 9: P_local at the crossing (rows m, n, s)
+  kQE = 12,                   // 4: Jones vector (m.re, m.im, n.re, n.im)
+  kQR1 = 16,                  // 3: r_1           -- CBS fields from here on
+  kQRn = 19,                  // 3: r_n
+  kQP1 = 22,                  // 9: frame after the first scatter
+  kQPn1 = 31,                 // 9: frame before the newest scatter
+  kQT = 40,                   // 8: interior Jones product (re, im) x 4
+  kQRFields = 48,
+  kQRBasic = 16               // fields every entry carries
+};
+
+struct Queue {
+  unsigned long long cap;
+  uint32_t *u32;                         // [kQU32Fields][cap]
+  double *f64;                           // [kQF64Fields][cap]
+  void *r;                               // R[kQRFields][cap]
+};
+
+enum ErrorFlag : unsigned int {
+  kErrNonFiniteWeight = 1u << 0,   // a photon ended with a NaN/inf weight
+  kErrAborted = 1u << 1,           // a photon was dropped: non-finite state (see kError)
+  kErrQueueOverflow = 1u << 2,     // more hits than the queue holds (tallies incomplete)
+};
+
+struct RunParams {
+  unsigned long long photon_begin, n_photons;
+  uint32_t key0, key1;
+  int max_events, track_reverse;
+  double *tallies;
+  lmc_record *records;
+  Scratch *scratch;
+  Queue queue;                           // used by the queued kernel pair
+  unsigned int cbs_mask;                 // sensors whose hits need the CBS fields
+  unsigned int pad;
+};
+
+}  // namespace dev
+}  // namespace lmc

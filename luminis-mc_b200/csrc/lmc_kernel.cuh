@@ -1,0 +1,1269 @@
+// lmc_kernel.cuh -- device code of the photon-propagation kernel (sm_100a).
+//
+// One persistent kernel replaces run_simulation_parallel's worker pool and
+// run_photon (src/simulation.cpp:105-617).  Each thread owns one photon at a
+// time and advances it ONE scattering event per loop iteration; a thread whose
+// photon died takes the next photon index in the same iteration (warp-
+// aggregated atomic on a global counter), so the 32 lanes of a warp keep doing
+// events instead of idling until the warp's longest path ends.  Each photon
+// draws from its own Philox4x32-10 stream keyed by (seed, photon index) in the
+// reference's draw order, so results do not depend on the launch shape, as the
+// reference's do not depend on n_threads.
+//
+// State layout: what every event reads lives in registers (position, frame,
+// Jones vector, weight, the running interior Jones product, the previous frame
+// and position); what only a CBS detection reads -- the first-scatter frame and
+// position and the newest event's raw Jones factors -- lives in shared memory,
+// one slot per thread.  The emission time is recomputed from the counter-based
+// stream when a detector needs it instead of being carried.
+//
+// Precision: `R` is the transport type (float or double).  The weight, the
+// geometric path length, the CBS geometric phase k (s_out + s_in).(r_n - r_1)
+// and every tally are binary64 in both modes.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "lmc_device.cuh"
+#include "luminis_b200.h"
+
+namespace lmc {
+namespace dev {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kBlock = 256;                 // threads per block (upper bound)
+
+// ------------------------------------------------------------------ math by type
+__device__ __forceinline__ float m_log(float x) { return logf(x); }
+__device__ __forceinline__ double m_log(double x) { return log(x); }
+__device__ __forceinline__ float m_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float m_atan2(float y, float x) { return atan2f(y, x); }
+__device__ __forceinline__ double m_atan2(double y, double x) { return atan2(y, x); }
+__device__ __forceinline__ void m_sincos(float x, float *s, float *c) { sincosf(x, s, c); }
+__device__ __forceinline__ void m_sincos(double x, double *s, double *c) { sincos(x, s, c); }
+__device__ __forceinline__ void m_sincospi(float x, float *s, float *c) { sincospif(x, s, c); }
+__device__ __forceinline__ void m_sincospi(double x, double *s, double *c) { sincospi(x, s, c); }
+__device__ __forceinline__ float m_nudge(float z, float zi, bool up)
+{
+  // The reference nudges by 1e-12 (src/simulation.cpp:351-352); in binary32 that
+  // is below one ulp of z for z > ~1e-5, so step to the adjacent float instead.
+  return (z != zi) ? z : nextafterf(zi, up ? INFINITY : -INFINITY);
+}
+__device__ __forceinline__ double m_nudge(double z, double, bool) { return z; }
+
+// Smallest norm the reference still divides by (1e-300, src/detector.cpp:1152,
+// src/simulation.cpp:557); the binary32 path uses the nearest normal float.
+template <typename R> __device__ __forceinline__ R tiny();
+template <> __device__ __forceinline__ float tiny<float>() { return 1e-37f; }
+template <> __device__ __forceinline__ double tiny<double>() { return 1e-300; }
+
+template <typename R> struct Cx {
+  R re, im;
+};
+template <typename R> __device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b)
+{
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename R> __device__ __forceinline__ Cx<R> cadd(Cx<R> a, Cx<R> b) { return {a.re + b.re, a.im + b.im}; }
+template <typename R> __device__ __forceinline__ Cx<R> cscale(Cx<R> a, R s) { return {a.re * s, a.im * s}; }
+template <typename R> __device__ __forceinline__ R cnorm(Cx<R> a) { return a.re * a.re + a.im * a.im; }
+
+// scalar fields by transport type
+template <typename R> __device__ __forceinline__ R med_mfp(const Medium &m);
+template <> __device__ __forceinline__ float med_mfp<float>(const Medium &m) { return m.mfp_f; }
+template <> __device__ __forceinline__ double med_mfp<double>(const Medium &m) { return m.mfp; }
+template <typename R> __device__ __forceinline__ R med_mut(const Medium &m);
+template <> __device__ __forceinline__ float med_mut<float>(const Medium &m) { return m.mu_t_f; }
+template <> __device__ __forceinline__ double med_mut<double>(const Medium &m) { return m.mu_t; }
+template <typename R> __device__ __forceinline__ R sc_iface(const Scene &s, int i);
+template <> __device__ __forceinline__ float sc_iface<float>(const Scene &s, int i) { return s.interfaces_f[i]; }
+template <> __device__ __forceinline__ double sc_iface<double>(const Scene &s, int i) { return s.interfaces[i]; }
+template <typename R> __device__ __forceinline__ R sc_plane(const Scene &s, int i);
+template <> __device__ __forceinline__ float sc_plane<float>(const Scene &s, int i) { return s.plane_z_f[i]; }
+template <> __device__ __forceinline__ double sc_plane<double>(const Scene &s, int i) { return s.plane_z[i]; }
+template <typename R> __device__ __forceinline__ R sc_top(const Scene &s);
+template <> __device__ __forceinline__ float sc_top<float>(const Scene &s) { return s.top_f; }
+template <> __device__ __forceinline__ double sc_top<double>(const Scene &s) { return s.top; }
+
+// ------------------------------------------------------------------------ RNG
+// Philox4x32-10 (Salmon et al., SC'11); stream contract in luminis_b200.h.
+struct Rng {
+  uint32_t p_lo, p_hi, draw;
+  uint32_t b0, b1, b2, b3;
+};
+
+__device__ __forceinline__ void philox_block(Rng &g, uint32_t block, uint32_t key0, uint32_t key1)
+{
+  uint32_t c0 = block, c1 = 0u, c2 = g.p_lo, c3 = g.p_hi;
+  uint32_t k0 = key0, k1 = key1;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+    const uint32_t n0 = hi1 ^ c1 ^ k0;
+    const uint32_t n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  g.b0 = c0;
+  g.b1 = c1;
+  g.b2 = c2;
+  g.b3 = c3;
+}
+
+template <typename R> __device__ __forceinline__ R uniform(Rng &g, const RunParams &rp);
+
+template <> __device__ __forceinline__ float uniform<float>(Rng &g, const RunParams &rp)   // "u24"
+{
+  const uint32_t slot = g.draw & 3u;
+  if (slot == 0u)
+    philox_block(g, g.draw >> 2, rp.key0, rp.key1);
+  g.draw++;
+  const uint32_t w = slot == 0u ? g.b0 : slot == 1u ? g.b1 : slot == 2u ? g.b2 : g.b3;
+  return __uint2float_rn(2u * (w >> 9) + 1u) * 5.9604644775390625e-8f;   // 2^-24
+}
+
+template <> __device__ __forceinline__ double uniform<double>(Rng &g, const RunParams &rp)  // "u53"
+{
+  const uint32_t slot = g.draw & 1u;
+  if (slot == 0u)
+    philox_block(g, g.draw >> 1, rp.key0, rp.key1);
+  g.draw++;
+  const unsigned long long w = slot == 0u ? ((unsigned long long)g.b1 << 32) | g.b0
+                                          : ((unsigned long long)g.b3 << 32) | g.b2;
+  return __ull2double_rn(2ull * (w >> 12) + 1ull) * 1.1102230246251565e-16;   // 2^-53
+}
+
+// --------------------------------------------------------------------- photon
+template <typename R> struct Photon {
+  R px, py, pz;
+  R P[9];                      // rows m, n, s of P_local (photon.hpp:117)
+  Cx<R> Em, En;                // Jones vector in (m, n)
+  double w;                    // weight: binary64 (thousands of products per path)
+  double opath;                // geometric path length (time): binary64
+  R pen;                       // penetration depth (records only)
+  uint32_t events;
+  int layer, last_med;
+  R rn[3];                     // position of the newest scatter (r_n)
+  R Pn1[9];                    // frame before the newest scatter (P_{n-1})
+  Cx<R> T[4];                  // matrix_T_raw: normalised interior Jones product
+  Rng rng;
+  __device__ __forceinline__ unsigned long long index() const
+  {
+    return ((unsigned long long)rng.p_hi << 32) | rng.p_lo;
+  }
+};
+
+// Per-thread CBS state that only a detection reads, in shared memory.
+template <typename R> struct Side {
+  R first[12][kBlock];         // r_1 (3), then P1 rows m_1, n_1, s_1 (9)
+  R last[6][kBlock];           // S2, S1 (re, im) and cos, sin(phi) of the newest scatter
+  int first_med[kBlock];
+};
+
+struct Counters {
+  uint32_t events, steps, draws;
+};
+
+template <typename R> __device__ __forceinline__ int layer_index_at(const Scene &sc, R z)
+{                                                          // src/sample.cpp:221-235
+  if (z < R(0))
+    return sc.n_layers;
+  if (!sc.top_is_inf && z >= sc_top<R>(sc))
+    return sc.n_layers;
+  int idx = 0;
+  for (int i = 0; i < sc.n_interfaces; ++i)
+    idx += (sc_iface<R>(sc, i) <= z) ? 1 : 0;              // upper_bound on a sorted list
+  return idx < sc.n_layers ? idx : sc.n_layers;
+}
+
+template <typename R>
+__device__ __forceinline__ bool find_next_interface(const Scene &sc, R zc, R zt, R &out)
+{                                                          // src/sample.cpp:237-266
+  if (zt > zc) {
+    for (int i = 0; i < sc.n_interfaces; ++i) {
+      const R zi = sc_iface<R>(sc, i);
+      if (zi > zc) {
+        if (zi <= zt) {
+          out = zi;
+          return true;
+        }
+        return false;
+      }
+    }
+  } else if (zt < zc) {
+    for (int i = sc.n_interfaces - 1; i >= 0; --i) {
+      const R zi = sc_iface<R>(sc, i);
+      if (zi < zc) {
+        if (zi >= zt) {
+          out = zi;
+          return true;
+        }
+        return false;
+      }
+    }
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------- theta sampling
+// SamplingTable::Sample (src/table.cpp:50-66) with a guide table that narrows
+// std::lower_bound's range; the index found is the same.
+__device__ __forceinline__ double table_sample_f64(const Medium &m, double u)
+{
+  const int j = (int)(u * (double)kGuideBuckets);
+  int lo = __ldg(m.guide_d + j), hi = __ldg(m.guide_d + j + 1);
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(m.th_cdf_d + mid) < u)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo == 0)
+    return __ldg(m.th_val_d);
+  const double c0 = __ldg(m.th_cdf_d + lo - 1), c1 = __ldg(m.th_cdf_d + lo);
+  const double v0 = __ldg(m.th_val_d + lo - 1), v1 = __ldg(m.th_val_d + lo);
+  const double t = (u - c0) / (c1 - c0);
+  return v0 + t * (v1 - v0);
+}
+
+// The binary32 path searches the same binary64 CDF: near cdf = 1 a binary32 CDF
+// keeps only ~6e-8 of resolution, coarser than the increments of low-probability
+// (back-scatter) bins.  u24 values are exact in binary64, so the search finds the
+// reference's index; the lerp uses a precomputed slope per node.
+__device__ __forceinline__ double table_sample_f32(const Medium &m, float u)
+{
+  const double ud = u;
+  const int j = (int)(u * (float)kGuideBuckets);
+  int lo = __ldg(m.guide_d + j), hi = __ldg(m.guide_d + j + 1);
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(m.th_cdf_d + mid) < ud)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo == 0)
+    return __ldg(m.th_val_d);
+  const double c0 = __ldg(m.th_cdf_d + lo - 1);
+  const double slope = __ldg(&m.th_cs[lo].y);
+  return __ldg(m.th_val_d + lo - 1) + (ud - c0) * slope;
+}
+
+template <typename R> __device__ __forceinline__ R sample_theta(const Medium &m, R u);
+
+template <> __device__ __forceinline__ float sample_theta<float>(const Medium &m, float u)
+{
+  if (m.theta_kind == LMC_THETA_HG) {                      // src/phase.cpp:108-115
+    // Same inverse CDF written through 1 -/+ cos(theta) so that neither cancels:
+    // 1 - c = (1-g)(1-u)(1-g+frac)/d, 1 + c = (1+g)u(1+g+frac)/d, d = 1-g+2gu,
+    // theta = 2 atan2(sqrt(1-c), sqrt(1+c)); acos(c) loses all precision near c = 1.
+    const float g = m.hg_g_f;
+    const float d = 1.0f - g + 2.0f * g * u;
+    const float frac = (1.0f - g * g) / d;
+    const float omc = (1.0f - g) * (1.0f - u) * (1.0f - g + frac) / d;
+    const float opc = (1.0f + g) * u * (1.0f + g + frac) / d;
+    return 2.0f * atan2f(sqrtf(omc), sqrtf(opc));
+  }
+  if (m.theta_kind == LMC_THETA_UNIFORM)
+    return 2.0f * atan2f(sqrtf(1.0f - u), sqrtf(u));        // acos(2u - 1)
+  const double v = table_sample_f32(m, u);
+  return m.theta_kind == LMC_THETA_TABLE ? (float)v : (float)acos(v);
+}
+
+template <> __device__ __forceinline__ double sample_theta<double>(const Medium &m, double u)
+{
+  if (m.theta_kind == LMC_THETA_HG) {
+    const double g = m.hg_g, gg = g * g;
+    const double frac = (1.0 - gg) / (1.0 - g + 2.0 * g * u);
+    // clamped: rounding can leave cos theta an ulp outside [-1, 1] near u -> 0, 1
+    return acos(fmin(fmax((1.0 + gg - frac * frac) / (2.0 * g), -1.0), 1.0));
+  }
+  if (m.theta_kind == LMC_THETA_UNIFORM)
+    return acos(2.0 * u - 1.0);
+  const double v = table_sample_f64(m, u);
+  return m.theta_kind == LMC_THETA_TABLE ? v : acos(v);
+}
+
+// DataTable::Sample on the uniform theta grid (src/table.cpp:100-118): S2, S1.
+template <typename R> __device__ __forceinline__ void amplitudes(const Medium &m, R theta, Cx<R> &s2, Cx<R> &s1);
+
+template <> __device__ __forceinline__ void amplitudes<float>(const Medium &m, float theta, Cx<float> &s2, Cx<float> &s1)
+{
+  const float pos = theta * m.amp_inv_dx_f;
+  const int last = m.amp_n - 1;
+  float4 a;
+  if (pos <= 0.0f) {
+    a = __ldg(m.amp_f);
+  } else if (pos >= (float)last) {
+    a = __ldg(m.amp_f + last);
+  } else {
+    const int i = (int)pos;
+    const float t = pos - (float)i;
+    const float4 y0 = __ldg(m.amp_f + i), y1 = __ldg(m.amp_f + i + 1);
+    a = make_float4(y0.x + t * (y1.x - y0.x), y0.y + t * (y1.y - y0.y), y0.z + t * (y1.z - y0.z),
+                    y0.w + t * (y1.w - y0.w));
+  }
+  s1 = {a.x, a.y};
+  s2 = {a.z, a.w};
+}
+
+template <> __device__ __forceinline__ void amplitudes<double>(const Medium &m, double theta, Cx<double> &s2, Cx<double> &s1)
+{
+  const double pos = theta * m.amp_inv_dx;
+  const int last = m.amp_n - 1;
+  double4 a;
+  if (pos <= 0.0) {
+    a = m.amp_d[0];
+  } else if (pos >= (double)last) {
+    a = m.amp_d[last];
+  } else {
+    const int i = (int)pos;
+    const double t = pos - (double)i;
+    const double4 y0 = m.amp_d[i], y1 = m.amp_d[i + 1];
+    a = make_double4(y0.x + t * (y1.x - y0.x), y0.y + t * (y1.y - y0.y), y0.z + t * (y1.z - y0.z),
+                     y0.w + t * (y1.w - y0.w));
+  }
+  s1 = {a.x, a.y};
+  s2 = {a.z, a.w};
+}
+
+// ------------------------------------------------------------------ geometry
+template <typename R> struct V3 {
+  R x, y, z;
+};
+template <typename R> __device__ __forceinline__ V3<R> v3(R x, R y, R z) { return {x, y, z}; }
+template <typename R> __device__ __forceinline__ R vdot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <typename R> __device__ __forceinline__ V3<R> vscale(V3<R> a, R s) { return {a.x * s, a.y * s, a.z * s}; }
+template <typename R> __device__ __forceinline__ V3<R> vcross_unit(V3<R> a, V3<R> b)
+{                                                          // src/vec.cpp:14-26 (normalises)
+  V3<R> r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+  const R nf = m_sqrt(vdot(r, r));
+  if (nf > R(0))
+    r = vscale(r, R(1) / nf);
+  return r;
+}
+template <typename R> __device__ __forceinline__ V3<R> safe_unit(V3<R> v, V3<R> fb)
+{                                                          // src/utils.cpp:39-50
+  const R eps = R(1e-20);
+  const R n2 = vdot(v, v);
+  if (n2 < eps) {
+    const R f2 = vdot(fb, fb);
+    if (f2 < eps)
+      return v3<R>(R(1), R(0), R(0));
+    return vscale(fb, R(1) / m_sqrt(f2));
+  }
+  return vscale(v, R(1) / m_sqrt(n2));
+}
+template <typename R> __device__ __forceinline__ V3<R> row(const R *P, int r) { return {P[3 * r], P[3 * r + 1], P[3 * r + 2]}; }
+
+// Angle between unit vectors.  binary64 follows the reference,
+// acos(clamp_pm1(a.b)) (src/detector.cpp:1098,1137); binary32 uses
+// atan2(|a x b|, a.b), because acos of a dot product near +-1 is ill-conditioned.
+__device__ __forceinline__ double unit_angle(V3<double> a, V3<double> b)
+{
+  double c = vdot(a, b);
+  c = c > 1.0 ? 1.0 : (c < -1.0 ? -1.0 : c);
+  return acos(c);
+}
+__device__ __forceinline__ float unit_angle(V3<float> a, V3<float> b)
+{
+  const float x = a.y * b.z - a.z * b.y, y = a.z * b.x - a.x * b.z, z = a.x * b.y - a.y * b.x;
+  return atan2f(sqrtf(x * x + y * y + z * z), vdot(a, b));
+}
+// Exit polar angle theta = acos(-s_z) (src/detector.cpp:1273); binary32 uses
+// atan2(sqrt(s_x^2 + s_y^2), -s_z), which resolves the small angles of the CBS cone.
+__device__ __forceinline__ double exit_theta(double, double, double sz) { return acos(-sz); }
+__device__ __forceinline__ float exit_theta(float sx, float sy, float sz)
+{
+  return atan2f(sqrtf(sx * sx + sy * sy), -sz);
+}
+
+// ---------------------------------------------------------------- source
+// Laser::emit_photon's random part (src/laser.cpp:11-28, :42-75, :77-99): launch
+// x, y and emission time, drawn from the photon's stream starting at draw 0.
+template <typename R>
+__device__ void source_sample(const Laser &L, Rng &g, const RunParams &rp, double &x, double &y,
+                              double &t)
+{
+  x = L.pos[0];
+  y = L.pos[1];
+  if (L.source == 1) {
+    const double th = (double)uniform<R>(g, rp) * 2.0 * 3.141592653589793;
+    const double r = sqrt((double)uniform<R>(g, rp)) * L.sigma;
+    x = x + r * cos(th);
+    y = y + r * sin(th);
+  } else if (L.source == 2) {
+    for (int axis = 0; axis < 2; ++axis) {                 // Rng::normal, src/rng.cpp:18-27
+      const double u1 = (double)uniform<R>(g, rp);         // never 0 in this stream
+      const double u2 = (double)uniform<R>(g, rp);
+      const double z0 = sqrt(-2.0 * log(u1)) * cos(2.0 * 3.141592653589793 * u2);
+      if (axis == 0)
+        x = z0 * L.sigma + x;
+      else
+        y = z0 * L.sigma + y;
+    }
+  }
+  const double t0 = L.time_offset * 1e-3;
+  t = t0;
+  switch (L.temporal) {
+  case 1: {
+    const double u1 = (double)uniform<R>(g, rp);
+    const double u2 = (double)uniform<R>(g, rp);
+    const double z0 = sqrt(-2.0 * log(u1)) * cos(2.0 * 3.141592653589793 * u2);
+    t = z0 * (L.pulse_duration * (1.0 / (2.0 * sqrt(2.0 * log(2.0)))) * 1e-3) + t0;
+    break;
+  }
+  case 2: t = t0 + ((double)uniform<R>(g, rp) - 0.5) * L.pulse_duration * 1e-3; break;
+  case 3: t = t0 - log((double)uniform<R>(g, rp)) * L.pulse_duration * 1e-3; break;
+  case 4: t = (L.repetition_rate <= 0.0) ? t0 : t0 + (double)uniform<R>(g, rp) * (1e9 / L.repetition_rate); break;
+  case 5: t = (L.pulse_duration <= 0.0) ? t0 : t0 + (double)uniform<R>(g, rp) * L.pulse_duration * 1e-3; break;
+  default: break;
+  }
+}
+
+// Emission time of the current photon, re-derived from its stream (counter-based,
+// so draws 0.. can be regenerated at any time).
+template <typename R>
+__device__ double launch_time(const Scene &sc, const RunParams &rp, const Photon<R> &ph)
+{
+  if (sc.laser.temporal == 0)
+    return sc.laser.time_offset * 1e-3;
+  Rng g = {ph.rng.p_lo, ph.rng.p_hi, 0u, 0u, 0u, 0u, 0u};
+  double x, y, t;
+  source_sample<R>(sc.laser, g, rp, x, y, t);
+  return t;
+}
+
+// ---------------------------------------------------------------- hit snapshot
+// What a sensor's process_hit reads from the photon at a plane crossing.
+template <typename R> struct HitData {
+  uint32_t p_lo, p_hi, events, first_med, last_med;
+  double w, opath;             // weight, geometric path length at the hit point
+  R hx, hy, hz;                // hit point
+  R P[9];                      // P_local rows m, n, s
+  Cx<R> Em, En;
+  R r1[3], rn[3];              // CBS: first and newest scatter positions
+  R P1[9], Pn1[9];             // CBS: frame after the first scatter, before the newest
+  Cx<R> T[4];                  // CBS: interior Jones product
+};
+
+// ---------------------------------------------------------------- CBS reverse path
+// reverse_field (src/detector.cpp:1080-1173): stages A (scatter at r_n), B
+// (interior by reciprocity, Q T^T Q) and C (scatter at r_1), normalised once.
+template <typename R>
+__device__ void reverse_field(const Scene &sc, const HitData<R> &h, Cx<R> &Om, Cx<R> &On)
+{
+  const Laser &L = sc.laser;
+  const V3<R> m0 = v3<R>(R(L.m[0]), R(L.m[1]), R(L.m[2]));
+  const V3<R> n0 = v3<R>(R(L.n[0]), R(L.n[1]), R(L.n[2]));
+  const V3<R> s0 = v3<R>(R(L.dir[0]), R(L.dir[1]), R(L.dir[2]));
+  const Cx<R> E0m = {R(L.E[0]), R(L.E[1])}, E0n = {R(L.E[2]), R(L.E[3])};
+  // Stage A: s0 -> -s_{n-1} at r_n, species of the last vertex
+  const V3<R> mnm1 = row(h.Pn1, 0), nnm1 = row(h.Pn1, 1), snm1 = row(h.Pn1, 2);
+  const V3<R> s_out_a = vscale(snm1, R(-1));
+  Cx<R> Sa2, Sa1;
+  amplitudes<R>(sc.media[h.last_med], unit_angle(s0, s_out_a), Sa2, Sa1);
+  const V3<R> np_ = safe_unit(vcross_unit(s0, s_out_a), n0);
+  const V3<R> mp_in = safe_unit(vcross_unit(np_, s0), m0);
+  const V3<R> mp_out = safe_unit(vcross_unit(np_, s_out_a), mnm1);
+  R r00 = vdot(mp_in, m0), r01 = vdot(mp_in, n0), r10 = vdot(np_, m0), r11 = vdot(np_, n0);
+  Cx<R> Em = cadd(cmul(cscale(Sa2, r00), E0m), cmul(cscale(Sa2, r01), E0n));
+  Cx<R> En = cadd(cmul(cscale(Sa1, r10), E0m), cmul(cscale(Sa1, r11), E0n));
+  const V3<R> nn1 = vscale(nnm1, R(-1));
+  r00 = vdot(mnm1, mp_out); r01 = vdot(mnm1, np_); r10 = vdot(nn1, mp_out); r11 = vdot(nn1, np_);
+  Cx<R> tm = cadd(cscale(Em, r00), cscale(En, r01));
+  Cx<R> tn = cadd(cscale(Em, r10), cscale(En, r11));
+  // Stage B: E <- Q T^T Q E, Q = diag(1, -1)
+  tn = {-tn.re, -tn.im};
+  Em = cadd(cmul(h.T[0], tm), cmul(h.T[2], tn));
+  En = cadd(cmul(h.T[1], tm), cmul(h.T[3], tn));
+  En = {-En.re, -En.im};
+  // Stage C: -s_1 -> s_n at r_1, species of the first vertex
+  const V3<R> m1 = row(h.P1, 0), n1 = row(h.P1, 1), s1 = row(h.P1, 2);
+  const V3<R> mn = row(h.P, 0), nn = row(h.P, 1), sn = row(h.P, 2);
+  const V3<R> s_in_c = vscale(s1, R(-1));
+  const V3<R> n1m = vscale(n1, R(-1));
+  Cx<R> Sc2, Sc1;
+  amplitudes<R>(sc.media[h.first_med], unit_angle(s_in_c, sn), Sc2, Sc1);
+  const V3<R> npp = safe_unit(vcross_unit(s_in_c, sn), n1m);
+  const V3<R> mpp_in = safe_unit(vcross_unit(npp, s_in_c), m1);
+  const V3<R> mpp_out = safe_unit(vcross_unit(npp, sn), mn);
+  r00 = vdot(mpp_in, m1); r01 = vdot(mpp_in, n1m); r10 = vdot(npp, m1); r11 = vdot(npp, n1m);
+  const Cx<R> Fm = cadd(cmul(cscale(Sc2, r00), Em), cmul(cscale(Sc2, r01), En));
+  const Cx<R> Fn = cadd(cmul(cscale(Sc1, r10), Em), cmul(cscale(Sc1, r11), En));
+  r00 = vdot(mn, mpp_out); r01 = vdot(mn, npp); r10 = vdot(nn, mpp_out); r11 = vdot(nn, npp);
+  Cx<R> gm = cadd(cscale(Fm, r00), cscale(Fn, r01));
+  Cx<R> gn = cadd(cscale(Fm, r10), cscale(Fn, r11));
+  const R nrm = m_sqrt(cnorm(gm) + cnorm(gn));
+  if (nrm > tiny<R>()) {
+    gm = {gm.re / nrm, gm.im / nrm};
+    gn = {gn.re / nrm, gn.im / nrm};
+  } else {
+    gm = {R(0), R(0)};
+    gn = {R(0), R(0)};
+  }
+  Om = gm;
+  On = gn;
+}
+
+// ------------------------------------------------------------------- tallies
+__device__ __forceinline__ void add4(double *base, unsigned long long stride, unsigned long long off,
+                                     double a, double b, double c, double d)
+{
+  atomicAdd(base + off, a);
+  atomicAdd(base + stride + off, b);
+  atomicAdd(base + 2 * stride + off, c);
+  atomicAdd(base + 3 * stride + off, d);
+}
+
+__device__ __forceinline__ int time_bin(const Sensor &s, double arrival)
+{                                                          // src/detector.cpp:1182-1190
+  if (s.dt <= 0)
+    return 0;
+  if (arrival < 0 || arrival >= s.len_t)
+    return -1;
+  const int idx = (int)(arrival / s.dt) + 1;
+  return (idx < s.N_t) ? idx : -1;
+}
+
+template <typename R>
+__device__ __forceinline__ double hit_launch_time(const Scene &sc, const RunParams &rp, const HitData<R> &h)
+{
+  if (sc.laser.temporal == 0)
+    return sc.laser.time_offset * 1e-3;
+  Rng g = {h.p_lo, h.p_hi, 0u, 0u, 0u, 0u, 0u};
+  double x, y, t;
+  source_sample<R>(sc.laser, g, rp, x, y, t);
+  return t;
+}
+
+// FarFieldCBSSensor::process_hit (src/detector.cpp:1231-1310) and the far-field
+// fluence sensor (same binning, reverse field zero).  exp(i k L) multiplies E_f
+// and E_r alike and cancels in every Stokes parameter, so it is not formed.
+template <typename R>
+__device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor &s,
+                             const HitData<R> &h, lmc_record *rec)
+{
+  const double t_launch = (s.dt > 0) ? hit_launch_time<R>(sc, rp, h) : 0.0;
+  const int t_idx = time_bin(s, t_launch + h.opath);
+  if (t_idx < 0)
+    return false;
+  const R sx = h.P[6], sy = h.P[7], sz = h.P[8];
+  const R theta = exit_theta(sx, sy, sz);
+  R phi = m_atan2(sy, sx);
+  if (phi < R(0))
+    phi += R(6.283185307179586);
+  const int it = (int)(theta / R(s.dtheta));
+  const int jp = (int)(phi / R(s.dphi));
+  if (it < 0 || it >= s.N_theta || jp < 0 || jp >= s.N_phi)
+    return false;
+  const R w_sqrt = R(sqrt(h.w));
+  const Cx<R> Em = cscale(h.Em, w_sqrt), En = cscale(h.En, w_sqrt);
+  // project_to_lab (src/detector.cpp:1048-1053)
+  const Cx<R> Efx = cadd(cscale(Em, h.P[0]), cscale(En, h.P[3]));
+  const Cx<R> Efy = cadd(cscale(Em, h.P[1]), cscale(En, h.P[4]));
+  const unsigned long long cell = ((unsigned long long)it) * s.N_phi + jp;
+  const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
+  double *base = rp.tallies + s.tally_off;
+  const unsigned long long P = s.plane_stride;
+  if (s.kind == LMC_SENSOR_FARFIELD_FLUENCE) {
+    const double q0 = (double)(cnorm(Efx) + cnorm(Efy)), q1 = (double)(cnorm(Efx) - cnorm(Efy));
+    const Cx<R> xy = cmul(Efx, Cx<R>{Efy.re, -Efy.im});
+    const double q2 = 2.0 * (double)xy.re, q3 = 2.0 * (double)xy.im;
+    add4(base, P, cell, q0, q1, q2, q3);
+    if (t_idx >= 1)
+      add4(base, P, t_idx * tstride + cell, q0, q1, q2, q3);
+    return true;
+  }
+  Cx<R> Erx = {R(0), R(0)}, Ery = {R(0), R(0)};
+  if (h.events >= 2) {
+    Cx<R> Rm, Rn;
+    reverse_field<R>(sc, h, Rm, Rn);
+    if (rec) {                     // photon.polarization_reverse, kept for the replay check
+      rec->Er[0] = Rm.re; rec->Er[1] = Rm.im; rec->Er[2] = Rn.re; rec->Er[3] = Rn.im;
+    }
+    // CBS geometric phase exp(i k (s_out + s_in).(r_n - r_1)) in binary64
+    const Laser &L = sc.laser;
+    const double qx = ((double)sx + L.dir[0]) * L.k, qy = ((double)sy + L.dir[1]) * L.k,
+                 qz = ((double)sz + L.dir[2]) * L.k;
+    const double arg = qx * ((double)h.rn[0] - (double)h.r1[0]) +
+                       qy * ((double)h.rn[1] - (double)h.r1[1]) +
+                       qz * ((double)h.rn[2] - (double)h.r1[2]);
+    double sp, cp;
+    sincos(arg, &sp, &cp);
+    const Cx<R> pp = {R(cp), R(sp)};
+    const Cx<R> Rm2 = cmul(cscale(Rm, w_sqrt), pp), Rn2 = cmul(cscale(Rn, w_sqrt), pp);
+    Erx = cadd(cscale(Rm2, h.P[0]), cscale(Rn2, h.P[3]));
+    Ery = cadd(cscale(Rm2, h.P[1]), cscale(Rn2, h.P[4]));
+  }
+  // accumulate_stokes (src/detector.cpp:1194-1226)
+  const Cx<R> Ex = cadd(Efx, Erx), Ey = cadd(Efy, Ery);
+  const Cx<R> c_xy = cmul(Ex, Cx<R>{Ey.re, -Ey.im});
+  const Cx<R> f_xy = cmul(Efx, Cx<R>{Efy.re, -Efy.im});
+  const Cx<R> r_xy = cmul(Erx, Cx<R>{Ery.re, -Ery.im});
+  const double c0 = (double)(cnorm(Ex) + cnorm(Ey)), c1 = (double)(cnorm(Ex) - cnorm(Ey));
+  const double c2 = 2.0 * (double)c_xy.re, c3 = 2.0 * (double)c_xy.im;
+  const double i0 = (double)(cnorm(Efx) + cnorm(Efy) + cnorm(Erx) + cnorm(Ery));
+  const double i1 = (double)(cnorm(Efx) - cnorm(Efy) + cnorm(Erx) - cnorm(Ery));
+  const double i2 = 2.0 * ((double)f_xy.re + (double)r_xy.re);
+  const double i3 = 2.0 * ((double)f_xy.im + (double)r_xy.im);
+  add4(base, P, cell, c0, c1, c2, c3);
+  add4(base + 4 * P, P, cell, i0, i1, i2, i3);
+  if (t_idx >= 1) {
+    add4(base, P, t_idx * tstride + cell, c0, c1, c2, c3);
+    add4(base + 4 * P, P, t_idx * tstride + cell, i0, i1, i2, i3);
+  }
+  return true;
+}
+
+// PlanarFluenceSensor::process_hit (src/detector.cpp:780-841): lab-frame Stokes
+// with E_x negated; exp(i k L) cancels and is not formed.
+template <typename R>
+__device__ bool hit_fluence(const Scene &sc, const RunParams &rp, const Sensor &s, const HitData<R> &h)
+{
+  int t_idx = -1;
+  if (s.dt > 0) {
+    const double arrival = hit_launch_time<R>(sc, rp, h) + h.opath;
+    if (arrival < 0 || arrival >= s.len_t)
+      return false;
+    t_idx = (int)(arrival / s.dt) + 1;
+    if (t_idx >= s.N_t)
+      return false;
+  }
+  const int xi = (int)(((double)h.hx + 0.5 * s.len_x) / s.dx);
+  const int yi = (int)(((double)h.hy + 0.5 * s.len_y) / s.dy);
+  if (xi < 0 || xi >= s.N_x || yi < 0 || yi >= s.N_y)
+    return false;
+  const R w_sqrt = R(sqrt(h.w));
+  const Cx<R> Em = cscale(h.Em, w_sqrt), En = cscale(h.En, w_sqrt);
+  const Cx<R> Ex = cscale(cadd(cscale(Em, h.P[0]), cscale(En, h.P[3])), R(-1));
+  const Cx<R> Ey = cadd(cscale(Em, h.P[1]), cscale(En, h.P[4]));
+  const Cx<R> xy = cmul(Ex, Cx<R>{Ey.re, -Ey.im});
+  const double q0 = (double)(cnorm(Ex) + cnorm(Ey)), q1 = (double)(cnorm(Ex) - cnorm(Ey));
+  const double q2 = 2.0 * (double)xy.re, q3 = 2.0 * (double)xy.im;
+  double *base = rp.tallies + s.tally_off;
+  const unsigned long long cell = (unsigned long long)xi * s.N_y + yi;
+  const unsigned long long tstride = (unsigned long long)s.N_x * s.N_y;
+  if (s.dt > 0)
+    add4(base, s.plane_stride, t_idx * tstride + cell, q0, q1, q2, q3);
+  add4(base, s.plane_stride, cell, q0, q1, q2, q3);
+  return true;
+}
+
+// PlanarFieldSensor::process_hit (src/detector.cpp:546-568): complex field with
+// the propagation phase exp(i k L), L = n * (path length at the hit).
+template <typename R>
+__device__ bool hit_field(const Scene &sc, const RunParams &rp, const Sensor &s, const HitData<R> &h)
+{
+  const int xi = (int)(((double)h.hx + 0.5 * s.len_x) / s.dx);
+  const int yi = (int)(((double)h.hy + 0.5 * s.len_y) / s.dy);
+  if (xi < 0 || xi >= s.N_x || yi < 0 || yi >= s.N_y)
+    return false;
+  double pi, pr;
+  sincos(sc.laser.k * (sc.n_step * h.opath), &pi, &pr);
+  const double w_sqrt = sqrt(h.w);
+  const double P0 = h.P[0], P1 = h.P[1], P3 = h.P[3], P4 = h.P[4];
+  const double exr = (double)h.Em.re * P0 + (double)h.En.re * P3;
+  const double exi = (double)h.Em.im * P0 + (double)h.En.im * P3;
+  const double eyr = (double)h.Em.re * P1 + (double)h.En.re * P4;
+  const double eyi = (double)h.Em.im * P1 + (double)h.En.im * P4;
+  double *base = rp.tallies + s.tally_off;
+  const unsigned long long off = ((unsigned long long)xi * s.N_y + yi) * 2;
+  atomicAdd(base + off, (exr * pr - exi * pi) * w_sqrt);
+  atomicAdd(base + off + 1, (exr * pi + exi * pr) * w_sqrt);
+  atomicAdd(base + s.plane_stride + off, (eyr * pr - eyi * pi) * w_sqrt);
+  atomicAdd(base + s.plane_stride + off + 1, (eyr * pi + eyi * pr) * w_sqrt);
+  return true;
+}
+
+// process_hit of every sensor in `mask` (all on the plane of this hit), in
+// insertion order, as SensorsGroup::record_hit calls them (src/detector.cpp:244-265).
+template <typename R>
+__device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData<R> &h,
+                             unsigned mask, unsigned long long *hits)
+{
+  lmc_record *rec = rp.records ? rp.records + ((((unsigned long long)h.p_hi << 32) | h.p_lo) -
+                                               rp.photon_begin)
+                               : nullptr;
+  for (int si = 0; si < sc.n_sensors; ++si) {
+    if (!(mask & (1u << si)))
+      continue;
+    const Sensor &s = sc.sensors[si];
+    bool counted;
+    if (s.kind == LMC_SENSOR_PLANAR_FLUENCE)
+      counted = hit_fluence<R>(sc, rp, s, h);
+    else if (s.kind == LMC_SENSOR_PLANAR_FIELD)
+      counted = hit_field<R>(sc, rp, s, h);
+    else
+      counted = hit_farfield<R>(sc, rp, s, h, rec);
+    if (counted) {
+      atomicAdd(hits + si, 1ull);
+      if (rec) {
+        rec->hit[0] = h.hx;
+        rec->hit[1] = h.hy;
+        rec->hit[2] = h.hz;
+        atomicAdd(&rec->n_hits, 1);
+      }
+    }
+  }
+}
+
+// Sensor::check_conditions (src/detector.cpp:374-417)
+template <typename R>
+__device__ __forceinline__ bool check_conditions(const Sensor &s, double hx, double hy, const Photon<R> &ph,
+                                                 int crossing)
+{
+  if (s.f_dir && s.direction != 2 && s.direction != crossing)
+    return false;
+  if (s.f_events && ((int)ph.events < s.events_min || (int)ph.events > s.events_max))
+    return false;
+  if (s.f_theta) {
+    const double ct = -1.0 * (double)ph.P[8];
+    if (ct < s.cos_min || ct > s.cos_max)
+      return false;
+  }
+  if (s.f_phi) {
+    double phi = atan2((double)ph.P[7], (double)ph.P[6]);
+    if (phi < 0)
+      phi += 2.0 * 3.141592653589793;
+    if (phi < s.phi_min || phi > s.phi_max)
+      return false;
+  }
+  if (s.f_pos) {
+    if (hx < s.x_min || hx > s.x_max || hy < s.y_min || hy > s.y_max)
+      return false;
+  }
+  return true;
+}
+
+template <typename R>
+__device__ __forceinline__ void fill_hit(const Photon<R> &ph, const Side<R> &side, R hx, R hy, R hz,
+                                         double opath, HitData<R> &h)
+{
+  const int tid = threadIdx.x;
+  h.p_lo = ph.rng.p_lo;
+  h.p_hi = ph.rng.p_hi;
+  h.events = ph.events;
+  h.first_med = side.first_med[tid];
+  h.last_med = ph.last_med;
+  h.w = ph.w;
+  h.opath = opath;
+  h.hx = hx; h.hy = hy; h.hz = hz;
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    h.P[j] = ph.P[j];
+    h.P1[j] = side.first[3 + j][tid];
+    h.Pn1[j] = ph.Pn1[j];
+  }
+  h.Em = ph.Em;
+  h.En = ph.En;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    h.r1[j] = side.first[j][tid];
+    h.rn[j] = ph.rn[j];
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    h.T[q] = ph.T[q];
+}
+
+// Append a hit to the queue (warp-aggregated slot).  Only the fields the
+// sensors in `mask` read are written.
+template <typename R>
+__device__ __forceinline__ void enqueue_hit(const RunParams &rp, const Photon<R> &ph, const Side<R> &side,
+                                            R hx, R hy, R hz, double opath, unsigned mask)
+{
+  const unsigned active = __activemask();
+  const unsigned lane = threadIdx.x & 31u;
+  const int leader = __ffs(active) - 1;
+  unsigned long long base = 0;
+  if ((int)lane == leader)
+    base = atomicAdd(&rp.scratch->queue_count, (unsigned long long)__popc(active));
+  base = __shfl_sync(active, base, leader);
+  const unsigned long long slot = base + __popc(active & ((1u << lane) - 1u));
+  const Queue &q = rp.queue;
+  if (slot >= q.cap) {
+    atomicOr(&rp.scratch->error_flags, (unsigned)kErrQueueOverflow);
+    return;
+  }
+  const int tid = threadIdx.x;
+  const unsigned long long C = q.cap;
+  q.u32[kQPhotonLo * C + slot] = ph.rng.p_lo;
+  q.u32[kQPhotonHi * C + slot] = ph.rng.p_hi;
+  q.u32[kQEvents * C + slot] = ph.events;
+  q.u32[kQMask * C + slot] = mask;
+  q.u32[kQMedia * C + slot] = (uint32_t)side.first_med[tid] | ((uint32_t)ph.last_med << 16);
+  q.f64[kQWeight * C + slot] = ph.w;
+  q.f64[kQOpath * C + slot] = opath;
+  R *r = static_cast<R *>(q.r);
+  r[(kQHit + 0) * C + slot] = hx;
+  r[(kQHit + 1) * C + slot] = hy;
+  r[(kQHit + 2) * C + slot] = hz;
+#pragma unroll
+  for (int j = 0; j < 9; ++j)
+    r[(kQP + j) * C + slot] = ph.P[j];
+  r[(kQE + 0) * C + slot] = ph.Em.re;
+  r[(kQE + 1) * C + slot] = ph.Em.im;
+  r[(kQE + 2) * C + slot] = ph.En.re;
+  r[(kQE + 3) * C + slot] = ph.En.im;
+  if (mask & rp.cbs_mask) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      r[(kQR1 + j) * C + slot] = side.first[j][tid];
+      r[(kQRn + j) * C + slot] = ph.rn[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      r[(kQP1 + j) * C + slot] = side.first[3 + j][tid];
+      r[(kQPn1 + j) * C + slot] = ph.Pn1[j];
+    }
+#pragma unroll
+    for (int qd = 0; qd < 4; ++qd) {
+      r[(kQT + 2 * qd) * C + slot] = ph.T[qd].re;
+      r[(kQT + 2 * qd + 1) * C + slot] = ph.T[qd].im;
+    }
+  }
+}
+
+// SensorsGroup::record_hit (src/detector.cpp:178-270) for the step (x0,y0,z0) -> pos.
+// kQueue: hits are appended to the queue for the tally kernel; otherwise they are
+// processed here.  Returns whether an absorbing sensor took the photon.
+template <typename R, bool kQueue>
+__device__ __forceinline__ bool record_hit(const Scene &sc, const RunParams &rp, Photon<R> &ph,
+                                           const Side<R> &side, R x0, R y0, R z0,
+                                           unsigned long long *s_hits)
+{
+  const R z1 = z0, z2 = ph.pz;
+  const int crossing = (z2 > z1) ? 0 : 1;
+  const R zmin = z1 < z2 ? z1 : z2, zmax = z1 < z2 ? z2 : z1;
+  bool killed = false;
+  for (int g = 0; g < sc.n_planes; ++g) {
+    const R zp = sc_plane<R>(sc, g);
+    if (!(zp >= zmin && zp <= zmax))
+      continue;
+    const R dx = ph.px - x0, dy = ph.py - y0, dz = z2 - z1;
+    const R t = (zp - z1) / dz;
+    const R hx = x0 + dx * t, hy = y0 + dy * t, hz = z1 + dz * t;
+    const R ex = hx - ph.px, ey = hy - ph.py, ez = hz - ph.pz;
+    const R corr = m_sqrt(ex * ex + ey * ey + ez * ez);
+    const double opath = ph.opath - (corr > R(0) ? (double)corr : 0.0);
+    unsigned mask = 0;
+    for (int si = 0; si < sc.n_sensors; ++si) {
+      const Sensor &s = sc.sensors[si];
+      if (s.plane != g || s.estimator)
+        continue;
+      if (!check_conditions<R>(s, (double)hx, (double)hy, ph, crossing))
+        continue;
+      mask |= 1u << si;
+      if (s.absorb)
+        killed = true;
+    }
+    if (mask) {
+      if (kQueue) {
+        enqueue_hit<R>(rp, ph, side, hx, hy, hz, opath, mask);
+      } else {
+        HitData<R> h;
+        fill_hit<R>(ph, side, hx, hy, hz, opath, h);
+        process_hits<R>(sc, rp, h, mask, s_hits);
+      }
+    }
+  }
+  return killed;
+}
+
+template <typename R>
+__device__ void init_photon(const Scene &sc, const RunParams &rp, Photon<R> &ph, Side<R> &side,
+                            unsigned long long index)
+{
+  const Laser &L = sc.laser;
+  ph.rng.p_lo = (uint32_t)index;
+  ph.rng.p_hi = (uint32_t)(index >> 32);
+  ph.rng.draw = 0;
+  double x, y, t;
+  source_sample<R>(L, ph.rng, rp, x, y, t);
+  ph.px = R(x);
+  ph.py = R(y);
+  ph.pz = R(L.pos[2]);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    ph.P[j] = R(L.m[j]);
+    ph.P[3 + j] = R(L.n[j]);
+    ph.P[6 + j] = R(L.dir[j]);
+  }
+  ph.Em = {R(L.E[0]), R(L.E[1])};
+  ph.En = {R(L.E[2]), R(L.E[3])};
+  ph.w = 1.0;
+  ph.pen = R(0);
+  ph.opath = 0.0;
+  ph.events = 0;
+  ph.layer = layer_index_at<R>(sc, ph.pz);
+  ph.last_med = 0;
+  ph.rn[0] = ph.px; ph.rn[1] = ph.py; ph.rn[2] = ph.pz;
+#pragma unroll
+  for (int j = 0; j < 9; ++j)
+    ph.Pn1[j] = ph.P[j];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    ph.T[q] = {R(q == 0 || q == 3 ? 1 : 0), R(0)};
+  const int tid = threadIdx.x;                              // r_1 = launch, P1 = P0
+  side.first[0][tid] = ph.px; side.first[1][tid] = ph.py; side.first[2][tid] = ph.pz;
+#pragma unroll
+  for (int j = 0; j < 9; ++j)
+    side.first[3 + j][tid] = ph.P[j];
+  side.first_med[tid] = 0;
+}
+
+enum Fate { kAlive = 0, kDetected = 1, kEscaped = 2, kStack = 3, kRoulette = 4, kCap = 5, kError = 6 };
+
+// Upper bound on azimuth rejection trials per event.  The acceptance rate is
+// >= 1/2 for any finite (S, E) (F(phi) averages (a+b)/2 >= Fmax/2), so this is
+// only reached when the state is not finite; the photon is then dropped and
+// the run reports kErrAborted instead of spinning.
+constexpr int kMaxRejectionTrials = 1 << 16;
+
+// One loop iteration of run_photon (src/simulation.cpp:297-614).  Returns the
+// photon's fate (kAlive if it continues).
+template <typename R, bool kQueue>
+__device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, Photon<R> &ph,
+                                          Side<R> &side, Counters &cnt, unsigned long long *s_hits)
+{
+  {
+    const Medium &cm = sc.media[sc.layers[ph.layer].medium];
+    R step = -med_mfp<R>(cm) * m_log(uniform<R>(ph.rng, rp));   // src/medium.cpp:123-126
+    cnt.steps++;
+    const R dx = ph.P[6], dy = ph.P[7], dz = ph.P[8];
+    if (sc.n_interfaces > 0) {                               // src/simulation.cpp:318-382
+      R zi;
+      bool found = find_next_interface<R>(sc, ph.pz, ph.pz + dz * step, zi);
+      for (int crossings = 0; found; ++crossings) {
+        if (crossings > sc.n_interfaces)                     // each crossing passes a distinct interface
+          return kError;
+        const R dz_total = dz * step;
+        if (fabs(dz_total) < R(1e-15))
+          break;
+        const R t = (zi - ph.pz) / dz_total;
+        if (t < R(0) || t > R(1))
+          break;
+        const R s_if = step * t;
+        const R rem = (step - s_if) * med_mut<R>(sc.media[sc.layers[ph.layer].medium]);
+        ph.opath += (double)s_if;
+        const R x0 = ph.px, y0 = ph.py, z0 = ph.pz;
+        ph.px += dx * s_if;
+        ph.py += dy * s_if;
+        ph.pz = m_nudge(zi + ((dz > R(0)) ? R(1e-12) : R(-1e-12)), zi, dz > R(0));
+        if (sc.n_planes > 0 && fabs(ph.pz - z0) >= R(1e-12) &&
+            record_hit<R, kQueue>(sc, rp, ph, side, x0, y0, z0, s_hits))
+          return kDetected;
+        const int nl = layer_index_at<R>(sc, ph.pz);
+        if (nl >= sc.n_layers)
+          return kStack;
+        ph.layer = nl;
+        const R nmt = med_mut<R>(sc.media[sc.layers[nl].medium]);
+        step = (nmt > R(0)) ? rem / nmt : rem;
+        found = find_next_interface<R>(sc, ph.pz, ph.pz + dz * step, zi);
+      }
+    }
+    ph.opath += (double)step;                                 // :389-400
+    const R x0 = ph.px, y0 = ph.py, z0 = ph.pz;
+    ph.px += dx * step;
+    ph.py += dy * step;
+    ph.pz += dz * step;
+    if (ph.pz > ph.pen)
+      ph.pen = ph.pz;
+    // record_hit (:403-408): only when the step can reach a plane
+    if (sc.n_planes > 0 && fabs(ph.pz - z0) >= R(1e-12)) {
+      const R zlo = z0 < ph.pz ? z0 : ph.pz, zhi = z0 < ph.pz ? ph.pz : z0;
+      if (sc_plane<R>(sc, 0) <= zhi && sc_plane<R>(sc, sc.n_planes - 1) >= zlo &&
+          record_hit<R, kQueue>(sc, rp, ph, side, x0, y0, z0, s_hits))
+        return kDetected;
+    }
+    // Sample::is_inside (src/sample.cpp:268-288)
+    if (!(isfinite(ph.px) && isfinite(ph.py) && isfinite(ph.pz)) || ph.pz < R(0) ||
+        (!sc.top_is_inf && ph.pz >= sc_top<R>(sc)))
+      return kEscaped;
+  }
+  ph.layer = layer_index_at<R>(sc, ph.pz);
+  const int med_idx = sc.layers[ph.layer].medium;
+  const Medium &m = sc.media[med_idx];
+
+  const R theta = sample_theta<R>(m, uniform<R>(ph.rng, rp));  // :429
+  Cx<R> S2, S1;
+  amplitudes<R>(m, theta, S2, S1);                            // :430
+  // sample_phi_conditional (src/phase.cpp:27-49)
+  const R s2sq = cnorm(S2), s1sq = cnorm(S1);
+  const R e1sq = cnorm(ph.Em), e2sq = cnorm(ph.En);
+  const R e12 = ph.Em.re * ph.En.re + ph.Em.im * ph.En.im;
+  const R a = s2sq * e1sq + s1sq * e2sq;
+  const R b = s1sq * e1sq + s2sq * e2sq;
+  const R c = R(2) * (s2sq - s1sq) * e12;
+  const R diff = a - b;
+  const R Fmax = R(0.5) * (a + b) + R(0.5) * m_sqrt(diff * diff + c * c);
+  R cp, sp;
+  for (int trial = 0;; ++trial) {
+    if (trial == kMaxRejectionTrials)
+      return kError;
+    const R u1 = uniform<R>(ph.rng, rp);
+    m_sincospi(R(2) * u1, &sp, &cp);
+    const R F = a * cp * cp + b * sp * sp + c * cp * sp;
+    const R Fc = F > R(0) ? F : R(0);
+    if (uniform<R>(ph.rng, rp) * Fmax <= Fc)
+      break;
+  }
+  R st, ct;
+  m_sincos(theta, &st, &ct);
+  // frame update P <- A(theta, phi) P (src/simulation.cpp:438-453); P_{n-1} <- old P
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const R mj = ph.P[j], nj = ph.P[3 + j], sj = ph.P[6 + j];
+    ph.Pn1[j] = mj;
+    ph.Pn1[3 + j] = nj;
+    ph.Pn1[6 + j] = sj;
+    ph.P[j] = ct * cp * mj + ct * sp * nj - st * sj;
+    ph.P[3 + j] = -sp * mj + cp * nj;
+    ph.P[6 + j] = st * cp * mj + st * sp * nj + ct * sj;
+  }
+  // Jones update E <- (S R(phi)) E / sqrt(F) (src/simulation.cpp:456-492)
+  {
+    const Cx<R> Em = ph.Em, En = ph.En;
+    const R pc = cp * cp, ps = sp * sp;
+    const R F = e1sq * (s2sq * pc + s1sq * ps) + e2sq * (s2sq * ps + s1sq * pc) +
+                R(2) * e12 * (s2sq - s1sq) * sp * cp;
+    const R inv = R(1) / m_sqrt(F);
+    const Cx<R> T00 = cscale(S2, cp * inv), T01 = cscale(S2, sp * inv);
+    const Cx<R> T10 = cscale(S1, -sp * inv), T11 = cscale(S1, cp * inv);
+    ph.Em = cadd(cmul(T00, Em), cmul(T01, En));
+    ph.En = cadd(cmul(T10, Em), cmul(T11, En));
+  }
+  if (rp.track_reverse) {                                     // :495-568
+    const int tid = threadIdx.x;
+    const uint32_t evt = ph.events + 1;
+    if (evt == 1) {
+      side.first[0][tid] = ph.px; side.first[1][tid] = ph.py; side.first[2][tid] = ph.pz;
+#pragma unroll
+      for (int j = 0; j < 9; ++j)
+        side.first[3 + j][tid] = ph.P[j];
+      side.first_med[tid] = med_idx;
+    }
+    ph.rn[0] = ph.px; ph.rn[1] = ph.py; ph.rn[2] = ph.pz;
+    ph.last_med = med_idx;
+    if (evt >= 3) {
+      // T <- normalise(J_{n-1} T), J_{n-1} = diag(S2, S1) R(phi) of the previous event
+      const Cx<R> pS2 = {side.last[0][tid], side.last[1][tid]};
+      const Cx<R> pS1 = {side.last[2][tid], side.last[3][tid]};
+      const R pc = side.last[4][tid], ps = side.last[5][tid];
+      const Cx<R> B00 = cscale(pS2, pc), B01 = cscale(pS2, ps), B10 = cscale(pS1, -ps), B11 = cscale(pS1, pc);
+      Cx<R> t0 = cadd(cmul(B00, ph.T[0]), cmul(B01, ph.T[2]));
+      Cx<R> t1 = cadd(cmul(B00, ph.T[1]), cmul(B01, ph.T[3]));
+      Cx<R> t2 = cadd(cmul(B10, ph.T[0]), cmul(B11, ph.T[2]));
+      Cx<R> t3 = cadd(cmul(B10, ph.T[1]), cmul(B11, ph.T[3]));
+      const R frob = m_sqrt(cnorm(t0) + cnorm(t1) + cnorm(t2) + cnorm(t3));
+      if (frob > tiny<R>()) {
+        const R inv = R(1) / frob;
+        t0 = cscale(t0, inv); t1 = cscale(t1, inv); t2 = cscale(t2, inv); t3 = cscale(t3, inv);
+      }
+      ph.T[0] = t0; ph.T[1] = t1; ph.T[2] = t2; ph.T[3] = t3;
+    }
+    if (evt >= 2) {
+      side.last[0][tid] = S2.re; side.last[1][tid] = S2.im;
+      side.last[2][tid] = S1.re; side.last[3][tid] = S1.im;
+      side.last[4][tid] = cp; side.last[5][tid] = sp;
+    }
+  }
+  ph.events++;                                                // :578-587
+  cnt.events++;
+  ph.w *= m.albedo;
+  if (ph.w < 1e-4) {                                          // :596-607
+    if (uniform<R>(ph.rng, rp) < R(0.1))
+      ph.w /= 0.1;
+    else
+      return kRoulette;
+  }
+  if ((int)ph.events > rp.max_events)                         // :609-613
+    return kCap;
+  return kAlive;
+}
+
+template <typename R>
+__device__ void write_record(const Scene &sc, const RunParams &rp, const Photon<R> &ph,
+                             const Side<R> &side, int fate)
+{
+  const int tid = threadIdx.x;
+  lmc_record &r = rp.records[ph.index() - rp.photon_begin];
+  r.photon = ph.index();
+  r.events = ph.events;
+  r.draws = ph.rng.draw;
+  r.fate = fate;
+  r.layer = ph.layer;
+  r.weight = ph.w;
+  r.opticalpath = ph.opath;
+  r.penetration_depth = ph.pen;
+  r.launch_time = launch_time<R>(sc, rp, ph);
+  r.pos[0] = ph.px; r.pos[1] = ph.py; r.pos[2] = ph.pz;
+  for (int j = 0; j < 3; ++j) {
+    r.m[j] = ph.P[j];
+    r.n[j] = ph.P[3 + j];
+    r.dir[j] = ph.P[6 + j];
+    r.r1[j] = side.first[j][tid];
+    r.rn[j] = ph.rn[j];
+  }
+  r.E[0] = ph.Em.re; r.E[1] = ph.Em.im; r.E[2] = ph.En.re; r.E[3] = ph.En.im;
+}
+
+// Copy the scene into shared memory (every thread reads it every event).
+__device__ __forceinline__ void load_scene(unsigned char *s_raw, const Scene *g_scene)
+{
+  const int4 *src = reinterpret_cast<const int4 *>(g_scene);
+  int4 *dst = reinterpret_cast<int4 *>(s_raw);
+  for (int i = threadIdx.x; i < (int)(sizeof(Scene) / 16); i += blockDim.x)
+    dst[i] = src[i];
+}
+
+template <typename R, bool kQueue>
+__global__ void __launch_bounds__(kBlock) transport_kernel(const Scene *__restrict__ g_scene, RunParams rp)
+{
+  __shared__ __align__(16) unsigned char s_raw[sizeof(Scene)];
+  __shared__ Side<R> side;
+  __shared__ unsigned long long s_hits[LMC_MAX_SENSORS];
+  __shared__ unsigned long long s_fate[7];
+  load_scene(s_raw, g_scene);
+  if (threadIdx.x < LMC_MAX_SENSORS)
+    s_hits[threadIdx.x] = 0;
+  if (threadIdx.x < 7)
+    s_fate[threadIdx.x] = 0;
+  __syncthreads();
+  const Scene &sc = *reinterpret_cast<const Scene *>(s_raw);
+  const unsigned lane = threadIdx.x & 31u;
+  Counters cnt = {0, 0, 0};
+  Photon<R> ph;
+  bool alive = false, done = false;
+  for (;;) {
+    const unsigned need = __ballot_sync(kFull, !alive && !done);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if ((int)lane == leader)
+        base = atomicAdd(&rp.scratch->next_photon, (unsigned long long)__popc(need));
+      base = __shfl_sync(kFull, base, leader);
+      if (!alive && !done) {
+        const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
+        if (idx < rp.n_photons) {
+          init_photon<R>(sc, rp, ph, side, rp.photon_begin + idx);
+          alive = true;
+        } else {
+          done = true;
+        }
+      }
+    }
+    if (__all_sync(kFull, done))
+      break;
+    if (alive) {
+      const int fate = event_step<R, kQueue>(sc, rp, ph, side, cnt, s_hits);
+      if (fate != kAlive) {
+        alive = false;
+        cnt.draws += ph.rng.draw;
+        atomicAdd(&s_fate[fate], 1ull);
+        if (rp.records)
+          write_record<R>(sc, rp, ph, side, fate);
+        if (fate == kError)
+          atomicOr(&rp.scratch->error_flags, (unsigned)kErrAborted);
+        if (!isfinite(ph.w))
+          atomicOr(&rp.scratch->error_flags, (unsigned)kErrNonFiniteWeight);
+      }
+    }
+  }
+  // warp-reduce the per-thread counters, then one atomic per warp
+  unsigned long long ev = cnt.events, st = cnt.steps, dr = cnt.draws;
+  for (int o = 16; o > 0; o >>= 1) {
+    ev += __shfl_down_sync(kFull, ev, o);
+    st += __shfl_down_sync(kFull, st, o);
+    dr += __shfl_down_sync(kFull, dr, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&rp.scratch->events, ev);
+    atomicAdd(&rp.scratch->steps, st);
+    atomicAdd(&rp.scratch->draws, dr);
+  }
+  __syncthreads();
+  if (threadIdx.x < LMC_MAX_SENSORS && s_hits[threadIdx.x])
+    atomicAdd(&rp.scratch->hits[threadIdx.x], s_hits[threadIdx.x]);
+  if (threadIdx.x == kError && s_fate[kError])
+    atomicAdd(&rp.scratch->photons, s_fate[kError]);
+  if (threadIdx.x >= 1 && threadIdx.x < 6 && s_fate[threadIdx.x]) {
+    unsigned long long *dst = threadIdx.x == kDetected ? &rp.scratch->detected
+                              : threadIdx.x == kEscaped ? &rp.scratch->escaped
+                              : threadIdx.x == kStack   ? &rp.scratch->stack
+                              : threadIdx.x == kRoulette ? &rp.scratch->roulette
+                                                         : &rp.scratch->cap;
+    atomicAdd(dst, s_fate[threadIdx.x]);
+    atomicAdd(&rp.scratch->photons, s_fate[threadIdx.x]);
+  }
+}
+
+// Tally kernel: one thread per queued hit runs the sensors' process_hit.
+template <typename R>
+__global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__ g_scene, RunParams rp)
+{
+  __shared__ __align__(16) unsigned char s_raw[sizeof(Scene)];
+  __shared__ unsigned long long s_hits[LMC_MAX_SENSORS];
+  load_scene(s_raw, g_scene);
+  if (threadIdx.x < LMC_MAX_SENSORS)
+    s_hits[threadIdx.x] = 0;
+  __syncthreads();
+  const Scene &sc = *reinterpret_cast<const Scene *>(s_raw);
+  const Queue &q = rp.queue;
+  const unsigned long long C = q.cap;
+  const unsigned long long count = *(volatile unsigned long long *)&rp.scratch->queue_count;
+  const unsigned long long n = count < C ? count : C;
+  const R *r = static_cast<const R *>(q.r);
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    HitData<R> h;
+    h.p_lo = q.u32[kQPhotonLo * C + i];
+    h.p_hi = q.u32[kQPhotonHi * C + i];
+    h.events = q.u32[kQEvents * C + i];
+    const unsigned mask = q.u32[kQMask * C + i];
+    const uint32_t media = q.u32[kQMedia * C + i];
+    h.first_med = media & 0xffffu;
+    h.last_med = media >> 16;
+    h.w = q.f64[kQWeight * C + i];
+    h.opath = q.f64[kQOpath * C + i];
+    h.hx = r[(kQHit + 0) * C + i];
+    h.hy = r[(kQHit + 1) * C + i];
+    h.hz = r[(kQHit + 2) * C + i];
+#pragma unroll
+    for (int j = 0; j < 9; ++j)
+      h.P[j] = r[(kQP + j) * C + i];
+    h.Em = {r[(kQE + 0) * C + i], r[(kQE + 1) * C + i]};
+    h.En = {r[(kQE + 2) * C + i], r[(kQE + 3) * C + i]};
+    if (mask & rp.cbs_mask) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        h.r1[j] = r[(kQR1 + j) * C + i];
+        h.rn[j] = r[(kQRn + j) * C + i];
+      }
+#pragma unroll
+      for (int j = 0; j < 9; ++j) {
+        h.P1[j] = r[(kQP1 + j) * C + i];
+        h.Pn1[j] = r[(kQPn1 + j) * C + i];
+      }
+#pragma unroll
+      for (int qd = 0; qd < 4; ++qd)
+        h.T[qd] = {r[(kQT + 2 * qd) * C + i], r[(kQT + 2 * qd + 1) * C + i]};
+    }
+    process_hits<R>(sc, rp, h, mask, s_hits);
+  }
+  __syncthreads();
+  if (threadIdx.x < LMC_MAX_SENSORS && s_hits[threadIdx.x])
+    atomicAdd(&rp.scratch->hits[threadIdx.x], s_hits[threadIdx.x]);
+}
+
+}  // namespace dev
+}  // namespace lmc

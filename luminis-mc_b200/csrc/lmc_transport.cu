@@ -1,0 +1,616 @@
+// lmc_transport.cu -- host side of the photon-propagation library: scene
+// validation and upload (lmc_create), launches (lmc_run, lmc_run_host), tally
+// layout and errors.  The kernel itself is in lmc_kernel.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "lmc_device.cuh"
+#include "lmc_internal.h"
+#include "lmc_kernel.cuh"
+#include "luminis_b200.h"
+
+namespace lmc {
+
+std::string &last_error()
+{
+  thread_local std::string s;
+  return s;
+}
+
+// ============================================================== host side ==
+namespace {
+
+struct CudaCheck {
+  cudaError_t e;
+};
+
+#define LMC_CUDA(call)                                                                      \
+  do {                                                                                      \
+    const cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(LMC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
+  } while (0)
+
+}  // namespace
+
+}  // namespace lmc
+
+struct lmc_handle {
+  lmc::dev::Scene scene;                 // host copy (device table pointers inside)
+  lmc::dev::Scene *d_scene = nullptr;
+  lmc::dev::Scratch *d_scratch = nullptr;
+  void *d_arena = nullptr;
+  size_t arena_bytes = 0;
+  size_t tally_doubles = 0;
+  size_t sensor_off[LMC_MAX_SENSORS] = {};
+  size_t sensor_count[LMC_MAX_SENSORS] = {};
+  int sensor_dims[LMC_MAX_SENSORS][4] = {};
+  int n_sensors = 0;
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double *d_host_tally = nullptr;        // staging for lmc_run_host
+  size_t host_tally_cap = 0;
+  void *d_queue = nullptr;               // hit queue (queued mode), grown on demand
+  size_t queue_bytes = 0;
+  unsigned cbs_mask = 0;                 // sensors that need the CBS fields of a hit
+  bool queued = false;                   // every sensor plane at z <= 0: queued kernel pair
+};
+
+namespace lmc {
+namespace {
+
+bool finite(double x) { return std::isfinite(x); }
+
+// Host lower_bound (first i with cdf[i] >= key), same predicate as the kernel.
+template <typename T> int lower_bound_idx(const std::vector<T> &cdf, T key)
+{
+  int lo = 0, hi = (int)cdf.size();
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (cdf[mid] < key)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+lmc_status validate(const lmc_scene *s)
+{
+  if (!s)
+    return fail(LMC_ERR_INVALID, "scene must not be null");
+  if (s->n_layers < 1 || s->n_layers > LMC_MAX_LAYERS)
+    return fail(LMC_ERR_INVALID, "the sample needs 1.." + std::to_string(LMC_MAX_LAYERS) + " layers");
+  if (s->n_media < 1 || s->n_media > LMC_MAX_MEDIA)
+    return fail(LMC_ERR_INVALID, "the sample needs 1.." + std::to_string(LMC_MAX_MEDIA) + " media");
+  if (s->n_sensors < 0 || s->n_sensors > LMC_MAX_SENSORS)
+    return fail(LMC_ERR_INVALID, "at most " + std::to_string(LMC_MAX_SENSORS) + " sensors");
+  if (!(s->n_host > 0.0) || !finite(s->n_host))
+    return fail(LMC_ERR_INVALID, "host refractive index must be positive and finite");
+  for (int l = 0; l < s->n_layers; ++l) {                  // src/sample.cpp:120-140
+    const lmc_layer_desc &L = s->layers[l];
+    if (L.medium < 0 || L.medium >= s->n_media)
+      return fail(LMC_ERR_INVALID, "layer medium index out of range");
+    if (!(L.z_max > L.z_min))
+      return fail(LMC_ERR_INVALID, "Sample::add_layer: z_max must be greater than z_min.");
+    if (l == 0 && L.z_min != 0.0)
+      return fail(LMC_ERR_INVALID, "Sample::add_layer: first layer must start at z = 0.");
+    if (l > 0 && L.z_min != s->layers[l - 1].z_max)
+      return fail(LMC_ERR_INVALID, "Sample::add_layer: layer z_min does not match previous z_max.");
+    if (l < s->n_layers - 1 && std::isinf(L.z_max))
+      return fail(LMC_ERR_INVALID, "Sample::add_layer: cannot add a layer after an infinite top layer.");
+  }
+  for (int i = 0; i < s->n_media; ++i) {
+    const lmc_medium_desc &M = s->media[i];
+    if (!finite(M.mu_a) || !finite(M.mu_s) || M.mu_a < 0 || M.mu_s < 0)
+      return fail(LMC_ERR_INVALID, "medium coefficients must be finite and non-negative");
+    if (!(M.mean_free_path > 0.0) || !finite(M.mean_free_path))
+      return fail(LMC_ERR_INVALID, "medium mean_free_path must be set (set_mean_free_path) and positive");
+    if (M.theta_kind == LMC_THETA_TABLE || M.theta_kind == LMC_THETA_TABLE_COS) {
+      if (M.theta_n < 2 || !M.theta_values || !M.theta_cdf)
+        return fail(LMC_ERR_INVALID, "phase-function sampling table missing");
+      for (int k = 1; k < M.theta_n; ++k)                    // std::lower_bound needs order
+        if (!(M.theta_cdf[k] >= M.theta_cdf[k - 1]))
+          return fail(LMC_ERR_INVALID, "phase-function CDF must be non-decreasing");
+      if (M.theta_cdf[M.theta_n - 1] != 1.0 || !(M.theta_cdf[0] >= 0.0))
+        return fail(LMC_ERR_INVALID, "phase-function CDF must lie in [0, 1] and end at 1");
+    } else if (M.theta_kind == LMC_THETA_HG) {
+      if (!(M.hg_g != 0.0) || !(M.hg_g >= -1.0 && M.hg_g <= 1.0))
+        return fail(LMC_ERR_INVALID, "Henyey-Greenstein g must be in [-1, 1] and non-zero");
+    } else if (M.theta_kind != LMC_THETA_UNIFORM) {
+      return fail(LMC_ERR_INVALID, "unknown theta sampling kind");
+    }
+    if (M.amp_n < 2 || !M.amp_s1 || !M.amp_s2 || !(M.amp_dtheta > 0.0))
+      return fail(LMC_ERR_INVALID, "medium amplitude table missing");
+  }
+  const lmc_laser_desc &L = s->laser;
+  if (!(L.wavelength > 0.0))
+    return fail(LMC_ERR_INVALID, "laser wavelength must be positive");
+  if (L.source < 0 || L.source > 2 || L.temporal < 0 || L.temporal > 5)
+    return fail(LMC_ERR_INVALID, "unknown laser source or temporal profile");
+  const double z = L.position[2];
+  const double top = s->layers[s->n_layers - 1].z_max;
+  if (!(z >= 0.0) || (!std::isinf(top) && z >= top))
+    return fail(LMC_ERR_INVALID, "laser position lies outside the sample (the reference throws "
+                                 "std::out_of_range from Sample::get_layer)");
+  for (int i = 0; i < s->n_sensors; ++i) {
+    const lmc_sensor_desc &S = s->sensors[i];
+    if (S.kind < 0 || S.kind > 3)
+      return fail(LMC_ERR_INVALID, "unknown sensor kind");
+    if (S.kind == LMC_SENSOR_FARFIELD_CBS && S.estimator)
+      return fail(LMC_ERR_UNSUPPORTED,
+                  "estimator-mode FarFieldCBSSensor (process_estimation) is not implemented");
+    if (S.kind == LMC_SENSOR_FARFIELD_CBS || S.kind == LMC_SENSOR_FARFIELD_FLUENCE) {
+      if (!(S.dtheta > 0) || !(S.dphi > 0) || !(S.theta_max_grid > 0) || !(S.phi_max_grid > 0))
+        return fail(LMC_ERR_INVALID, "far-field sensor bin widths and extents must be positive");
+    } else if (!(S.dx > 0) || !(S.dy > 0) || !(S.len_x > 0) || !(S.len_y > 0)) {
+      return fail(LMC_ERR_INVALID, "planar sensor pixel sizes and extents must be positive");
+    }
+    if (S.dt < 0 || (S.dt > 0 && !(S.len_t > 0)))
+      return fail(LMC_ERR_INVALID, "sensor time axis must have len_t > 0 when dt > 0");
+  }
+  return LMC_OK;
+}
+
+void fill_sensor(const lmc_sensor_desc &S, dev::Sensor &d, size_t &count, int dims[4])
+{
+  std::memset(&d, 0, sizeof(d));
+  d.kind = S.kind;
+  d.absorb = S.absorb;
+  d.estimator = S.estimator;
+  // Sensor::Sensor forces the estimator off away from z = 0 (src/detector.cpp:323-331)
+  if (S.z != 0.0 && S.estimator)
+    d.estimator = 0;
+  d.f_theta = S.f_theta;
+  if (S.f_theta) {                                          // src/detector.cpp:334-343
+    const double c1 = std::cos(S.theta_min), c2 = std::cos(S.theta_max);
+    d.cos_min = std::min(c1, c2);
+    d.cos_max = std::max(c1, c2);
+  }
+  d.f_phi = S.f_phi; d.phi_min = S.phi_min; d.phi_max = S.phi_max;
+  d.f_pos = S.f_pos; d.x_min = S.x_min; d.x_max = S.x_max; d.y_min = S.y_min; d.y_max = S.y_max;
+  d.f_dir = S.f_dir; d.direction = S.direction;
+  d.f_events = S.f_events; d.events_min = S.events_min; d.events_max = S.events_max;
+  d.len_x = S.len_x; d.len_y = S.len_y; d.len_t = S.len_t; d.dx = S.dx; d.dy = S.dy; d.dt = S.dt;
+  d.dtheta = S.dtheta; d.dphi = S.dphi;
+  if (S.kind == LMC_SENSOR_FARFIELD_CBS || S.kind == LMC_SENSOR_FARFIELD_FLUENCE) {
+    d.absorb = 1;                                           // Sensor(0.0, true, ...)
+    d.N_t = (S.dt == 0) ? 1 : (int)std::ceil(S.len_t / S.dt) + 1;
+    d.N_theta = (int)std::ceil(S.theta_max_grid / S.dtheta);
+    d.N_phi = (int)std::ceil(S.phi_max_grid / S.dphi);
+    const int planes = S.kind == LMC_SENSOR_FARFIELD_CBS ? 8 : 4;
+    d.plane_stride = (unsigned long long)d.N_t * d.N_theta * d.N_phi;
+    count = (size_t)planes * d.plane_stride;
+    dims[0] = planes; dims[1] = d.N_t; dims[2] = d.N_theta; dims[3] = d.N_phi;
+  } else if (S.kind == LMC_SENSOR_PLANAR_FLUENCE) {
+    d.N_t = (S.dt == 0) ? 1 : (int)std::ceil(S.len_t / S.dt) + 1;
+    d.N_x = (int)std::ceil(S.len_x / S.dx);
+    d.N_y = (int)std::ceil(S.len_y / S.dy);
+    d.plane_stride = (unsigned long long)d.N_t * d.N_x * d.N_y;
+    count = 4 * (size_t)d.plane_stride;
+    dims[0] = 4; dims[1] = d.N_t; dims[2] = d.N_x; dims[3] = d.N_y;
+  } else {
+    d.N_x = (int)std::ceil(S.len_x / S.dx);
+    d.N_y = (int)std::ceil(S.len_y / S.dy);
+    d.plane_stride = (unsigned long long)d.N_x * d.N_y * 2;
+    count = 2 * (size_t)d.plane_stride;
+    dims[0] = 2; dims[1] = d.N_x; dims[2] = d.N_y; dims[3] = 2;
+  }
+}
+
+}  // namespace
+}  // namespace lmc
+
+using lmc::fail;
+
+extern "C" {
+
+size_t lmc_last_error(char *buf, size_t len)
+{
+  const std::string &e = lmc::last_error();
+  if (buf && len) {
+    const size_t n = std::min(len - 1, e.size());
+    std::memcpy(buf, e.data(), n);
+    buf[n] = 0;
+  }
+  return e.size();
+}
+
+lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
+{
+  using namespace lmc;
+  if (!out)
+    return fail(LMC_ERR_INVALID, "out must not be null");
+  *out = nullptr;
+  const lmc_status v = validate(s);
+  if (v != LMC_OK)
+    return v;
+  int device = 0;
+  LMC_CUDA(cudaGetDevice(&device));
+  lmc_handle *h = new lmc_handle();
+  h->device = device;
+  LMC_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device));
+
+  dev::Scene &sc = h->scene;
+  std::memset(&sc, 0, sizeof(sc));
+  sc.n_layers = s->n_layers;
+  sc.n_media = s->n_media;
+  sc.n_sensors = s->n_sensors;
+  sc.top = s->layers[s->n_layers - 1].z_max;
+  sc.top_is_inf = std::isinf(sc.top) ? 1 : 0;
+  sc.top_f = (float)sc.top;
+  sc.n_step = 1.0 / (1.0 / s->n_host);                      // src/simulation.cpp:343,390
+  for (int l = 0; l < s->n_layers; ++l) {
+    sc.layers[l].z_min = s->layers[l].z_min;
+    sc.layers[l].z_max = s->layers[l].z_max;
+    sc.layers[l].medium = s->layers[l].medium;
+    if (l > 0) {
+      sc.interfaces[sc.n_interfaces] = s->layers[l].z_min;
+      sc.interfaces_f[sc.n_interfaces] = (float)s->layers[l].z_min;
+      sc.n_interfaces++;
+    }
+  }
+  const lmc_laser_desc &L = s->laser;
+  for (int j = 0; j < 3; ++j) {
+    sc.laser.pos[j] = L.position[j];
+    sc.laser.dir[j] = L.direction[j];
+    sc.laser.m[j] = L.local_m[j];
+    sc.laser.n[j] = L.local_n[j];
+  }
+  for (int j = 0; j < 4; ++j)
+    sc.laser.E[j] = L.jones[j];
+  sc.laser.k = 2.0 * M_PI / L.wavelength;                   // src/photon.cpp:39
+  sc.laser.sigma = L.sigma;
+  sc.laser.source = L.source;
+  sc.laser.temporal = L.temporal;
+  sc.laser.pulse_duration = L.pulse_duration;
+  sc.laser.repetition_rate = L.repetition_rate;
+  sc.laser.time_offset = L.time_offset;
+
+  // sensor planes: one key per z within 1e-9 (DoubleComparator, detector.hpp:46-48)
+  std::vector<double> planes;
+  size_t off = 0;
+  for (int i = 0; i < s->n_sensors; ++i) {
+    const lmc_sensor_desc &S = s->sensors[i];
+    dev::Sensor &d = sc.sensors[i];
+    size_t count = 0;
+    fill_sensor(S, d, count, h->sensor_dims[i]);
+    const double z = (S.kind == LMC_SENSOR_FARFIELD_CBS || S.kind == LMC_SENSOR_FARFIELD_FLUENCE) ? 0.0 : S.z;
+    if (S.kind == LMC_SENSOR_PLANAR_FIELD && !d.estimator)
+      sc.need_phase = 1;
+    int g = -1;
+    for (size_t k = 0; k < planes.size(); ++k)
+      if (!(planes[k] < z - 1e-9) && !(z < planes[k] - 1e-9))
+        g = (int)k;
+    if (g < 0) {
+      planes.push_back(z);
+      g = (int)planes.size() - 1;
+    }
+    d.plane = g;
+    d.tally_off = off;
+    h->sensor_off[i] = off;
+    h->sensor_count[i] = count;
+    off += count;
+  }
+  // sort planes ascending and remap (record_hit walks the map in key order)
+  std::vector<int> order(planes.size());
+  for (size_t k = 0; k < planes.size(); ++k)
+    order[k] = (int)k;
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return planes[a] < planes[b]; });
+  std::vector<int> rank(planes.size());
+  for (size_t k = 0; k < order.size(); ++k) {
+    rank[order[k]] = (int)k;
+    sc.plane_z[k] = planes[order[k]];
+    sc.plane_z_f[k] = (float)planes[order[k]];
+  }
+  for (int i = 0; i < s->n_sensors; ++i)
+    sc.sensors[i].plane = rank[sc.sensors[i].plane];
+  sc.n_planes = (int)planes.size();
+  h->n_sensors = s->n_sensors;
+  h->tally_doubles = off;
+  // A photon below z = 0 has left the sample, so a plane at z <= 0 is crossed at
+  // most once per photon: hits fit a queue of (photons x planes) entries and are
+  // tallied by a second kernel.  Planes inside the sample may be crossed any
+  // number of times; such scenes tally inside the transport kernel.
+  h->queued = sc.n_planes == 0 || sc.plane_z[sc.n_planes - 1] <= 0.0;
+  for (int i = 0; i < s->n_sensors; ++i)
+    if (s->sensors[i].kind == LMC_SENSOR_FARFIELD_CBS)
+      h->cbs_mask |= 1u << i;
+
+  // table arena: per medium double/float theta tables, guide tables, amplitudes
+  struct Span { size_t off, bytes; };
+  std::vector<unsigned char> arena;
+  auto put = [&](const void *src, size_t bytes) -> size_t {
+    const size_t o = (arena.size() + 255) & ~size_t(255);
+    arena.resize(o + bytes);
+    std::memcpy(arena.data() + o, src, bytes);
+    return o;
+  };
+  struct MedOff { size_t tvd, tcd, tcs, gd, ad, af; };
+  std::vector<MedOff> mo(s->n_media);
+  for (int i = 0; i < s->n_media; ++i) {
+    const lmc_medium_desc &M = s->media[i];
+    dev::Medium &d = sc.media[i];
+    d.theta_kind = M.theta_kind;
+    d.hg_g = M.hg_g;
+    d.hg_g_f = (float)M.hg_g;
+    d.mu_t = M.mu_a + M.mu_s;                               // src/medium.cpp:61-71
+    d.mfp = M.mean_free_path;
+    d.albedo = d.mu_t > 0 ? M.mu_s / d.mu_t : 1.0;          // src/simulation.cpp:580-587
+    d.mu_t_f = (float)d.mu_t;
+    d.mfp_f = (float)d.mfp;
+    d.albedo_f = (float)d.albedo;
+    d.amp_n = M.amp_n;
+    d.amp_inv_dx = 1.0 / M.amp_dtheta;
+    d.amp_inv_dx_f = (float)d.amp_inv_dx;
+    MedOff &o = mo[i];
+    o = MedOff{0, 0, 0, 0, 0, 0};
+    if (M.theta_kind == LMC_THETA_TABLE || M.theta_kind == LMC_THETA_TABLE_COS) {
+      const int n = M.theta_n;
+      d.theta_n = n;
+      std::vector<double> vd(M.theta_values, M.theta_values + n), cd(M.theta_cdf, M.theta_cdf + n);
+      std::vector<double2> cs(n);
+      for (int k = 0; k < n; ++k) {
+        const double dc = k ? cd[k] - cd[k - 1] : 0.0;
+        cs[k] = make_double2(cd[k], dc > 0.0 ? (vd[k] - vd[k - 1]) / dc : 0.0);
+      }
+      std::vector<int> gd(dev::kGuideBuckets + 1);
+      for (int j = 0; j <= dev::kGuideBuckets; ++j)
+        gd[j] = std::min(lower_bound_idx(cd, (double)j / dev::kGuideBuckets), n - 1);
+      o.tvd = put(vd.data(), n * sizeof(double));
+      o.tcd = put(cd.data(), n * sizeof(double));
+      o.tcs = put(cs.data(), n * sizeof(double2));
+      o.gd = put(gd.data(), gd.size() * sizeof(int));
+    }
+    std::vector<double4> ad(M.amp_n);
+    std::vector<float4> af(M.amp_n);
+    for (int k = 0; k < M.amp_n; ++k) {
+      ad[k] = make_double4(M.amp_s1[2 * k], M.amp_s1[2 * k + 1], M.amp_s2[2 * k], M.amp_s2[2 * k + 1]);
+      af[k] = make_float4((float)ad[k].x, (float)ad[k].y, (float)ad[k].z, (float)ad[k].w);
+    }
+    o.ad = put(ad.data(), ad.size() * sizeof(double4));
+    o.af = put(af.data(), af.size() * sizeof(float4));
+  }
+  h->arena_bytes = arena.size();
+  cudaError_t e = cudaMalloc(&h->d_arena, std::max<size_t>(h->arena_bytes, 256));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(h->d_arena, arena.data(), arena.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMalloc(&h->d_scene, sizeof(dev::Scene));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&h->d_scratch, sizeof(dev::Scratch));
+  if (e == cudaSuccess)
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&h->ev0);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&h->ev1);
+  if (e != cudaSuccess) {
+    lmc_destroy(h);
+    return fail(LMC_ERR_CUDA, std::string("lmc_create: ") + cudaGetErrorString(e));
+  }
+  unsigned char *base = static_cast<unsigned char *>(h->d_arena);
+  for (int i = 0; i < s->n_media; ++i) {
+    dev::Medium &d = sc.media[i];
+    const MedOff &o = mo[i];
+    if (d.theta_n) {
+      d.th_val_d = reinterpret_cast<const double *>(base + o.tvd);
+      d.th_cdf_d = reinterpret_cast<const double *>(base + o.tcd);
+      d.th_cs = reinterpret_cast<const double2 *>(base + o.tcs);
+      d.guide_d = reinterpret_cast<const int *>(base + o.gd);
+    }
+    d.amp_d = reinterpret_cast<const double4 *>(base + o.ad);
+    d.amp_f = reinterpret_cast<const float4 *>(base + o.af);
+  }
+  e = cudaMemcpy(h->d_scene, &sc, sizeof(sc), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    lmc_destroy(h);
+    return fail(LMC_ERR_CUDA, std::string("lmc_create: ") + cudaGetErrorString(e));
+  }
+  *out = h;
+  return LMC_OK;
+}
+
+void lmc_destroy(lmc_handle *h)
+{
+  if (!h)
+    return;
+  if (h->stream)
+    cudaStreamSynchronize(h->stream);
+  cudaFree(h->d_arena);
+  cudaFree(h->d_scene);
+  cudaFree(h->d_scratch);
+  cudaFree(h->d_host_tally);
+  cudaFree(h->d_queue);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+lmc_status lmc_tally_layout(const lmc_handle *h, int sensor, size_t *offset, size_t *count, int dims[4])
+{
+  if (!h)
+    return fail(LMC_ERR_INVALID, "handle must not be null");
+  if (sensor == -1) {
+    if (offset) *offset = 0;
+    if (count) *count = h->tally_doubles;
+    return LMC_OK;
+  }
+  if (sensor < 0 || sensor >= h->n_sensors)
+    return fail(LMC_ERR_INVALID, "sensor index out of range");
+  if (offset) *offset = h->sensor_off[sensor];
+  if (count) *count = h->sensor_count[sensor];
+  if (dims)
+    for (int k = 0; k < 4; ++k)
+      dims[k] = h->sensor_dims[sensor][k];
+  return LMC_OK;
+}
+
+lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
+                   const lmc_run_opts *opts, double *d_tallies, lmc_stats *stats)
+{
+  using namespace lmc;
+  if (!h || !opts)
+    return fail(LMC_ERR_INVALID, "handle and options must not be null");
+  if (h->tally_doubles && !d_tallies)
+    return fail(LMC_ERR_INVALID, "device tally buffer must not be null");
+  if (opts->precision != LMC_PRECISION_FP32 && opts->precision != LMC_PRECISION_FP64)
+    return fail(LMC_ERR_INVALID, "unknown precision");
+  if (opts->max_events < 0)
+    return fail(LMC_ERR_INVALID, "max_events must be non-negative");
+  for (int i = 0; i < h->scene.n_sensors; ++i)
+    if (h->scene.sensors[i].kind == LMC_SENSOR_FARFIELD_CBS && !opts->track_reverse_paths)
+      return fail(LMC_ERR_INVALID, "FarFieldCBSSensor needs track_reverse_paths (the reference "
+                                   "dereferences null species pointers without it)");
+  LMC_CUDA(cudaSetDevice(h->device));
+  cudaStream_t stream = opts->stream ? static_cast<cudaStream_t>(opts->stream) : h->stream;
+  LMC_CUDA(cudaMemsetAsync(h->d_scratch, 0, sizeof(dev::Scratch), stream));
+  dev::RunParams rp;
+  std::memset(&rp, 0, sizeof(rp));
+  rp.key0 = (uint32_t)seed;
+  rp.key1 = (uint32_t)(seed >> 32);
+  rp.max_events = opts->max_events;
+  rp.track_reverse = opts->track_reverse_paths ? 1 : 0;
+  rp.tallies = d_tallies;
+  rp.records = static_cast<lmc_record *>(opts->records);
+  rp.scratch = h->d_scratch;
+  rp.cbs_mask = h->cbs_mask;
+  const bool fp32 = opts->precision == LMC_PRECISION_FP32;
+  const int block = opts->block_size > 0 ? opts->block_size : dev::kBlock;
+  if (block % 32 != 0 || block > dev::kBlock)
+    return fail(LMC_ERR_INVALID, "block_size must be a multiple of 32 and at most 256");
+  const void *tk = fp32 ? (h->queued ? (const void *)dev::transport_kernel<float, true>
+                                     : (const void *)dev::transport_kernel<float, false>)
+                        : (h->queued ? (const void *)dev::transport_kernel<double, true>
+                                     : (const void *)dev::transport_kernel<double, false>);
+  int per_sm = 0;
+  LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tk, block, 0));
+  if (opts->blocks_per_sm > 0)
+    per_sm = std::min(per_sm, opts->blocks_per_sm);
+  per_sm = std::max(per_sm, 1);
+
+  // batches: the whole range at once inline; queue-sized batches when queued
+  unsigned long long batch = n_photons;
+  if (h->queued && n_photons > 0) {
+    batch = opts->batch_photons ? opts->batch_photons : (8ull << 20);
+    batch = std::min<unsigned long long>(batch, n_photons);
+    const unsigned long long planes = std::max(1, h->scene.n_planes);
+    const unsigned long long cap = batch * planes + batch / 16 + 1024;
+    const size_t rbytes = fp32 ? sizeof(float) : sizeof(double);
+    const size_t need = (size_t)cap * (dev::kQU32Fields * 4 + dev::kQF64Fields * 8 +
+                                       dev::kQRFields * rbytes) + 3 * 256;
+    if (h->queue_bytes < need) {
+      cudaFree(h->d_queue);
+      h->d_queue = nullptr;
+      h->queue_bytes = 0;
+      const cudaError_t e = cudaMalloc(&h->d_queue, need);
+      if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? LMC_ERR_NOMEM : LMC_ERR_CUDA,
+                    std::string("hit queue allocation: ") + cudaGetErrorString(e));
+      h->queue_bytes = need;
+    }
+    unsigned char *q = static_cast<unsigned char *>(h->d_queue);
+    auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+    rp.queue.cap = cap;
+    rp.queue.u32 = reinterpret_cast<uint32_t *>(q);
+    size_t o = align((size_t)cap * dev::kQU32Fields * 4);
+    rp.queue.f64 = reinterpret_cast<double *>(q + o);
+    o += align((size_t)cap * dev::kQF64Fields * 8);
+    rp.queue.r = q + o;
+  }
+  LMC_CUDA(cudaEventRecord(h->ev0, stream));
+  for (unsigned long long done = 0; done < n_photons; done += batch) {
+    const unsigned long long nb = std::min(batch, n_photons - done);
+    rp.photon_begin = photon_begin + done;
+    rp.n_photons = nb;
+    // reset the work counter and the queue fill of this batch
+    LMC_CUDA(cudaMemsetAsync(h->d_scratch, 0, 2 * sizeof(unsigned long long), stream));
+    const int grid = (int)std::max<unsigned long long>(
+        1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * per_sm,
+                                           (nb + block - 1) / block));
+    if (fp32) {
+      if (h->queued)
+        dev::transport_kernel<float, true><<<grid, block, 0, stream>>>(h->d_scene, rp);
+      else
+        dev::transport_kernel<float, false><<<grid, block, 0, stream>>>(h->d_scene, rp);
+    } else {
+      if (h->queued)
+        dev::transport_kernel<double, true><<<grid, block, 0, stream>>>(h->d_scene, rp);
+      else
+        dev::transport_kernel<double, false><<<grid, block, 0, stream>>>(h->d_scene, rp);
+    }
+    LMC_CUDA(cudaGetLastError());
+    if (h->queued && h->scene.n_sensors > 0) {
+      const int tgrid = (int)std::max<unsigned long long>(
+          1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * 8,
+                                             (rp.queue.cap + dev::kBlock - 1) / dev::kBlock));
+      if (fp32)
+        dev::tally_kernel<float><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
+      else
+        dev::tally_kernel<double><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
+      LMC_CUDA(cudaGetLastError());
+    }
+  }
+  LMC_CUDA(cudaEventRecord(h->ev1, stream));
+  if (stats) {
+    dev::Scratch sc;
+    LMC_CUDA(cudaMemcpyAsync(&sc, h->d_scratch, sizeof(sc), cudaMemcpyDeviceToHost, stream));
+    LMC_CUDA(cudaStreamSynchronize(stream));
+    std::memset(stats, 0, sizeof(*stats));
+    stats->photons = sc.photons; stats->events = sc.events; stats->steps = sc.steps;
+    stats->detected = sc.detected; stats->escaped = sc.escaped; stats->stack = sc.stack;
+    stats->roulette = sc.roulette; stats->cap = sc.cap; stats->draws = sc.draws;
+    for (int i = 0; i < LMC_MAX_SENSORS; ++i)
+      stats->hits[i] = sc.hits[i];
+    stats->error_flags = sc.error_flags;
+    float ms = 0.f;
+    LMC_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    stats->kernel_ms = ms;
+    if (sc.error_flags)
+      return fail(LMC_ERR_KERNEL, "transport kernel raised error flags " + std::to_string(sc.error_flags));
+  }
+  return LMC_OK;
+}
+
+lmc_status lmc_run_host(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
+                        const lmc_run_opts *opts, double *h_tallies, lmc_stats *stats)
+{
+  using namespace lmc;
+  if (!h)
+    return fail(LMC_ERR_INVALID, "handle must not be null");
+  if (h->tally_doubles && !h_tallies)
+    return fail(LMC_ERR_INVALID, "host tally buffer must not be null");
+  LMC_CUDA(cudaSetDevice(h->device));
+  const size_t bytes = h->tally_doubles * sizeof(double);
+  if (h->host_tally_cap < bytes) {
+    cudaFree(h->d_host_tally);
+  cudaFree(h->d_queue);
+    h->d_host_tally = nullptr;
+    h->host_tally_cap = 0;
+    LMC_CUDA(cudaMalloc(&h->d_host_tally, std::max<size_t>(bytes, 8)));
+    h->host_tally_cap = bytes;
+  }
+  cudaStream_t stream = opts && opts->stream ? static_cast<cudaStream_t>(opts->stream) : h->stream;
+  if (bytes)
+    LMC_CUDA(cudaMemcpyAsync(h->d_host_tally, h_tallies, bytes, cudaMemcpyHostToDevice, stream));
+  lmc_stats local;
+  const lmc_status st = lmc_run(h, seed, photon_begin, n_photons, opts, h->d_host_tally,
+                                stats ? stats : &local);
+  if (st != LMC_OK)
+    return st;
+  if (bytes)
+    LMC_CUDA(cudaMemcpyAsync(h_tallies, h->d_host_tally, bytes, cudaMemcpyDeviceToHost, stream));
+  LMC_CUDA(cudaStreamSynchronize(stream));
+  return LMC_OK;
+}
+
+}  // extern "C"

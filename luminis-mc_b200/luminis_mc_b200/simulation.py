@@ -1,0 +1,343 @@
+"""run_simulation_parallel on the GPU, and the reference's post-processing.
+
+``run_simulation_parallel(config)`` keeps the reference's contract
+(python/python_module.cpp:664-673, src/simulation.cpp:105-249): it blocks, it
+ADDS each sensor's contribution into the sensor objects owned by
+``config.detector`` and increments their ``hits``, and it raises ValueError for
+a config without sample, laser or detector.  The work runs in one CUDA kernel
+through the C ABI (include/luminis_b200.h); there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import random
+
+import numpy as np
+
+from . import _native as N
+from .core import (FarFieldCBSSensor, FarFieldFluenceSensor, HenyeyGreensteinPhaseFunction,
+                   Matrix, PlanarFieldSensor, PlanarFluenceSensor, UniformPhaseFunction,
+                   _TablePhase, solid_angle_bin)  # noqa: F401
+
+
+class SimConfig:
+    """Run configuration (include/luminis/core/simulation.hpp:67-90)."""
+
+    def __init__(self):
+        self.MAX_EVENTS = 1000
+        self.batch_size = 0
+        self.show_progress = True
+        self.progress_interval_pct = 5
+        self.seed = random.getrandbits(32)
+        self.n_threads = 1
+        self.n_photons = 0
+        self.pin_threads_to_cores = False
+        self.track_reverse_paths = False
+        self.sample = None
+        self.laser = None
+        self.detector = None
+        self.absorption = None
+
+
+_last_stats: dict = {}
+
+
+def last_run_stats() -> dict:
+    """Counters of the most recent run: photons, events, steps (free flights),
+    fates, draws, per-sensor hits, kernel_ms."""
+    return dict(_last_stats)
+
+
+def validate_sim_config(config: SimConfig) -> None:
+    """src/simulation.cpp:95-103."""
+    if config.sample is None:
+        raise ValueError("SimConfig::sample must not be null")
+    if config.laser is None:
+        raise ValueError("SimConfig::laser must not be null")
+    if config.detector is None:
+        raise ValueError("SimConfig::detector must not be null")
+
+
+def _medium_desc(d: N.MediumDesc, medium, keep: list) -> None:
+    ph = medium.phase_function
+    if ph is None:
+        raise ValueError("ScatteringMedium: Phase function is not defined!")
+    if isinstance(ph, HenyeyGreensteinPhaseFunction):
+        d.theta_kind = N.THETA_HG
+        d.hg_g = ph.g
+    elif isinstance(ph, UniformPhaseFunction):
+        d.theta_kind = N.THETA_UNIFORM
+    elif isinstance(ph, _TablePhase):
+        d.theta_kind = N.THETA_TABLE if ph._samples_theta else N.THETA_TABLE_COS
+        values, cdf = ph._table()
+        keep += [values, cdf]
+        d.theta_n = values.size
+        d.theta_values = N.as_dptr(values)
+        d.theta_cdf = N.as_dptr(cdf)
+    else:
+        raise NotImplementedError(f"phase function {type(ph).__name__} has no GPU sampler")
+    s1 = np.ascontiguousarray(medium._s1).view(np.float64)
+    s2 = np.ascontiguousarray(medium._s2).view(np.float64)
+    keep += [s1, s2]
+    d.amp_n = medium._s1.size
+    d.amp_dtheta = medium._dtheta
+    d.amp_s1 = N.as_dptr(s1)
+    d.amp_s2 = N.as_dptr(s2)
+    d.mu_a = medium.mu_a
+    d.mu_s = medium.mu_s
+    d.mean_free_path = medium.mean_free_path
+
+
+def _sensor_desc(d: N.SensorDesc, s) -> None:
+    d.kind = s._kind
+    d.z = s.origin.z
+    d.absorb = int(s.absorb_photons)
+    d.estimator = int(s.estimator_enabled)
+    d.f_theta = int(s.filter_theta_enabled)
+    d.theta_min, d.theta_max = s.filter_theta_min, s.filter_theta_max
+    d.f_phi = int(s.filter_phi_enabled)
+    d.phi_min, d.phi_max = s.filter_phi_min, s.filter_phi_max
+    d.f_pos = int(s.filter_position_enabled)
+    d.x_min, d.x_max, d.y_min, d.y_max = (s.filter_x_min, s.filter_x_max, s.filter_y_min,
+                                          s.filter_y_max)
+    d.f_dir = int(s.filter_direction_enabled)
+    d.direction = int(s.filter_direction)
+    d.f_events = int(s.filter_events_enabled)
+    d.events_min, d.events_max = s.filter_events_min, s.filter_events_max
+    if isinstance(s, (FarFieldCBSSensor, FarFieldFluenceSensor)):
+        d.theta_max_grid, d.phi_max_grid = s.theta_max, s.phi_max
+        d.dtheta, d.dphi = s.dtheta, s.dphi
+        d.len_t, d.dt = s.t_max, s.dt
+        if isinstance(s, FarFieldCBSSensor) and s.phi_explicit:
+            d.phi_max_grid = s.N_phi * s.dphi       # the explicit slices set the column count
+    elif isinstance(s, PlanarFluenceSensor):
+        d.len_x, d.len_y, d.len_t = s.len_x, s.len_y, s.len_t
+        d.dx, d.dy, d.dt = s.dx, s.dy, s.dt
+    else:
+        d.len_x, d.len_y, d.dx, d.dy = s.len_x, s.len_y, s.dx, s.dy
+
+
+def scene_desc(config: SimConfig):
+    """Pack the config's Sample / Laser / SensorsGroup into the C scene.
+    Returns (scene, keep-alive list, gpu sensors)."""
+    validate_sim_config(config)
+    if config.absorption is not None:
+        raise NotImplementedError("the Absorption recorder is not supported by the GPU transport")
+    sample, laser, group = config.sample, config.laser, config.detector
+    sc = N.SceneDesc()
+    keep: list = []
+    sc.n_host = sample.refractive_index
+    media: list = []
+    if len(sample.layers) > N.MAX_LAYERS:
+        raise ValueError(f"at most {N.MAX_LAYERS} layers")
+    for i, layer in enumerate(sample.layers):
+        m = layer.medium
+        idx = next((k for k, x in enumerate(media) if x is m), None)
+        if idx is None:
+            if len(media) == N.MAX_MEDIA:
+                raise ValueError(f"at most {N.MAX_MEDIA} distinct media")
+            idx = len(media)
+            media.append(m)
+            _medium_desc(sc.media[idx], m, keep)
+        sc.layers[i].z_min = layer.z_min
+        sc.layers[i].z_max = layer.z_max
+        sc.layers[i].medium = idx
+    sc.n_layers = len(sample.layers)
+    sc.n_media = len(media)
+    L = sc.laser
+    for dst, v in ((L.position, laser.position), (L.direction, laser.direction),
+                   (L.local_m, laser.local_m), (L.local_n, laser.local_n)):
+        dst[0], dst[1], dst[2] = v.x, v.y, v.z
+    pm, pn = laser.polarization.m, laser.polarization.n
+    L.jones[0], L.jones[1], L.jones[2], L.jones[3] = pm.real, pm.imag, pn.real, pn.imag
+    L.wavelength = laser.wavelength
+    L.sigma = laser.sigma
+    L.source = int(laser.source_type)
+    L.temporal = int(laser.temporal_profile)
+    L.pulse_duration = laser.pulse_duration
+    L.repetition_rate = laser.repetition_rate
+    L.time_offset = laser.time_offset
+    sensors = list(group.detectors)
+    for s in sensors:
+        if not s._gpu:
+            raise NotImplementedError(f"{type(s).__name__} is not supported by the GPU transport")
+    if len(sensors) > N.MAX_SENSORS:
+        raise ValueError(f"at most {N.MAX_SENSORS} sensors")
+    for i, s in enumerate(sensors):
+        _sensor_desc(sc.sensors[i], s)
+    sc.n_sensors = len(sensors)
+    return sc, keep, sensors
+
+
+class Transport:
+    """A created scene (lmc_create) that can run many photon ranges.
+
+    ``run_simulation_parallel`` uses one per call; benchmarks and tests keep one
+    to run repeatedly (tallies stay on the device between ``run_device`` calls).
+    """
+
+    def __init__(self, config: SimConfig):
+        self.config = config
+        self.scene, self._keep, self.sensors = scene_desc(config)
+        h = C.c_void_p()
+        N.check(N.lib().lmc_create(C.byref(self.scene), C.byref(h)))
+        self._h = h
+        total = C.c_size_t()
+        N.check(N.lib().lmc_tally_layout(self._h, -1, None, C.byref(total), None))
+        self.tally_size = int(total.value)
+        self.layout = []
+        for i in range(len(self.sensors)):
+            off, cnt = C.c_size_t(), C.c_size_t()
+            dims = (C.c_int * 4)()
+            N.check(N.lib().lmc_tally_layout(self._h, i, C.byref(off), C.byref(cnt), dims))
+            self.layout.append((int(off.value), int(cnt.value), tuple(dims)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().lmc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def opts(self, precision="fp32", max_events=None, track_reverse_paths=None, block_size=0,
+             blocks_per_sm=0, records_ptr=None, stream=None, batch_photons=0) -> N.RunOpts:
+        if precision not in N.PRECISION:
+            raise ValueError("precision must be 'fp32' or 'fp64'")
+        c = self.config
+        o = N.RunOpts()
+        o.precision = N.PRECISION[precision]
+        o.max_events = int(c.MAX_EVENTS if max_events is None else max_events)
+        o.track_reverse_paths = int(bool(c.track_reverse_paths if track_reverse_paths is None
+                                         else track_reverse_paths))
+        o.block_size = int(block_size)
+        o.blocks_per_sm = int(blocks_per_sm)
+        o.records = records_ptr
+        o.stream = stream
+        o.batch_photons = int(batch_photons)
+        return o
+
+    def run_host(self, tallies: np.ndarray, n_photons: int, seed: int, begin: int = 0,
+                 **kw) -> dict:
+        """lmc_run_host: tallies is a float64 host array of tally_size, accumulated."""
+        assert tallies.dtype == np.float64 and tallies.size == self.tally_size
+        st = N.Stats()
+        o = self.opts(**kw)
+        N.check(N.lib().lmc_run_host(self._h, int(seed) & (2 ** 64 - 1), int(begin),
+                                     int(n_photons), C.byref(o), N.as_dptr(tallies),
+                                     C.byref(st)))
+        return st.as_dict()
+
+    def run_device(self, d_tallies_ptr: int, n_photons: int, seed: int, begin: int = 0,
+                   want_stats: bool = True, **kw) -> dict:
+        """lmc_run on a caller-owned device buffer (e.g. a torch tensor's data_ptr())."""
+        st = N.Stats()
+        o = self.opts(**kw)
+        N.check(N.lib().lmc_run(self._h, int(seed) & (2 ** 64 - 1), int(begin), int(n_photons),
+                                C.byref(o), C.c_void_p(d_tallies_ptr),
+                                C.byref(st) if want_stats else None))
+        return st.as_dict() if want_stats else {}
+
+    def split(self, tallies: np.ndarray):
+        """Per-sensor views of a flat tally buffer, in the sensor layouts."""
+        return [tallies[o:o + c].reshape(d) for (o, c, d) in self.layout]
+
+
+def run_simulation_parallel(config: SimConfig, *, precision: str = "fp32", block_size: int = 0,
+                            blocks_per_sm: int = 0) -> None:
+    """GPU drop-in for luminis_mc.run_simulation_parallel(config).
+
+    Photon i draws the Philox stream (config.seed, i), so results do not depend
+    on the launch shape (as the reference's do not depend on n_threads).
+    ``n_threads``, ``batch_size``, ``pin_threads_to_cores`` and ``show_progress``
+    are accepted and ignored.
+    """
+    global _last_stats
+    validate_sim_config(config)
+    t = Transport(config)
+    try:
+        flat = np.zeros(t.tally_size)
+        stats = t.run_host(flat, int(config.n_photons), int(config.seed), 0,
+                           precision=precision, block_size=block_size,
+                           blocks_per_sm=blocks_per_sm)
+        for i, (s, (off, cnt, _)) in enumerate(zip(t.sensors, t.layout)):
+            s._tally += flat[off:off + cnt]
+            s.hits += stats["hits"][i]
+        _last_stats = stats
+    finally:
+        t.close()
+
+
+# --------------------------------------------------------------------- post-processing
+class StokesMatrixProcessed:
+    def __init__(self, S0, S1, S2, S3):
+        self.S0, self.S1, self.S2, self.S3 = S0, S1, S2, S3
+
+
+class FarFieldCBSProcessed:
+    def __init__(self, dOmega, coherent, incoherent):
+        self.dOmega, self.coherent, self.incoherent = dOmega, coherent, incoherent
+
+
+class PlanarFluenceProcessed:
+    def __init__(self, S0, S1, S2, S3):
+        self.S0, self.S1, self.S2, self.S3 = S0, S1, S2, S3
+
+
+class PlanarFieldProcessed:
+    def __init__(self, Ex, Ey):
+        self.Ex, self.Ey = Ex, Ey
+
+
+def postprocess_farfield_cbs(det, n_photons, normalize_per_solid_angle=True,
+                             normalize_per_photon=True, eps=1e-30) -> FarFieldCBSProcessed:
+    """Divide by N and by the theta band's solid angle (src/results.cpp:61-101)."""
+    a = det._tally.reshape(det._shape())
+    invN = 1.0 / float(n_photons) if (normalize_per_photon and n_photons > 0) else 1.0
+    dOm = np.array([solid_angle_bin(i, det.dtheta, det.dphi) if normalize_per_solid_angle else 1.0
+                    for i in range(det.N_theta)])
+    invOm = np.where(dOm > eps, 1.0 / np.where(dOm > eps, dOm, 1.0), 0.0)
+    norm = (invN * invOm)[:, None]
+    dOmega = np.repeat(dOm[:, None], det.N_phi, axis=1).view(Matrix)
+    coh, inc = [], []
+    for t in range(det.N_t):
+        coh.append(StokesMatrixProcessed(*[(a[q, t] * norm).view(Matrix) for q in range(4)]))
+        inc.append(StokesMatrixProcessed(*[(a[4 + q, t] * norm).view(Matrix) for q in range(4)]))
+    return FarFieldCBSProcessed(dOmega, coh, inc)
+
+
+def postprocess_farfield_fluence(det, n_photons, normalize_per_solid_angle=True,
+                                 normalize_per_photon=True, eps=1e-30) -> list:
+    """Per time bin StokesMatrixProcessed, normalised like postprocess_farfield_cbs."""
+    a = det._tally.reshape(det._shape())
+    invN = 1.0 / float(n_photons) if (normalize_per_photon and n_photons > 0) else 1.0
+    dOm = np.array([solid_angle_bin(i, det.dtheta, det.dphi) if normalize_per_solid_angle else 1.0
+                    for i in range(det.N_theta)])
+    invOm = np.where(dOm > eps, 1.0 / np.where(dOm > eps, dOm, 1.0), 0.0)
+    norm = (invN * invOm)[:, None]
+    return [StokesMatrixProcessed(*[(a[q, t] * norm).view(Matrix) for q in range(4)])
+            for t in range(det.N_t)]
+
+
+def postprocess_planar_fluence(det, n_photons, normalize_per_photon=True, normalize_per_area=True,
+                               eps=1e-30) -> PlanarFluenceProcessed:
+    """src/results.cpp:5-35."""
+    a = det._tally.reshape(det._shape())
+    invN = 1.0 / float(n_photons) if (normalize_per_photon and n_photons > 0) else 1.0
+    area = det.dx * det.dy
+    norm = invN * ((1.0 / area) if (normalize_per_area and area > eps) else 1.0)
+    return PlanarFluenceProcessed(*[[(a[q, t] * norm).view(Matrix) for t in range(det.N_t)]
+                                    for q in range(4)])
+
+
+def postprocess_planar_field(det, n_photons, normalize_per_photon=True, normalize_per_area=True,
+                             eps=1e-30) -> PlanarFieldProcessed:
+    """src/results.cpp:37-58."""
+    invN = 1.0 / float(n_photons) if (normalize_per_photon and n_photons > 0) else 1.0
+    area = det.dx * det.dy
+    norm = invN * ((1.0 / area) if (normalize_per_area and area > eps) else 1.0)
+    return PlanarFieldProcessed(np.asarray(det.Ex) * norm, np.asarray(det.Ey) * norm)

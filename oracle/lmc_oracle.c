@@ -1366,3 +1366,13 @@ double lmc_oracle_phase_sample_theta(const lmc_o_handle *h, int medium, double u
 {
   return ophase_sample_theta(&h->phase[h->media[medium].phase], u);
 }
+
+void lmc_oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+  lmc_ref_philox4x32_10(ctr, key, out);
+}
+
+double lmc_oracle_stream_uniform(uint64_t seed, uint64_t photon, uint64_t draw, int format)
+{
+  return lmc_ref_stream_uniform(seed, photon, draw, format);
+}

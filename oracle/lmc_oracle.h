@@ -159,6 +159,10 @@ int lmc_oracle_amp_table(const lmc_o_handle *h, int medium, int *n, double *dthe
                          const double **s1, const double **s2);
 double lmc_oracle_phase_sample_theta(const lmc_o_handle *h, int medium, double u);
 
+/* The Philox4x32-10 block function and the stream contract (oracle/philox_ref.h). */
+void lmc_oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+double lmc_oracle_stream_uniform(uint64_t seed, uint64_t photon, uint64_t draw, int format);
+
 /* MIEV0 restatement helpers (oracle/miev0.c). */
 int lmc_oracle_miev0_selftest(double *worst_rel_err);
 void lmc_oracle_mie(double x, double m_re, double m_im, int n, const double *mu, double *s1,

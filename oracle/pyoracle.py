@@ -126,6 +126,10 @@ def lib():
                                            C.POINTER(C.POINTER(C.c_double))]
         L.lmc_oracle_phase_sample_theta.restype = C.c_double
         L.lmc_oracle_phase_sample_theta.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.lmc_oracle_philox.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                        C.POINTER(C.c_uint32)]
+        L.lmc_oracle_stream_uniform.restype = C.c_double
+        L.lmc_oracle_stream_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_int]
         L.lmc_oracle_miev0_selftest.argtypes = [C.POINTER(C.c_double)]
         L.lmc_oracle_mie.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int,
                                      C.POINTER(C.c_double), C.POINTER(C.c_double),
@@ -311,6 +315,18 @@ class Oracle:
 
     def sample_theta(self, medium: int, u: float) -> float:
         return lib().lmc_oracle_phase_sample_theta(self._h, medium, float(u))
+
+
+def philox(ctr, key):
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib().lmc_oracle_philox(c, k, o)
+    return tuple(o)
+
+
+def stream_uniform(seed: int, photon: int, draw: int, fmt: str = "u53") -> float:
+    return lib().lmc_oracle_stream_uniform(seed, photon, draw, 0 if fmt == "u53" else 1)
 
 
 def miev0_selftest() -> tuple[bool, float]:

@@ -1,0 +1,101 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Runs the reference's own Python API (its pybind module built from its sources by
+oracle/Makefile into oracle/_ref) on small scenes and stores every sensor's
+tallies and hit counts:
+
+  ref_xoshiro_<scene>.npz  the unmodified reference, its own RNG, n_threads=1
+                           ("pin" build: -O2 -ffp-contract=off)
+  ref_philox_<scene>.npz   the reference with the Philox replay seam
+                           (oracle/replay_rng.cpp), the stream the GPU draws
+
+    python tests/golden/make_golden.py        (needs oracle/_ref; run `make -C oracle ref`)
+
+The fixtures pin the oracle (tests/test_oracle_golden.py) and the GPU path
+(tests/test_gpu_golden.py) without the reference present at test time.
+"""
+import ctypes
+import glob
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "luminis-mc_b200"))
+
+from luminis_mc_b200 import workloads as W  # noqa: E402
+
+
+def golden_scenes():
+    """Small scenes covering every sensor type the reference has, both media, HG,
+    interfaces, time bins, filters and circular/linear polarisation."""
+    a = W.mie_cbs_small(2000, 20240)
+    b = W.bilayer_rgd_mie(2000, 77)
+    b["name"] = "bilayer_small"
+    b["sensors"][1].update(len_x=4.0, len_y=4.0, dx=0.2, dy=0.2, len_t=15.0, d_t=1.0)
+    b["sensors"].pop(2)           # FarFieldFluence has no reference class
+    c = W.bilayer_hg(1500, 5)
+    c["name"] = "bilayer_hg_small"
+    c["sensors"][1].update(len_x=4.0, len_y=4.0, dx=0.25, dy=0.25, len_t=0.0, d_t=0.0)
+    c["sensors"].pop(2)
+    d = W.mie_long_paths(150, 9)
+    d["name"] = "mie_speckle_small"
+    d["max_events"] = 5000
+    d["sensors"][1].update(len_x=0.64, len_y=0.64, dx=0.02, dy=0.02)
+    return [a, b, c, d]
+
+
+def run_flavour(flavour, scene_name, fmt=None):
+    """Run one scene in a fresh interpreter (each reference flavour is a module
+    named luminis_mc) and return {sensor index: tally, 'hits': [...]}."""
+    code = f"""
+import sys, json, glob, ctypes, numpy as np
+sys.path.insert(0, {REPO!r}); sys.path.insert(0, {os.path.join(REPO, 'luminis-mc_b200')!r})
+from tests.golden.make_golden import golden_scenes
+from luminis_mc_b200 import workloads as W
+from oracle import pyoracle as O
+lm = O.reference_module({flavour!r}); lm.set_log_level(lm.LogLevel.off)
+if {fmt is not None!r}:
+    so = ctypes.CDLL(glob.glob({os.path.join(REPO, 'oracle', '_ref', flavour, 'luminis_mc', '_core*.so')!r})[0])
+    so.lmc_replay_set_format({fmt if fmt is not None else 0})
+spec = [s for s in golden_scenes() if s["name"] == {scene_name!r}][0]
+cfg, hs, keep = W.build(lm, spec, n_threads=1)
+lm.run_simulation_parallel(cfg)
+out = {{}}
+for i, (h, s) in enumerate(zip(hs, spec["sensors"])):
+    out[f"sensor{{i}}"] = W.tally_arrays(h, s["kind"])
+out["hits"] = np.array([h.hits for h in hs], dtype=np.int64)
+np.savez(sys.argv[1], **out)
+"""
+    tmp = os.path.join(HERE, f"_tmp_{flavour}_{scene_name}.npz")
+    subprocess.run([sys.executable, "-c", code, tmp], check=True)
+    data = dict(np.load(tmp))
+    os.unlink(tmp)
+    return data
+
+
+def main():
+    meta = {}
+    for spec in golden_scenes():
+        name = spec["name"]
+        np.savez_compressed(os.path.join(HERE, f"ref_xoshiro_{name}.npz"),
+                            **run_flavour("pin", name))
+        np.savez_compressed(os.path.join(HERE, f"ref_philox_{name}.npz"),
+                            **run_flavour("replay", name, fmt=0))
+        meta[name] = {"n_photons": spec["n_photons"], "seed": spec["seed"],
+                      "max_events": spec["max_events"],
+                      "sensors": [s["kind"] for s in spec["sensors"]]}
+    with open(os.path.join(HERE, "golden_meta.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py",
+                   "reference_builds": "oracle/_ref/pin (own RNG), oracle/_ref/replay (Philox u53)",
+                   "scenes": meta}, f, indent=1)
+    print("wrote", sorted(os.listdir(HERE)))
+
+
+if __name__ == "__main__":
+    main()

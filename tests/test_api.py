@@ -1,0 +1,139 @@
+"""The Python API mirrors the reference's (python/python_module.cpp): names,
+arguments, error behaviour, post-processing; checked on CPU."""
+import math
+
+import numpy as np
+import pytest
+
+import luminis_mc_b200 as lm
+from luminis_mc_b200 import workloads as W
+from luminis_mc_b200.simulation import Transport, scene_desc
+from oracle import pyoracle as O
+
+
+def reference():
+    try:
+        return O.reference_module("pin")
+    except ImportError as e:
+        pytest.skip(str(e))
+
+
+def test_run_rejects_missing_pointers_like_the_reference():
+    cfg = lm.SimConfig()
+    with pytest.raises(ValueError, match="sample"):
+        lm.run_simulation_parallel(cfg)
+    cfg2, _, keep = W.build(lm, W.mie_cbs_small(10, 1))
+    cfg2.laser = None
+    with pytest.raises(ValueError, match="laser"):
+        lm.run_simulation_parallel(cfg2)
+    cfg2, _, keep = W.build(lm, W.mie_cbs_small(10, 1))
+    cfg2.detector = None
+    with pytest.raises(ValueError, match="detector"):
+        lm.run_simulation_parallel(cfg2)
+
+
+def test_sample_validation_messages():
+    s = lm.Sample(1.33)
+    med = lm.MieMedium(lm.HenyeyGreensteinPhaseFunction(0.9), 0.5e-3, 1.59, 1.33, 0.633e-3)
+    with pytest.raises(ValueError, match="first layer must start at z = 0"):
+        s.add_layer(med, 0.1, 1.0)
+    s.add_layer(med, 0.0, 1.0)
+    with pytest.raises(ValueError, match="does not match previous"):
+        s.add_layer(med, 2.0, 3.0)
+    s.add_layer(med, 1.0, math.inf)
+    with pytest.raises(ValueError, match="infinite top layer"):
+        s.add_layer(med, 5.0, 6.0)
+    assert s.size() == 2 and s.interfaces == [1.0]
+    assert s.is_inside(lm.Vec3(0, 0, 5.0)) and not s.is_inside(lm.Vec3(0, 0, -1e-9))
+
+
+@pytest.mark.parametrize("extra", ["photon_record", "statistics", "absorption", "mixture"])
+def test_unsupported_parts_raise_before_any_launch(extra):
+    cfg, _, keep = W.build(lm, W.mie_cbs_small(10, 1))
+    if extra == "photon_record":
+        cfg.detector.add_detector(lm.PhotonRecordSensor(0.0))
+    elif extra == "statistics":
+        cfg.detector.add_detector(lm.StatisticsSensor(0.0))
+    elif extra == "absorption":
+        cfg.absorption = lm.Absorption(1.0, 1.0, 0.1, 0.1)
+    else:
+        with pytest.raises(NotImplementedError):
+            cfg.sample.add_mixture_layer([], [], 0.0, 1.0)
+        return
+    with pytest.raises(NotImplementedError):
+        scene_desc(cfg)
+
+
+@pytest.mark.parametrize("mutate,match", [
+    (lambda c: c.sample.layers[0].medium.set_mean_free_path(0.0), "mean_free_path"),
+    (lambda c: setattr(c.laser, "position", lm.Vec3(0, 0, -1.0)), "outside the sample"),
+    (lambda c: setattr(c.laser, "wavelength", 0.0), "wavelength"),
+])
+def test_library_validates_scenes_before_touching_a_gpu(mutate, match):
+    cfg, _, keep = W.build(lm, W.mie_cbs_small(10, 1))
+    mutate(cfg)
+    with pytest.raises(ValueError, match=match):
+        Transport(cfg)
+
+
+def test_hg_g_zero_is_rejected():
+    spec = W.bilayer_hg(10, 1)
+    spec["phases"][0]["g"] = 0.0
+    cfg, _, keep = W.build(lm, spec)
+    with pytest.raises(ValueError, match="Henyey-Greenstein"):
+        Transport(cfg)
+
+
+def test_sensor_shapes_and_filters_match_the_reference():
+    ref = reference()
+    spec = W.bilayer_rgd_mie(10, 1)
+    spec["sensors"] = spec["sensors"][:2] + [
+        {"kind": "planar_field", "z": 0.0, "len_x": 2.56, "len_y": 2.56, "dx": 0.01, "dy": 0.01}]
+    c1, h1, k1 = W.build(lm, spec)
+    c2, h2, k2 = W.build(ref, spec)
+    for a, b in zip(h1, h2):
+        for attr in ("N_theta", "N_phi", "N_t", "N_x", "N_y", "dtheta", "dphi", "dx", "dy", "dt",
+                     "filter_theta_enabled", "filter_position_enabled", "filter_x_min",
+                     "filter_x_max", "absorb_photons", "estimator_enabled", "id"):
+            if hasattr(b, attr):
+                assert getattr(a, attr) == getattr(b, attr), attr
+    assert np.array(h1[0].S0_coh[0]).shape == np.array(h2[0].S0_coh[0]).shape
+    assert len(h1[1].S0) == len(h2[1].S0)
+    assert np.array(h1[2].Ex).shape == np.array(h2[2].Ex).shape
+
+
+def test_postprocess_matches_the_reference_on_the_same_tallies():
+    ref = reference()
+    spec = W.bilayer_rgd_mie(10, 1)
+    spec["sensors"][1].update(len_x=2.0, len_y=2.0, dx=0.1, dy=0.1, len_t=7.0, d_t=1.0)
+    spec["sensors"] = spec["sensors"][:2]
+    c2, h2, k2 = W.build(ref, spec, n_photons=3000)
+    ref.run_simulation_parallel(c2)
+    c1, h1, k1 = W.build(lm, spec)
+    for a, b, s in zip(h1, h2, spec["sensors"]):
+        a._tally[:] = W.tally_arrays(b, s["kind"]).ravel()
+    p1 = lm.postprocess_farfield_cbs(h1[0], 3000)
+    p2 = ref.postprocess_farfield_cbs(h2[0], 3000)
+    np.testing.assert_allclose(np.array(p1.dOmega), np.array(p2.dOmega), rtol=1e-15)
+    for t in range(len(p2.coherent)):
+        for q in ("S0", "S1", "S2", "S3"):
+            np.testing.assert_allclose(np.array(getattr(p1.coherent[t], q)),
+                                       np.array(getattr(p2.coherent[t], q)), rtol=1e-14)
+            np.testing.assert_allclose(np.array(getattr(p1.incoherent[t], q)),
+                                       np.array(getattr(p2.incoherent[t], q)), rtol=1e-14)
+    f1 = lm.postprocess_planar_fluence(h1[1], 3000)
+    f2 = ref.postprocess_planar_fluence(h2[1], 3000)
+    for q in ("S0", "S1", "S2", "S3"):
+        for t in range(len(getattr(f2, q))):
+            np.testing.assert_allclose(np.array(getattr(f1, q)[t]), np.array(getattr(f2, q)[t]),
+                                       rtol=1e-14)
+
+
+def test_add_detector_clones_like_the_reference():
+    g = lm.SensorsGroup()
+    d = lm.FarFieldCBSSensor(0.1, 2 * math.pi, 0.0, 1e-3, 2 * math.pi, 0.0)
+    d.set_theta_limit(0.0, 0.1)
+    h = g.add_detector(d)
+    assert h is not d and h is g.detectors[0] and h.filter_theta_enabled
+    d.set_phi_limit(0.0, 1.0)
+    assert not h.filter_phi_enabled

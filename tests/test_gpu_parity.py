@@ -1,0 +1,164 @@
+"""GPU parity: the CUDA transport against the CPU oracle on the same Philox stream.
+
+(a) per-photon replay: every photon's final state (events, draws, fate, position,
+    direction, frame, Jones vector, weight, path length, reverse field at CBS
+    detection) from the GPU record buffer against the oracle's record;
+(b) tallies: every sensor bin against the oracle's tallies.
+FP64 transport must match to 1e-9 relative with all event counts exact; FP32
+transport (draws "u24") must agree on the discrete history (events, draws, fate)
+for at least 99.5 % of photons and, for those, on positions to 1e-5 of the path
+length, on directions and frames to 1e-5, on weights to 1e-12 (the weight is
+binary64 in both modes) and on Jones vectors to 2e-4 (the 1/sqrt(F)
+renormalisation amplifies rounding by up to ~1e3, as the FP64 comparison shows:
+1e-13 against 1e-16 ulps).
+"""
+import numpy as np
+import pytest
+
+import luminis_mc_b200 as lm
+from luminis_mc_b200 import workloads as W
+from luminis_mc_b200.device import DeviceRun
+from oracle import pyoracle as O
+
+pytestmark = pytest.mark.gpu
+
+FP64_RTOL = 1e-9
+# The speckle field sums exp(i k L) with k L ~ 1e6 rad over 100 mm paths, which
+# turns 1e-13 path differences (FMA contraction, libm ulps) into ~1e-7 rad.
+FP64_FIELD_RTOL = 1e-6
+FP32_RTOL = {"weight": 1e-12, "opticalpath": 1e-5, "dir": 1e-5, "m": 1e-5, "n": 1e-5,
+             "E": 2e-4, "Er": 2e-4}
+FP32_POS_OF_PATH = 1e-5       # positions: |difference| / path length
+FP32_MAX_DIVERGED = 0.005
+
+
+def small_specs():
+    yield W.mie_cbs_small(3000, 20240)
+    yield W.bilayer_rgd_mie(3000, 77)
+    yield W.bilayer_hg(3000, 5)
+    spec = W.mie_long_paths(300, 9)
+    spec["max_events"] = 20000
+    yield spec
+
+
+def _relerr(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = np.maximum(np.abs(b), 1.0)
+    return np.abs(a - b) / scale
+
+
+def _compare_records(gpu, ora, rtol):
+    """Indices of photons whose discrete history agrees, and the max relative
+    error of their continuous state."""
+    assert np.array_equal(gpu["photon"], ora["photon"])
+    same = ((gpu["events"] == ora["events"]) & (gpu["draws"] == ora["draws"]) &
+            (gpu["fate"] == ora["fate"]) & (gpu["n_hits"] == ora["n_hits"]))
+    worst = {}
+    for f in ("weight", "opticalpath", "pos", "dir", "m", "n", "E", "r1", "rn", "Er", "hit"):
+        e = _relerr(gpu[f][same], ora[f][same])
+        worst[f] = float(e.max()) if e.size else 0.0
+    return same, worst
+
+
+@pytest.mark.parametrize("spec", list(small_specs()), ids=lambda s: s["name"])
+def test_replay_fp64_exact(spec, cuda):
+    cfg, _, keep = W.build(lm, spec)
+    run = DeviceRun(cfg)
+    n = cfg.n_photons
+    stats, rec = run.run(n, cfg.seed, precision="fp64", records=True)
+    ref = O.Oracle(spec).run(n, cfg.seed, rng="philox_u53", records=True)
+    same, worst = _compare_records(rec, ref.records, FP64_RTOL)
+    assert same.all(), f"{(~same).sum()} photons differ in events/draws/fate"
+    for f, e in worst.items():
+        assert e < FP64_RTOL, f"{f}: {e}"
+    assert stats["events"] == ref.stats["events"]
+    assert stats["steps"] == ref.stats["steps"]
+    assert stats["draws"] == ref.stats["draws"]
+    for s_idx, (g, o) in enumerate(zip(run.host_tallies(), ref.tallies)):
+        # Stokes S1..S3 bins can cancel to ~0, so the floor scales with the sensor
+        tol = FP64_FIELD_RTOL if spec["sensors"][s_idx]["kind"] == "planar_field" else FP64_RTOL
+        np.testing.assert_allclose(g, o, rtol=tol, atol=tol * np.abs(o).max(),
+                                   err_msg=f"sensor {s_idx}")
+        assert stats["hits"][s_idx] == ref.hits[s_idx]
+    run.close()
+
+
+@pytest.mark.parametrize("spec", list(small_specs()), ids=lambda s: s["name"])
+def test_replay_fp32_tolerance(spec, cuda):
+    cfg, _, keep = W.build(lm, spec)
+    run = DeviceRun(cfg)
+    n = cfg.n_photons
+    stats, rec = run.run(n, cfg.seed, precision="fp32", records=True)
+    ref = O.Oracle(spec).run(n, cfg.seed, rng="philox_u24", records=True)
+    same, worst = _compare_records(rec, ref.records, FP32_RTOL)
+    diverged = 1.0 - same.mean()
+    assert diverged <= FP32_MAX_DIVERGED, f"diverged fraction {diverged}"
+    for f, tol in FP32_RTOL.items():
+        assert worst[f] < tol, f"{f}: max relative error {worst[f]} over {same.sum()} photons"
+    g, o = rec[same], ref.records[same]
+    path = np.maximum(o["opticalpath"], 1.0)[:, None]
+    for f in ("pos", "r1", "rn", "hit"):
+        e = float((np.abs(g[f] - o[f]) / path).max())
+        assert e < FP32_POS_OF_PATH, f"{f}: {e} of the path length"
+    # tallies: binary32 transport against the binary64 oracle, bin by bin
+    for s_idx, (gt, ot) in enumerate(zip(run.host_tallies(), ref.tallies)):
+        scale = np.abs(ot).max()
+        assert np.abs(gt - ot).max() <= 0.05 * scale + 1e-300, f"sensor {s_idx}"
+        assert abs(gt[0].sum() - ot[0].sum()) <= 1e-3 * abs(ot[0].sum()) + 1e-300
+    run.close()
+
+
+def test_launch_shape_independence(cuda):
+    """Results depend on (seed, photon index) only, like the reference's per-photon
+    seeding makes them independent of n_threads (src/simulation.cpp:172-197)."""
+    spec = W.bilayer_rgd_mie(2000, 31)
+    cfg, _, keep = W.build(lm, spec)
+    a = DeviceRun(cfg)
+    _, ra = a.run(2000, 31, precision="fp64", records=True, block_size=256)
+    b = DeviceRun(cfg)
+    _, rb = b.run(2000, 31, precision="fp64", records=True, block_size=64, blocks_per_sm=1)
+    assert ra.tobytes() == rb.tobytes()
+    a.close()
+    b.close()
+
+
+def test_photon_ranges_compose(cuda):
+    """Two runs over [0, n/2) and [n/2, n) tally the same as one run over [0, n)."""
+    spec = W.mie_cbs_small(4000, 99)
+    cfg, _, keep = W.build(lm, spec)
+    one = DeviceRun(cfg)
+    one.run(4000, 99, precision="fp64")
+    two = DeviceRun(cfg)
+    two.run(2000, 99, 0, precision="fp64")
+    two.run(2000, 99, 2000, precision="fp64")
+    for x, y in zip(one.host_tallies(), two.host_tallies()):
+        np.testing.assert_allclose(x, y, rtol=1e-11, atol=1e-13)
+    one.close()
+    two.close()
+
+
+def test_zero_photons(cuda):
+    cfg, hs, keep = W.build(lm, W.mie_cbs_small(0, 1))
+    lm.run_simulation_parallel(cfg)
+    assert hs[0].hits == 0
+    assert np.all(np.asarray(hs[0].S0_coh[0]) == 0)
+
+
+def test_public_api_matches_oracle(cuda):
+    """run_simulation_parallel through host buffers equals the oracle's tallies, and
+    accumulates into existing tallies like the reference's merge_from."""
+    spec = W.bilayer_rgd_mie(3000, 123)
+    cfg, hs, keep = W.build(lm, spec)
+    lm.run_simulation_parallel(cfg, precision="fp64")
+    ref = O.Oracle(spec).run(3000, 123, rng="philox_u53")
+    for i, (h, s) in enumerate(zip(hs, spec["sensors"])):
+        got = W.tally_arrays(h, s["kind"])
+        np.testing.assert_allclose(got, ref.tallies[i], rtol=FP64_RTOL,
+                                   atol=FP64_RTOL * np.abs(ref.tallies[i]).max())
+        assert h.hits == ref.hits[i]
+    lm.run_simulation_parallel(cfg, precision="fp64")
+    for i, (h, s) in enumerate(zip(hs, spec["sensors"])):
+        np.testing.assert_allclose(W.tally_arrays(h, s["kind"]), 2 * ref.tallies[i],
+                                   rtol=FP64_RTOL, atol=2 * FP64_RTOL * np.abs(ref.tallies[i]).max())
+        assert h.hits == 2 * ref.hits[i]
