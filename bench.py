@@ -48,6 +48,9 @@ def parse():
                     help="CPU work per reference sample (bounded)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--block-size", type=int, default=0)
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--batch-photons", type=int, default=0)
     return ap.parse_args()
 
 
@@ -64,7 +67,9 @@ def config_block(spec, args, n_gpus):
             "sensors": [s["kind"] for s in spec["sensors"]], "layers": len(spec["layers"]),
             "max_events": spec.get("max_events", 1000), "precision": args.precision,
             "l2": "flushed between steps (256 MiB write)", "parallelism": f"photon-range x{n_gpus}",
-            "seed": spec["seed"]}
+            "seed": spec["seed"], "block_size": args.block_size or 256,
+            "blocks_per_sm": args.blocks_per_sm or "auto",
+            "batch_photons": args.batch_photons or (8 << 20)}
 
 
 # ------------------------------------------------------------------------- clocks
@@ -232,7 +237,8 @@ def run_ours(args):
     def step(k):
         flush.zero_()
         st, _ = run.run(P, seed, begin=(k * world * P) + base, precision=args.precision,
-                        stream=stream.cuda_stream)
+                        stream=stream.cuda_stream, block_size=args.block_size,
+                        blocks_per_sm=args.blocks_per_sm, batch_photons=args.batch_photons)
         return st
 
     for k in range(args.warmup):

@@ -89,14 +89,26 @@ template <> __device__ __forceinline__ double sc_top<double>(const Scene &s) { r
 
 // ------------------------------------------------------------------------ RNG
 // Philox4x32-10 (Salmon et al., SC'11); stream contract in luminis_b200.h.
+// Each photon keeps the block holding its next draw (`cur`) and the block after
+// it (`nxt`).  The look-ahead block is generated by rng_prefetch() at the top of
+// every event, where the whole warp is converged, instead of at the draw that
+// empties the current block; lanes sit at different stream positions, so a
+// refill on demand would run the ten Philox rounds at almost every draw site
+// with a few lanes active.
 struct Rng {
-  uint32_t p_lo, p_hi, draw;
-  uint32_t b0, b1, b2, b3;
+  uint32_t p_lo, p_hi;
+  uint32_t draw;               // draws consumed (stream position)
+  uint32_t c0, c1, c2, c3;     // block (draw >> log2(per block))
+  uint32_t n0, n1, n2, n3;     // the block after it
+  uint32_t state;              // bit 0: cur valid, bit 1: nxt valid
 };
 
-__device__ __forceinline__ void philox_block(Rng &g, uint32_t block, uint32_t key0, uint32_t key1)
+// One copy of the ten rounds (called from three places; keeping a single copy
+// keeps the event loop small enough for the instruction cache).
+__device__ __noinline__ uint4 philox_block(uint32_t block, uint32_t p_lo, uint32_t p_hi,
+                                           uint32_t key0, uint32_t key1)
 {
-  uint32_t c0 = block, c1 = 0u, c2 = g.p_lo, c3 = g.p_hi;
+  uint32_t c0 = block, c1 = 0u, c2 = p_lo, c3 = p_hi;
   uint32_t k0 = key0, k1 = key1;
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
@@ -111,32 +123,79 @@ __device__ __forceinline__ void philox_block(Rng &g, uint32_t block, uint32_t ke
     k0 += 0x9E3779B9u;
     k1 += 0xBB67AE85u;
   }
-  g.b0 = c0;
-  g.b1 = c1;
-  g.b2 = c2;
-  g.b3 = c3;
+  return make_uint4(c0, c1, c2, c3);
+}
+
+// log2(draws per block): u24 takes one 32-bit word per draw, u53 two.
+template <typename R> struct DrawsPerBlock;
+template <> struct DrawsPerBlock<float> { static constexpr uint32_t kLog2 = 2; };
+template <> struct DrawsPerBlock<double> { static constexpr uint32_t kLog2 = 1; };
+
+__device__ __forceinline__ void rng_reset(Rng &g, unsigned long long index)
+{
+  g.p_lo = (uint32_t)index;
+  g.p_hi = (uint32_t)(index >> 32);
+  g.draw = 0;
+  g.state = 0;
+}
+
+// Make sure the block after the current one is generated (call while converged).
+template <typename R> __device__ __forceinline__ void rng_prefetch(Rng &g, const RunParams &rp)
+{
+  constexpr uint32_t L = DrawsPerBlock<R>::kLog2;
+  if (!(g.state & 1u)) {
+    const uint4 b = philox_block(g.draw >> L, g.p_lo, g.p_hi, rp.key0, rp.key1);
+    g.c0 = b.x; g.c1 = b.y; g.c2 = b.z; g.c3 = b.w;
+    g.state |= 1u;
+  }
+  if (!(g.state & 2u)) {
+    const uint4 b = philox_block((g.draw >> L) + 1u, g.p_lo, g.p_hi, rp.key0, rp.key1);
+    g.n0 = b.x; g.n1 = b.y; g.n2 = b.z; g.n3 = b.w;
+    g.state |= 2u;
+  }
+}
+
+// Next word of the stream: slot `draw & (per block - 1)` of the current block;
+// moving past the block's end promotes the look-ahead block.
+template <typename R> __device__ __forceinline__ void rng_words(Rng &g, const RunParams &rp,
+                                                                uint32_t &lo, uint32_t &hi)
+{
+  constexpr uint32_t L = DrawsPerBlock<R>::kLog2;
+  constexpr uint32_t M = (1u << L) - 1u;
+  if (!(g.state & 1u)) {                    // look-ahead exhausted inside one event
+    const uint4 b = philox_block(g.draw >> L, g.p_lo, g.p_hi, rp.key0, rp.key1);
+    g.c0 = b.x; g.c1 = b.y; g.c2 = b.z; g.c3 = b.w;
+    g.state |= 1u;
+  }
+  const uint32_t slot = g.draw & M;
+  if (L == 2) {
+    lo = slot == 0u ? g.c0 : slot == 1u ? g.c1 : slot == 2u ? g.c2 : g.c3;
+    hi = 0u;
+  } else {
+    lo = slot == 0u ? g.c0 : g.c2;
+    hi = slot == 0u ? g.c1 : g.c3;
+  }
+  g.draw++;
+  if ((g.draw & M) == 0u) {                 // current block used up
+    g.c0 = g.n0; g.c1 = g.n1; g.c2 = g.n2; g.c3 = g.n3;
+    g.state = (g.state & 2u) ? 1u : 0u;
+  }
 }
 
 template <typename R> __device__ __forceinline__ R uniform(Rng &g, const RunParams &rp);
 
 template <> __device__ __forceinline__ float uniform<float>(Rng &g, const RunParams &rp)   // "u24"
 {
-  const uint32_t slot = g.draw & 3u;
-  if (slot == 0u)
-    philox_block(g, g.draw >> 2, rp.key0, rp.key1);
-  g.draw++;
-  const uint32_t w = slot == 0u ? g.b0 : slot == 1u ? g.b1 : slot == 2u ? g.b2 : g.b3;
+  uint32_t w, unused;
+  rng_words<float>(g, rp, w, unused);
   return __uint2float_rn(2u * (w >> 9) + 1u) * 5.9604644775390625e-8f;   // 2^-24
 }
 
 template <> __device__ __forceinline__ double uniform<double>(Rng &g, const RunParams &rp)  // "u53"
 {
-  const uint32_t slot = g.draw & 1u;
-  if (slot == 0u)
-    philox_block(g, g.draw >> 1, rp.key0, rp.key1);
-  g.draw++;
-  const unsigned long long w = slot == 0u ? ((unsigned long long)g.b1 << 32) | g.b0
-                                          : ((unsigned long long)g.b3 << 32) | g.b2;
+  uint32_t lo, hi;
+  rng_words<double>(g, rp, lo, hi);
+  const unsigned long long w = ((unsigned long long)hi << 32) | lo;
   return __ull2double_rn(2ull * (w >> 12) + 1ull) * 1.1102230246251565e-16;   // 2^-53
 }
 
@@ -275,7 +334,11 @@ template <> __device__ __forceinline__ float sample_theta<float>(const Medium &m
   if (m.theta_kind == LMC_THETA_UNIFORM)
     return 2.0f * atan2f(sqrtf(1.0f - u), sqrtf(u));        // acos(2u - 1)
   const double v = table_sample_f32(m, u);
-  return m.theta_kind == LMC_THETA_TABLE ? (float)v : (float)acos(v);
+  if (m.theta_kind == LMC_THETA_TABLE)
+    return (float)v;
+  // cos-theta tables: theta = 2 atan2(sqrt(1 - c), sqrt(1 + c)) with 1 -/+ c formed
+  // in binary64, accurate near c = +-1 where acosf of a rounded c is not
+  return 2.0f * atan2f(sqrtf((float)(1.0 - v)), sqrtf((float)(1.0 + v)));
 }
 
 template <> __device__ __forceinline__ double sample_theta<double>(const Medium &m, double u)
@@ -429,17 +492,24 @@ __device__ void source_sample(const Laser &L, Rng &g, const RunParams &rp, doubl
   }
 }
 
-// Emission time of the current photon, re-derived from its stream (counter-based,
-// so draws 0.. can be regenerated at any time).
+// Emission time of photon `index`, re-derived from its stream (counter-based, so
+// draws 0.. can be regenerated at any time) instead of carried in registers.
 template <typename R>
-__device__ double launch_time(const Scene &sc, const RunParams &rp, const Photon<R> &ph)
+__device__ __noinline__ double emission_time(const Laser &L, RunParams rp, unsigned long long index)
 {
-  if (sc.laser.temporal == 0)
-    return sc.laser.time_offset * 1e-3;
-  Rng g = {ph.rng.p_lo, ph.rng.p_hi, 0u, 0u, 0u, 0u, 0u};
+  if (L.temporal == 0)
+    return L.time_offset * 1e-3;
+  Rng g;
+  rng_reset(g, index);
   double x, y, t;
-  source_sample<R>(sc.laser, g, rp, x, y, t);
+  source_sample<R>(L, g, rp, x, y, t);
   return t;
+}
+
+template <typename R>
+__device__ __forceinline__ double launch_time(const Scene &sc, const RunParams &rp, const Photon<R> &ph)
+{
+  return emission_time<R>(sc.laser, rp, ph.index());
 }
 
 // ---------------------------------------------------------------- hit snapshot
@@ -537,12 +607,7 @@ __device__ __forceinline__ int time_bin(const Sensor &s, double arrival)
 template <typename R>
 __device__ __forceinline__ double hit_launch_time(const Scene &sc, const RunParams &rp, const HitData<R> &h)
 {
-  if (sc.laser.temporal == 0)
-    return sc.laser.time_offset * 1e-3;
-  Rng g = {h.p_lo, h.p_hi, 0u, 0u, 0u, 0u, 0u};
-  double x, y, t;
-  source_sample<R>(sc.laser, g, rp, x, y, t);
-  return t;
+  return emission_time<R>(sc.laser, rp, ((unsigned long long)h.p_hi << 32) | h.p_lo);
 }
 
 // FarFieldCBSSensor::process_hit (src/detector.cpp:1231-1310) and the far-field
@@ -884,9 +949,7 @@ __device__ void init_photon(const Scene &sc, const RunParams &rp, Photon<R> &ph,
                             unsigned long long index)
 {
   const Laser &L = sc.laser;
-  ph.rng.p_lo = (uint32_t)index;
-  ph.rng.p_hi = (uint32_t)(index >> 32);
-  ph.rng.draw = 0;
+  rng_reset(ph.rng, index);
   double x, y, t;
   source_sample<R>(L, ph.rng, rp, x, y, t);
   ph.px = R(x);
@@ -935,55 +998,57 @@ template <typename R, bool kQueue>
 __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, Photon<R> &ph,
                                           Side<R> &side, Counters &cnt, unsigned long long *s_hits)
 {
+  rng_prefetch<R>(ph.rng, rp);
   {
+    // free path (src/medium.cpp:123-126)
     const Medium &cm = sc.media[sc.layers[ph.layer].medium];
-    R step = -med_mfp<R>(cm) * m_log(uniform<R>(ph.rng, rp));   // src/medium.cpp:123-126
+    R step = -med_mfp<R>(cm) * m_log(uniform<R>(ph.rng, rp));
     cnt.steps++;
     const R dx = ph.P[6], dy = ph.P[7], dz = ph.P[8];
-    if (sc.n_interfaces > 0) {                               // src/simulation.cpp:318-382
-      R zi;
-      bool found = find_next_interface<R>(sc, ph.pz, ph.pz + dz * step, zi);
-      for (int crossings = 0; found; ++crossings) {
-        if (crossings > sc.n_interfaces)                     // each crossing passes a distinct interface
-          return kError;
+    // Move to the next interface (src/simulation.cpp:318-382) or by the whole
+    // step (:389-400), testing the sensor planes after each move (:355, :403).
+    for (int crossing = 0;; ++crossing) {
+      bool at_iface = false;
+      R zi = R(0), s_move = step;
+      if (sc.n_interfaces > 0 && find_next_interface<R>(sc, ph.pz, ph.pz + dz * step, zi)) {
         const R dz_total = dz * step;
-        if (fabs(dz_total) < R(1e-15))
-          break;
-        const R t = (zi - ph.pz) / dz_total;
-        if (t < R(0) || t > R(1))
-          break;
-        const R s_if = step * t;
-        const R rem = (step - s_if) * med_mut<R>(sc.media[sc.layers[ph.layer].medium]);
-        ph.opath += (double)s_if;
-        const R x0 = ph.px, y0 = ph.py, z0 = ph.pz;
-        ph.px += dx * s_if;
-        ph.py += dy * s_if;
+        if (fabs(dz_total) >= R(1e-15)) {
+          const R t = (zi - ph.pz) / dz_total;
+          if (t >= R(0) && t <= R(1)) {
+            at_iface = true;
+            s_move = step * t;
+          }
+        }
+      }
+      if (at_iface && crossing >= sc.n_interfaces)   // each crossing passes a distinct interface
+        return kError;
+      const R rem = at_iface ? (step - s_move) * med_mut<R>(sc.media[sc.layers[ph.layer].medium])
+                             : R(0);
+      ph.opath += (double)s_move;
+      const R x0 = ph.px, y0 = ph.py, z0 = ph.pz;
+      ph.px += dx * s_move;
+      ph.py += dy * s_move;
+      if (at_iface) {
         ph.pz = m_nudge(zi + ((dz > R(0)) ? R(1e-12) : R(-1e-12)), zi, dz > R(0));
-        if (sc.n_planes > 0 && fabs(ph.pz - z0) >= R(1e-12) &&
+      } else {
+        ph.pz += dz * s_move;
+        if (ph.pz > ph.pen)
+          ph.pen = ph.pz;
+      }
+      if (sc.n_planes > 0 && fabs(ph.pz - z0) >= R(1e-12)) {
+        const R zlo = z0 < ph.pz ? z0 : ph.pz, zhi = z0 < ph.pz ? ph.pz : z0;
+        if (sc_plane<R>(sc, 0) <= zhi && sc_plane<R>(sc, sc.n_planes - 1) >= zlo &&
             record_hit<R, kQueue>(sc, rp, ph, side, x0, y0, z0, s_hits))
           return kDetected;
-        const int nl = layer_index_at<R>(sc, ph.pz);
-        if (nl >= sc.n_layers)
-          return kStack;
-        ph.layer = nl;
-        const R nmt = med_mut<R>(sc.media[sc.layers[nl].medium]);
-        step = (nmt > R(0)) ? rem / nmt : rem;
-        found = find_next_interface<R>(sc, ph.pz, ph.pz + dz * step, zi);
       }
-    }
-    ph.opath += (double)step;                                 // :389-400
-    const R x0 = ph.px, y0 = ph.py, z0 = ph.pz;
-    ph.px += dx * step;
-    ph.py += dy * step;
-    ph.pz += dz * step;
-    if (ph.pz > ph.pen)
-      ph.pen = ph.pz;
-    // record_hit (:403-408): only when the step can reach a plane
-    if (sc.n_planes > 0 && fabs(ph.pz - z0) >= R(1e-12)) {
-      const R zlo = z0 < ph.pz ? z0 : ph.pz, zhi = z0 < ph.pz ? ph.pz : z0;
-      if (sc_plane<R>(sc, 0) <= zhi && sc_plane<R>(sc, sc.n_planes - 1) >= zlo &&
-          record_hit<R, kQueue>(sc, rp, ph, side, x0, y0, z0, s_hits))
-        return kDetected;
+      if (!at_iface)
+        break;
+      const int nl = layer_index_at<R>(sc, ph.pz);
+      if (nl >= sc.n_layers)
+        return kStack;
+      ph.layer = nl;
+      const R nmt = med_mut<R>(sc.media[sc.layers[nl].medium]);
+      step = (nmt > R(0)) ? rem / nmt : rem;
     }
     // Sample::is_inside (src/sample.cpp:268-288)
     if (!(isfinite(ph.px) && isfinite(ph.py) && isfinite(ph.pz)) || ph.pz < R(0) ||
@@ -1126,8 +1191,10 @@ __device__ __forceinline__ void load_scene(unsigned char *s_raw, const Scene *g_
     dst[i] = src[i];
 }
 
-template <typename R, bool kQueue>
-__global__ void __launch_bounds__(kBlock) transport_kernel(const Scene *__restrict__ g_scene, RunParams rp)
+// kMinBlocks > 1 asks the compiler to fit that many 256-thread blocks per SM
+// (register cap 65536 / (256 kMinBlocks)); lmc_run picks the variant.
+template <typename R, bool kQueue, int kMinBlocks>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
   __shared__ __align__(16) unsigned char s_raw[sizeof(Scene)];
   __shared__ Side<R> side;

@@ -488,10 +488,14 @@ lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t
   const int block = opts->block_size > 0 ? opts->block_size : dev::kBlock;
   if (block % 32 != 0 || block > dev::kBlock)
     return fail(LMC_ERR_INVALID, "block_size must be a multiple of 32 and at most 256");
-  const void *tk = fp32 ? (h->queued ? (const void *)dev::transport_kernel<float, true>
-                                     : (const void *)dev::transport_kernel<float, false>)
-                        : (h->queued ? (const void *)dev::transport_kernel<double, true>
-                                     : (const void *)dev::transport_kernel<double, false>);
+  // binary32 queued transport: a 2-block (<=128 registers) and a 3-block (<=85
+  // registers, some spills) variant; blocks_per_sm >= 3 selects the latter
+  const bool three = fp32 && h->queued && opts->blocks_per_sm >= 3;
+  const void *tk = fp32 ? (h->queued ? (three ? (const void *)dev::transport_kernel<float, true, 3>
+                                              : (const void *)dev::transport_kernel<float, true, 2>)
+                                     : (const void *)dev::transport_kernel<float, false, 1>)
+                        : (h->queued ? (const void *)dev::transport_kernel<double, true, 1>
+                                     : (const void *)dev::transport_kernel<double, false, 1>);
   int per_sm = 0;
   LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tk, block, 0));
   if (opts->blocks_per_sm > 0)
@@ -538,15 +542,17 @@ lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t
         1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * per_sm,
                                            (nb + block - 1) / block));
     if (fp32) {
-      if (h->queued)
-        dev::transport_kernel<float, true><<<grid, block, 0, stream>>>(h->d_scene, rp);
+      if (h->queued && three)
+        dev::transport_kernel<float, true, 3><<<grid, block, 0, stream>>>(h->d_scene, rp);
+      else if (h->queued)
+        dev::transport_kernel<float, true, 2><<<grid, block, 0, stream>>>(h->d_scene, rp);
       else
-        dev::transport_kernel<float, false><<<grid, block, 0, stream>>>(h->d_scene, rp);
+        dev::transport_kernel<float, false, 1><<<grid, block, 0, stream>>>(h->d_scene, rp);
     } else {
       if (h->queued)
-        dev::transport_kernel<double, true><<<grid, block, 0, stream>>>(h->d_scene, rp);
+        dev::transport_kernel<double, true, 1><<<grid, block, 0, stream>>>(h->d_scene, rp);
       else
-        dev::transport_kernel<double, false><<<grid, block, 0, stream>>>(h->d_scene, rp);
+        dev::transport_kernel<double, false, 1><<<grid, block, 0, stream>>>(h->d_scene, rp);
     }
     LMC_CUDA(cudaGetLastError());
     if (h->queued && h->scene.n_sensors > 0) {
