@@ -599,7 +599,6 @@ lmc_status lmc_run_host(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uin
   const size_t bytes = h->tally_doubles * sizeof(double);
   if (h->host_tally_cap < bytes) {
     cudaFree(h->d_host_tally);
-  cudaFree(h->d_queue);
     h->d_host_tally = nullptr;
     h->host_tally_cap = 0;
     LMC_CUDA(cudaMalloc(&h->d_host_tally, std::max<size_t>(bytes, 8)));

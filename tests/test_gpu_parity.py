@@ -186,3 +186,20 @@ def test_public_api_matches_oracle(cuda):
         np.testing.assert_allclose(W.tally_arrays(h, s["kind"]), 2 * ref.tallies[i],
                                    rtol=FP64_RTOL, atol=2 * FP64_RTOL * np.abs(ref.tallies[i]).max())
         assert h.hits == 2 * ref.hits[i]
+
+
+def test_device_then_host_run_on_one_handle(cuda):
+    """lmc_run (grows the hit queue) followed by lmc_run_host on the same handle:
+    the host path's staging buffer must not disturb the queue the next run reuses."""
+    import torch
+    spec = W.mie_cbs_small(2000, 57)
+    cfg, _, keep = W.build(lm, spec)
+    run = DeviceRun(cfg)
+    run.run(2000, 57, precision="fp64")
+    host = np.zeros(run.transport.tally_size)
+    run.transport.run_host(host, 2000, 57, precision="fp64")
+    run.run(2000, 57, precision="fp64")
+    torch.cuda.synchronize()
+    for d, h in zip(run.host_tallies(), run.transport.split(host)):
+        np.testing.assert_allclose(d, 2 * h, rtol=FP64_RTOL, atol=FP64_RTOL * np.abs(h).max())
+    run.close()
