@@ -8,8 +8,12 @@ tallies and hit counts:
                            ("pin" build: -O2 -ffp-contract=off)
   ref_philox_<scene>.npz   the reference with the Philox replay seam
                            (oracle/replay_rng.cpp), the stream the GPU draws
+  stat_ref_<scene>.npz     R independent-seed replicas of the unmodified reference
+                           (its own RNG): per-bin mean and variance of tally / N,
+                           the statistical oracle for other random streams
 
     python tests/golden/make_golden.py        (needs oracle/_ref; run `make -C oracle ref`)
+    python tests/golden/make_golden.py stat   (the replica fixtures only)
 
 The fixtures pin the oracle (tests/test_oracle_golden.py) and the GPU path
 (tests/test_gpu_golden.py) without the reference present at test time.
@@ -48,6 +52,75 @@ def golden_scenes():
     d["max_events"] = 5000
     d["sensors"][1].update(len_x=0.64, len_y=0.64, dx=0.02, dy=0.02)
     return [a, b, c, d]
+
+
+STAT_REPLICAS = 16
+STAT_PHOTONS = 100_000
+
+
+def stat_scenes():
+    """Scenes with coarse detectors, so that a CPU reference run of R x 1e5 photons fills
+    most bins: mu_a = 0.5/mm keeps paths short.  Every detector kind the reference has,
+    both polarisations, an interface, time bins."""
+    PI = W.PI
+    cbs = {"kind": "farfield_cbs", "theta_max": 0.5, "phi_max": 2 * PI, "len_t": 0.0,
+           "d_theta": 0.05, "d_phi": PI / 2, "d_t": 0.0, "theta_limit": (0.0, 0.5)}
+    flu = {"kind": "planar_fluence", "z": 0.0, "len_x": 4.0, "len_y": 4.0, "len_t": 8.0,
+           "dx": 0.5, "dy": 0.5, "d_t": 2.0, "absorb": True}
+    a = W.mie_cbs_small(STAT_PHOTONS, 1)
+    a["name"] = "stat_mie"
+    a["media"][0].update(mu_a=0.5)
+    a["sensors"] = [dict(cbs), dict(flu)]
+    b = W.bilayer_rgd_mie(STAT_PHOTONS, 1)
+    b["name"] = "stat_bilayer"
+    b["media"][0].update(mu_a=0.5)
+    b["media"][1].update(mu_a=0.5)
+    b["sensors"] = [dict(cbs, len_t=6.0, d_t=3.0), dict(flu),
+                    {"kind": "planar_field", "z": 0.0, "len_x": 1.6, "len_y": 1.6,
+                     "dx": 0.2, "dy": 0.2, "absorb": True}]
+    return [a, b]
+
+
+def replica_moments(tallies_by_replica, n_photons):
+    """Per-bin mean and sample variance (ddof=1) of tally / N over the replicas,
+    one (mean, var) pair per sensor."""
+    out = []
+    for sensor in zip(*tallies_by_replica):
+        x = np.stack([np.asarray(t, dtype=np.float64) / n_photons for t in sensor])
+        out.append((x.mean(axis=0), x.var(axis=0, ddof=1)))
+    return out
+
+
+def run_stat_reference(scene_name):
+    """R replicas of one stat scene with the reference's own RNG (pin build), in a
+    fresh interpreter; returns {sensor<i>_mean, sensor<i>_var, R, N}."""
+    code = f"""
+import os, sys, numpy as np
+sys.path.insert(0, {REPO!r}); sys.path.insert(0, {os.path.join(REPO, 'luminis-mc_b200')!r})
+from tests.golden.make_golden import stat_scenes, replica_moments, STAT_REPLICAS, STAT_PHOTONS
+from luminis_mc_b200 import workloads as W
+from oracle import pyoracle as O
+lm = O.reference_module("pin"); lm.set_log_level(lm.LogLevel.off)
+spec = [s for s in stat_scenes() if s["name"] == {scene_name!r}][0]
+reps = []
+for r in range(STAT_REPLICAS):
+    cfg, hs, keep = W.build(lm, spec, seed=1000 + r, n_threads=os.cpu_count())
+    lm.run_simulation_parallel(cfg)
+    reps.append([W.tally_arrays(h, s["kind"]) for h, s in zip(hs, spec["sensors"])])
+out = {{"R": np.int64(STAT_REPLICAS), "N": np.int64(STAT_PHOTONS)}}
+for i, (m, v) in enumerate(replica_moments(reps, STAT_PHOTONS)):
+    out[f"sensor{{i}}_mean"] = m
+    out[f"sensor{{i}}_var"] = v
+np.savez_compressed(sys.argv[1], **out)
+"""
+    path = os.path.join(HERE, f"stat_ref_{scene_name}.npz")
+    subprocess.run([sys.executable, "-c", code, path], check=True)
+    return path
+
+
+def stat_main():
+    for spec in stat_scenes():
+        print("wrote", run_stat_reference(spec["name"]))
 
 
 def run_flavour(flavour, scene_name, fmt=None):
@@ -98,4 +171,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "stat":
+        stat_main()
+    else:
+        main()
