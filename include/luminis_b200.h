@@ -212,6 +212,28 @@ LMC_API lmc_status lmc_run_host(lmc_handle *h, uint64_t seed, uint64_t photon_be
 /* Copy of the last error message on this thread; returns its length. */
 LMC_API size_t lmc_last_error(char *buf, size_t len);
 
+/* lmc_create + lmc_run + lmc_destroy in one call that allocates no memory: for
+ * callers that cannot allocate device memory, e.g. a host program that runs inside
+ * a memory pool it does not own, or one that must not let cudaMalloc's implicit
+ * device synchronisation stall other streams.  `scene` holds HOST pointers (as for
+ * lmc_create); d_tallies is caller-owned device memory sized as lmc_tally_layout
+ * reports for the same scene, and contributions are ADDED to it.  Everything else
+ * (device scene, derived tables, run counters, hit queue) lives in one static
+ * 64 MiB device array that the CUDA runtime reserves per GPU when this library is
+ * loaded.  Limits: the scene's tables must fit in 8 MiB (a larger scene returns
+ * LMC_ERR_INVALID with the size it needs); photons are processed in batches that
+ * fit the remaining ~56 MiB hit queue.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress), so make that first call before
+ * any stream capture.  All calls on one device share the array: calls that
+ * overlap in time -- from two threads, or on two streams -- race and corrupt each
+ * other's results; serialise them.  Runs on opts->stream (NULL = legacy default
+ * stream) and returns after the stream has finished the run.  stats->kernel_ms is
+ * always 0 (timing events would be allocations).
+ * No counterpart in the reference. */
+LMC_API lmc_status lmc_run_noalloc(const lmc_scene *scene, uint64_t seed, uint64_t photon_begin,
+                                   uint64_t n_photons, const lmc_run_opts *opts, double *d_tallies,
+                                   lmc_stats *stats);
+
 /* ---- set-up physics (host), the constructors' work -------------------------------- */
 
 /* Mie amplitudes S1, S2 (interleaved re/im) at the n cosines mu for size parameter x

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -619,3 +620,359 @@ lmc_status lmc_run_host(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uin
 }
 
 }  // extern "C"
+
+// ======================================================== allocation-free path ==
+// lmc_run_noalloc: the transport for callers that cannot allocate device memory.
+// Everything the kernels need beyond the caller's inputs and outputs -- the
+// device scene, the derived tables, the run counters and the hit queue -- lives
+// in one file-scope __device__ array.  The CUDA runtime reserves it on every GPU
+// that loads this library, until the process exits.
+namespace lmc {
+namespace {
+
+constexpr size_t kNoAllocBytes = size_t(64) << 20;          // 64 MiB per GPU
+constexpr size_t kNaSceneOff = 0;                           // dev::Scene
+constexpr size_t kNaCountersOff = 8192;                     // dev::Scratch
+constexpr size_t kNaTablesOff = 16384;                      // copied + derived tables
+constexpr size_t kNaTablesBytes = size_t(8) << 20;
+constexpr size_t kNaQueueOff = kNaTablesOff + kNaTablesBytes;   // hit queue: the rest
+static_assert(sizeof(dev::Scene) <= kNaCountersOff - kNaSceneOff, "scene region too small");
+static_assert(sizeof(dev::Scratch) <= kNaTablesOff - kNaCountersOff, "counter region too small");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mutex;
+unsigned char *g_noalloc_base[256] = {};                      // per device ordinal
+
+// Device address of g_noalloc_scratch on the current device (looked up once per
+// device; host code cannot use the symbol itself as a device pointer).
+lmc_status noalloc_base(int device, unsigned char **out)
+{
+  if (device < 0 || device >= 256)
+    return fail(LMC_ERR_INVALID, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_base[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(LMC_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") +
+                                    cudaGetErrorString(e));
+    g_noalloc_base[device] = static_cast<unsigned char *>(p);
+  }
+  *out = g_noalloc_base[device];
+  return LMC_OK;
+}
+
+// Guide, (cdf, slope) and interleaved amplitude tables from the copied base tables,
+// the same values lmc_create computes on the host.
+struct DeriveArgs {
+  const double *vals, *cdf;
+  int n;
+  double2 *cs;
+  int *guide;
+  const double *s1, *s2;
+  int amp_n;
+  double4 *amp_d;
+  float4 *amp_f;
+};
+
+__global__ void derive_tables(DeriveArgs a)
+{
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    const double dc = i ? a.cdf[i] - a.cdf[i - 1] : 0.0;
+    a.cs[i] = make_double2(a.cdf[i], dc > 0.0 ? (a.vals[i] - a.vals[i - 1]) / dc : 0.0);
+  }
+  if (a.n > 0)
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j <= dev::kGuideBuckets; j += stride) {
+      const double key = (double)j / dev::kGuideBuckets;
+      int lo = 0, hi = a.n;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a.cdf[mid] < key)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      a.guide[j] = lo < a.n - 1 ? lo : a.n - 1;
+    }
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.amp_n; k += stride) {
+    const double4 v = make_double4(a.s1[2 * k], a.s1[2 * k + 1], a.s2[2 * k], a.s2[2 * k + 1]);
+    a.amp_d[k] = v;
+    a.amp_f[k] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
+  }
+}
+
+}  // namespace
+}  // namespace lmc
+
+extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_t photon_begin,
+                                      uint64_t n_photons, const lmc_run_opts *opts,
+                                      double *d_tallies, lmc_stats *stats)
+{
+  using namespace lmc;
+  if (!opts)
+    return fail(LMC_ERR_INVALID, "options must not be null");
+  const lmc_status v = validate(s);
+  if (v != LMC_OK)
+    return v;
+  if (opts->precision != LMC_PRECISION_FP32 && opts->precision != LMC_PRECISION_FP64)
+    return fail(LMC_ERR_INVALID, "unknown precision");
+  if (opts->max_events < 0)
+    return fail(LMC_ERR_INVALID, "max_events must be non-negative");
+  for (int i = 0; i < s->n_sensors; ++i)
+    if (s->sensors[i].kind == LMC_SENSOR_FARFIELD_CBS && !opts->track_reverse_paths)
+      return fail(LMC_ERR_INVALID, "FarFieldCBSSensor needs track_reverse_paths (the reference "
+                                   "dereferences null species pointers without it)");
+  int device = 0, sm_count = 0;
+  LMC_CUDA(cudaGetDevice(&device));
+  LMC_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
+  unsigned char *base = nullptr;
+  const lmc_status b = noalloc_base(device, &base);
+  if (b != LMC_OK)
+    return b;
+  cudaStream_t stream = static_cast<cudaStream_t>(opts->stream);
+
+  // ---- device scene, built on the stack (no host or device allocation)
+  dev::Scene sc;
+  std::memset(&sc, 0, sizeof(sc));
+  sc.n_layers = s->n_layers;
+  sc.n_media = s->n_media;
+  sc.n_sensors = s->n_sensors;
+  sc.top = s->layers[s->n_layers - 1].z_max;
+  sc.top_is_inf = std::isinf(sc.top) ? 1 : 0;
+  sc.top_f = (float)sc.top;
+  sc.n_step = 1.0 / (1.0 / s->n_host);
+  for (int l = 0; l < s->n_layers; ++l) {
+    sc.layers[l].z_min = s->layers[l].z_min;
+    sc.layers[l].z_max = s->layers[l].z_max;
+    sc.layers[l].medium = s->layers[l].medium;
+    if (l > 0) {
+      sc.interfaces[sc.n_interfaces] = s->layers[l].z_min;
+      sc.interfaces_f[sc.n_interfaces] = (float)s->layers[l].z_min;
+      sc.n_interfaces++;
+    }
+  }
+  const lmc_laser_desc &L = s->laser;
+  for (int j = 0; j < 3; ++j) {
+    sc.laser.pos[j] = L.position[j];
+    sc.laser.dir[j] = L.direction[j];
+    sc.laser.m[j] = L.local_m[j];
+    sc.laser.n[j] = L.local_n[j];
+  }
+  for (int j = 0; j < 4; ++j)
+    sc.laser.E[j] = L.jones[j];
+  sc.laser.k = 2.0 * M_PI / L.wavelength;
+  sc.laser.sigma = L.sigma;
+  sc.laser.source = L.source;
+  sc.laser.temporal = L.temporal;
+  sc.laser.pulse_duration = L.pulse_duration;
+  sc.laser.repetition_rate = L.repetition_rate;
+  sc.laser.time_offset = L.time_offset;
+  double planes[LMC_MAX_SENSORS];
+  int n_planes = 0;
+  size_t tally_doubles = 0;
+  unsigned cbs_mask = 0;
+  for (int i = 0; i < s->n_sensors; ++i) {
+    const lmc_sensor_desc &S = s->sensors[i];
+    dev::Sensor &d = sc.sensors[i];
+    size_t count = 0;
+    int dims[4];
+    fill_sensor(S, d, count, dims);
+    const double z = (S.kind == LMC_SENSOR_FARFIELD_CBS || S.kind == LMC_SENSOR_FARFIELD_FLUENCE) ? 0.0 : S.z;
+    if (S.kind == LMC_SENSOR_PLANAR_FIELD && !d.estimator)
+      sc.need_phase = 1;
+    if (S.kind == LMC_SENSOR_FARFIELD_CBS)
+      cbs_mask |= 1u << i;
+    int g = -1;
+    for (int k = 0; k < n_planes; ++k)
+      if (!(planes[k] < z - 1e-9) && !(z < planes[k] - 1e-9))
+        g = k;
+    if (g < 0) {
+      planes[n_planes] = z;
+      g = n_planes++;
+    }
+    d.plane = g;
+    d.tally_off = tally_doubles;
+    tally_doubles += count;
+  }
+  int rank[LMC_MAX_SENSORS];                                 // planes in ascending z
+  for (int k = 0; k < n_planes; ++k) {
+    int r = 0;
+    for (int q = 0; q < n_planes; ++q)
+      r += (planes[q] < planes[k] || (planes[q] == planes[k] && q < k)) ? 1 : 0;
+    rank[k] = r;
+    sc.plane_z[r] = planes[k];
+    sc.plane_z_f[r] = (float)planes[k];
+  }
+  for (int i = 0; i < s->n_sensors; ++i)
+    sc.sensors[i].plane = rank[sc.sensors[i].plane];
+  sc.n_planes = n_planes;
+  const bool queued = n_planes == 0 || sc.plane_z[n_planes - 1] <= 0.0;
+  if (tally_doubles && !d_tallies)
+    return fail(LMC_ERR_INVALID, "device tally buffer must not be null");
+
+  // ---- tables: base arrays copied in, derived arrays computed on the device
+  auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+  size_t toff = 0;
+  struct MediumSpan { size_t vals, cdf, cs, guide, s1, s2, amp_d, amp_f; };
+  MediumSpan span[LMC_MAX_MEDIA];
+  for (int i = 0; i < s->n_media; ++i) {
+    const lmc_medium_desc &M = s->media[i];
+    const size_t nt = (M.theta_kind == LMC_THETA_TABLE || M.theta_kind == LMC_THETA_TABLE_COS)
+                          ? (size_t)M.theta_n : 0;
+    MediumSpan &p = span[i];
+    p.vals = toff; toff = align(toff + nt * sizeof(double));
+    p.cdf = toff; toff = align(toff + nt * sizeof(double));
+    p.cs = toff; toff = align(toff + nt * sizeof(double2));
+    p.guide = toff; toff = align(toff + (nt ? (dev::kGuideBuckets + 1) * sizeof(int) : 0));
+    p.s1 = toff; toff = align(toff + (size_t)M.amp_n * 2 * sizeof(double));
+    p.s2 = toff; toff = align(toff + (size_t)M.amp_n * 2 * sizeof(double));
+    p.amp_d = toff; toff = align(toff + (size_t)M.amp_n * sizeof(double4));
+    p.amp_f = toff; toff = align(toff + (size_t)M.amp_n * sizeof(float4));
+  }
+  if (toff > kNaTablesBytes)
+    return fail(LMC_ERR_INVALID, "lmc_run_noalloc: the scene's tables need " + std::to_string(toff) +
+                                     " bytes of device memory; this entry point holds at most " +
+                                     std::to_string(kNaTablesBytes) + " (use lmc_create/lmc_run)");
+  unsigned char *tb = base + kNaTablesOff;
+  for (int i = 0; i < s->n_media; ++i) {
+    const lmc_medium_desc &M = s->media[i];
+    const MediumSpan &p = span[i];
+    dev::Medium &d = sc.media[i];
+    d.theta_kind = M.theta_kind;
+    d.hg_g = M.hg_g;
+    d.hg_g_f = (float)M.hg_g;
+    d.mu_t = M.mu_a + M.mu_s;
+    d.mfp = M.mean_free_path;
+    d.albedo = d.mu_t > 0 ? M.mu_s / d.mu_t : 1.0;
+    d.mu_t_f = (float)d.mu_t;
+    d.mfp_f = (float)d.mfp;
+    d.albedo_f = (float)d.albedo;
+    d.amp_n = M.amp_n;
+    d.amp_inv_dx = 1.0 / M.amp_dtheta;
+    d.amp_inv_dx_f = (float)d.amp_inv_dx;
+    const int nt = (M.theta_kind == LMC_THETA_TABLE || M.theta_kind == LMC_THETA_TABLE_COS) ? M.theta_n : 0;
+    DeriveArgs a;
+    std::memset(&a, 0, sizeof(a));
+    if (nt) {
+      d.theta_n = nt;
+      d.th_val_d = reinterpret_cast<const double *>(tb + p.vals);
+      d.th_cdf_d = reinterpret_cast<const double *>(tb + p.cdf);
+      d.th_cs = reinterpret_cast<const double2 *>(tb + p.cs);
+      d.guide_d = reinterpret_cast<const int *>(tb + p.guide);
+      LMC_CUDA(cudaMemcpyAsync(tb + p.vals, M.theta_values, nt * sizeof(double),
+                               cudaMemcpyHostToDevice, stream));
+      LMC_CUDA(cudaMemcpyAsync(tb + p.cdf, M.theta_cdf, nt * sizeof(double),
+                               cudaMemcpyHostToDevice, stream));
+      a.vals = d.th_val_d;
+      a.cdf = d.th_cdf_d;
+      a.n = nt;
+      a.cs = reinterpret_cast<double2 *>(tb + p.cs);
+      a.guide = reinterpret_cast<int *>(tb + p.guide);
+    }
+    d.amp_d = reinterpret_cast<const double4 *>(tb + p.amp_d);
+    d.amp_f = reinterpret_cast<const float4 *>(tb + p.amp_f);
+    LMC_CUDA(cudaMemcpyAsync(tb + p.s1, M.amp_s1, (size_t)M.amp_n * 2 * sizeof(double),
+                             cudaMemcpyHostToDevice, stream));
+    LMC_CUDA(cudaMemcpyAsync(tb + p.s2, M.amp_s2, (size_t)M.amp_n * 2 * sizeof(double),
+                             cudaMemcpyHostToDevice, stream));
+    a.s1 = reinterpret_cast<const double *>(tb + p.s1);
+    a.s2 = reinterpret_cast<const double *>(tb + p.s2);
+    a.amp_n = M.amp_n;
+    a.amp_d = reinterpret_cast<double4 *>(tb + p.amp_d);
+    a.amp_f = reinterpret_cast<float4 *>(tb + p.amp_f);
+    derive_tables<<<64, 256, 0, stream>>>(a);
+    LMC_CUDA(cudaGetLastError());
+  }
+  dev::Scene *d_scene = reinterpret_cast<dev::Scene *>(base + kNaSceneOff);
+  dev::Scratch *d_counters = reinterpret_cast<dev::Scratch *>(base + kNaCountersOff);
+  LMC_CUDA(cudaMemcpyAsync(d_scene, &sc, sizeof(sc), cudaMemcpyHostToDevice, stream));
+  // the array keeps the previous call's contents: counters must start at zero
+  LMC_CUDA(cudaMemsetAsync(d_counters, 0, sizeof(dev::Scratch), stream));
+
+  // ---- launches: the same kernels and batch loop as lmc_run, queue in the array
+  dev::RunParams rp;
+  std::memset(&rp, 0, sizeof(rp));
+  rp.key0 = (uint32_t)seed;
+  rp.key1 = (uint32_t)(seed >> 32);
+  rp.max_events = opts->max_events;
+  rp.track_reverse = opts->track_reverse_paths ? 1 : 0;
+  rp.tallies = d_tallies;
+  rp.records = static_cast<lmc_record *>(opts->records);
+  rp.scratch = d_counters;
+  rp.cbs_mask = cbs_mask;
+  const bool fp32 = opts->precision == LMC_PRECISION_FP32;
+  const int block = dev::kBlock;
+  const void *tk = fp32 ? (queued ? (const void *)dev::transport_kernel<float, true, 2>
+                                  : (const void *)dev::transport_kernel<float, false, 1>)
+                        : (queued ? (const void *)dev::transport_kernel<double, true, 1>
+                                  : (const void *)dev::transport_kernel<double, false, 1>);
+  int per_sm = 0;
+  LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tk, block, 0));
+  per_sm = std::max(per_sm, 1);
+  unsigned long long batch = n_photons;
+  if (queued && n_photons > 0) {
+    const size_t entry = dev::kQU32Fields * 4 + dev::kQF64Fields * 8 +
+                         dev::kQRFields * (fp32 ? sizeof(float) : sizeof(double));
+    const unsigned long long cap = (kNoAllocBytes - kNaQueueOff - 3 * 256) / entry;
+    const unsigned long long planes_n = std::max(1, n_planes);
+    // cap = batch * planes + batch / 16 + 1024, as in lmc_run
+    batch = std::min<unsigned long long>(n_photons, ((cap - 1024) * 16) / (16 * planes_n + 1));
+    if (batch == 0)
+      return fail(LMC_ERR_INVALID, "lmc_run_noalloc: too many sensor planes for the hit queue");
+    unsigned char *q = base + kNaQueueOff;
+    rp.queue.cap = cap;
+    rp.queue.u32 = reinterpret_cast<uint32_t *>(q);
+    size_t o = align((size_t)cap * dev::kQU32Fields * 4);
+    rp.queue.f64 = reinterpret_cast<double *>(q + o);
+    o += align((size_t)cap * dev::kQF64Fields * 8);
+    rp.queue.r = q + o;
+  }
+  for (unsigned long long done = 0; done < n_photons; done += batch) {
+    const unsigned long long nb = std::min(batch, n_photons - done);
+    rp.photon_begin = photon_begin + done;
+    rp.n_photons = nb;
+    LMC_CUDA(cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned long long), stream));
+    const int grid = (int)std::max<unsigned long long>(
+        1ull, std::min<unsigned long long>((unsigned long long)sm_count * per_sm, (nb + block - 1) / block));
+    if (fp32) {
+      if (queued)
+        dev::transport_kernel<float, true, 2><<<grid, block, 0, stream>>>(d_scene, rp);
+      else
+        dev::transport_kernel<float, false, 1><<<grid, block, 0, stream>>>(d_scene, rp);
+    } else {
+      if (queued)
+        dev::transport_kernel<double, true, 1><<<grid, block, 0, stream>>>(d_scene, rp);
+      else
+        dev::transport_kernel<double, false, 1><<<grid, block, 0, stream>>>(d_scene, rp);
+    }
+    LMC_CUDA(cudaGetLastError());
+    if (queued && s->n_sensors > 0) {
+      const int tgrid = (int)std::max<unsigned long long>(
+          1ull, std::min<unsigned long long>((unsigned long long)sm_count * 8,
+                                             (rp.queue.cap + dev::kBlock - 1) / dev::kBlock));
+      if (fp32)
+        dev::tally_kernel<float><<<tgrid, dev::kBlock, 0, stream>>>(d_scene, rp);
+      else
+        dev::tally_kernel<double><<<tgrid, dev::kBlock, 0, stream>>>(d_scene, rp);
+      LMC_CUDA(cudaGetLastError());
+    }
+  }
+  dev::Scratch c;
+  LMC_CUDA(cudaMemcpyAsync(&c, d_counters, sizeof(c), cudaMemcpyDeviceToHost, stream));
+  LMC_CUDA(cudaStreamSynchronize(stream));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->photons = c.photons; stats->events = c.events; stats->steps = c.steps;
+    stats->detected = c.detected; stats->escaped = c.escaped; stats->stack = c.stack;
+    stats->roulette = c.roulette; stats->cap = c.cap; stats->draws = c.draws;
+    for (int i = 0; i < LMC_MAX_SENSORS; ++i)
+      stats->hits[i] = c.hits[i];
+    stats->error_flags = c.error_flags;
+    stats->kernel_ms = 0.f;                  // not timed: timing events would be allocations
+  }
+  if (c.error_flags)
+    return fail(LMC_ERR_KERNEL, "transport kernel raised error flags " + std::to_string(c.error_flags));
+  return LMC_OK;
+}

@@ -101,7 +101,7 @@ RECORD_FIELDS = [("photon", "<u8"), ("events", "<u4"), ("draws", "<u4"), ("fate"
 # Every symbol the header declares (checked by the CPU test suite).
 EXPORTED = ["lmc_create", "lmc_destroy", "lmc_tally_layout", "lmc_run", "lmc_run_host",
             "lmc_last_error", "lmc_mie", "lmc_sampling_table", "lmc_phase_cross_section",
-            "lmc_amplitude_table", "lmc_probe_fp32_peak"]
+            "lmc_amplitude_table", "lmc_probe_fp32_peak", "lmc_run_noalloc"]
 
 _lib = None
 
@@ -148,6 +148,9 @@ def lib():
     L.lmc_amplitude_table.restype = C.c_int
     L.lmc_probe_fp32_peak.argtypes = [C.c_int, dptr, dptr]
     L.lmc_probe_fp32_peak.restype = C.c_int
+    L.lmc_run_noalloc.argtypes = [C.POINTER(SceneDesc), C.c_uint64, C.c_uint64, C.c_uint64,
+                                  C.POINTER(RunOpts), vp, C.POINTER(Stats)]
+    L.lmc_run_noalloc.restype = C.c_int
     _lib = L
     return L
 
