@@ -653,6 +653,114 @@ typedef struct {
   double opticalpath_at_hit;
 } ointeraction;
 
+/* ------------------------------------------------------------ adjoint (LR)
+ * Score of a photon history: d/d(param) of log(path density x weight), summed
+ * over its free flights, albedo factors and HG angle draws.  Free flight from
+ * medium a: tau ~ Exp(1), step = mfp_a tau, and at each interface the remaining
+ * distance is rescaled by mu_t_old / mu_t_new (src/simulation.cpp:318-382), so the
+ * optical depth O = sum_i d_i mu_t_i of a flight is Exp(mean m_a = mfp_a mu_t_a).
+ * A flight ending in a scatter in medium c has log density
+ * log mu_t_c - log m_a - O / m_a; a flight cut by a sensor hit after depth O has
+ * log survival -O / m_a.  Parameters per medium: (mu_a, mu_s, mfp, g). */
+#define OADJ_K (4 * LMC_O_MAX_MEDIA)
+typedef struct {
+  const lmc_o_adjoint *a;
+  double *out;
+  size_t n_out, radial_off, cbs_off[LMC_O_MAX_SENSORS];
+  int K;
+  double score[OADJ_K];       /* running score of the photon (completed segments)  */
+  double hit_score[OADJ_K];   /* score of the current sensor crossing              */
+  int fl_a, fl_cross, seg_med;
+  double fl_m, fl_O, seg_len;
+  const osensor *sensors0;    /* h->sensors, to tell sensors apart */
+} oadj;
+
+static __thread oadj *t_adj;
+
+static void oadj_flight_start(const lmc_o_handle *h, int med)
+{
+  oadj *A = t_adj;
+  A->fl_a = med;
+  A->fl_m = h->media[med].p.mfp * h->media[med].mu_t;
+  A->fl_O = 0.0;
+  A->fl_cross = 0;
+}
+
+/* a segment of length d in medium `med` ended at an interface */
+static void oadj_segment_done(const lmc_o_handle *h, int med, double d)
+{
+  oadj *A = t_adj;
+  A->score[4 * med + 0] -= d / A->fl_m;
+  A->score[4 * med + 1] -= d / A->fl_m;
+  A->fl_O += d * h->media[med].mu_t;
+  A->fl_cross = 1;
+}
+
+/* the flight ended in a scatter in medium c after a last segment of length d */
+static void oadj_flight_scatter(const lmc_o_handle *h, int c, double d)
+{
+  oadj *A = t_adj;
+  const int a = A->fl_a;
+  const double mfp_a = h->media[a].p.mfp;
+  if (!A->fl_cross) {
+    A->score[4 * a + 2] += (d / mfp_a - 1.0) / mfp_a;
+    return;
+  }
+  const double mt_a = h->media[a].mu_t, mt_c = h->media[c].mu_t;
+  A->score[4 * c + 0] -= d / A->fl_m;
+  A->score[4 * c + 1] -= d / A->fl_m;
+  const double O = A->fl_O + d * mt_c;
+  A->score[4 * c + 0] += 1.0 / mt_c;
+  A->score[4 * c + 1] += 1.0 / mt_c;
+  A->score[4 * a + 0] += O / (A->fl_m * mt_a) - 1.0 / mt_a;
+  A->score[4 * a + 1] += O / (A->fl_m * mt_a) - 1.0 / mt_a;
+  A->score[4 * a + 2] += O / (mfp_a * A->fl_m) - 1.0 / mfp_a;
+}
+
+/* score of a crossing at fraction t of the current segment */
+static void oadj_hit(const lmc_o_handle *h, double t)
+{
+  oadj *A = t_adj;
+  memcpy(A->hit_score, A->score, sizeof(double) * (size_t)A->K);
+  const double d = t * A->seg_len;
+  const int a = A->fl_a;
+  const double mfp_a = h->media[a].p.mfp;
+  if (!A->fl_cross) {
+    A->hit_score[4 * a + 2] += (d / mfp_a) / mfp_a;
+    return;
+  }
+  const int sm = A->seg_med;
+  A->hit_score[4 * sm + 0] -= d / A->fl_m;
+  A->hit_score[4 * sm + 1] -= d / A->fl_m;
+  const double O = A->fl_O + d * h->media[sm].mu_t;
+  A->hit_score[4 * a + 0] += O / (A->fl_m * h->media[a].mu_t);
+  A->hit_score[4 * a + 1] += O / (A->fl_m * h->media[a].mu_t);
+  A->hit_score[4 * a + 2] += O / (mfp_a * A->fl_m);
+}
+
+/* a scatter in medium c with sampled cos(theta): albedo and HG terms */
+static void oadj_scatter(const lmc_o_handle *h, const ophase *ph, int c, double cos_theta)
+{
+  oadj *A = t_adj;
+  const omedium *m = &h->media[c];
+  if (m->mu_t > 0) {
+    A->score[4 * c + 0] += -1.0 / m->mu_t;
+    A->score[4 * c + 1] += 1.0 / m->p.mu_s - 1.0 / m->mu_t;
+  }
+  if (ph->p.kind == LMC_O_PHASE_HG) {
+    const double g = ph->p.g;
+    A->score[4 * c + 3] += -2.0 * g / (1.0 - g * g) - 3.0 * (g - cos_theta) / (1.0 + g * g - 2.0 * g * cos_theta);
+  }
+}
+
+static void oadj_add(size_t idx, double v)
+{
+  oadj *A = t_adj;
+  A->out[idx] += v;
+  for (int k = 0; k < A->K; ++k)
+    A->out[(size_t)(1 + k) * A->n_out + idx] += v * A->hit_score[k];
+}
+
 static int time_bin(const osensor *s, double arrival)         /* src/detector.cpp:1182-1190 */
 {
   if (s->p.dt <= 0)
@@ -762,6 +870,26 @@ static void reverse_field_suffix(const lmc_o_handle *h, const m3 *P1, const m3 *
   *Eo_n = fn;
 }
 
+/* adjoint outputs of a FarFieldCBS hit: S0 coherent and incoherent, the bins
+ * accumulate_stokes fills */
+static void oadj_cbs(const lmc_o_handle *h, const osensor *s, int it, int jp, int t_idx, cplx Efx,
+                     cplx Efy, cplx Erx, cplx Ery)
+{
+  const size_t si = (size_t)(s - h->sensors);
+  const cplx Ex = Efx + Erx, Ey = Efy + Ery;
+  const double S0c = cnrm(Ex) + cnrm(Ey);
+  const double S0i = cnrm(Efx) + cnrm(Efy) + cnrm(Erx) + cnrm(Ery);
+  const size_t plane = (size_t)s->N_t * s->N_theta * s->N_phi;
+  for (int pass = 0; pass < 2; ++pass) {
+    const int t = pass == 0 ? 0 : t_idx;
+    if (pass == 1 && t_idx < 1)
+      break;
+    const size_t off = t_adj->cbs_off[si] + ((size_t)t * s->N_theta + it) * s->N_phi + jp;
+    oadj_add(off, S0c);
+    oadj_add(off + plane, S0i);
+  }
+}
+
 /* FarFieldCBSSensor::process_hit, src/detector.cpp:1231-1310; the far-field
  * fluence sensor uses the same binning with the reverse field set to zero. */
 static void process_hit_farfield(const lmc_o_handle *h, const osensor *s, double *tally, ophoton *ph,
@@ -800,6 +928,8 @@ static void process_hit_farfield(const lmc_o_handle *h, const osensor *s, double
       }
     } else {
       accumulate_stokes(s, tally, it, jp, t_idx, Efx, Efy, 0.0, 0.0);
+      if (t_adj)
+        oadj_cbs(h, s, it, jp, t_idx, Efx, Efy, 0.0, 0.0);
     }
     *hits += 1;
     return;
@@ -819,6 +949,8 @@ static void process_hit_farfield(const lmc_o_handle *h, const osensor *s, double
   project_to_lab(Efm, Efn, P, &Efx, &Efy);
   project_to_lab(Ermm, Ernn, P, &Erx, &Ery);
   accumulate_stokes(s, tally, it, jp, t_idx, Efx, Efy, Erx, Ery);
+  if (t_adj)
+    oadj_cbs(h, s, it, jp, t_idx, Efx, Efy, Erx, Ery);
   *hits += 1;
 }
 
@@ -856,6 +988,16 @@ static void process_hit_fluence(const osensor *s, double *tally, const ophoton *
   const size_t off0 = (size_t)x_idx * s->N_y + y_idx;
   for (int q = 0; q < 4; ++q)
     tally[q * plane + off0] += v[q];
+  if (t_adj && (int)(s - t_adj->sensors0) == t_adj->a->radial_sensor) {
+    const size_t r0 = t_adj->radial_off;
+    oadj_add(r0, v[0]);
+    const double r = sqrt(info->point.x * info->point.x + info->point.y * info->point.y);
+    if (r < t_adj->a->radial_max) {
+      const int ir = (int)(r / (t_adj->a->radial_max / t_adj->a->radial_bins));
+      if (ir >= 0 && ir < t_adj->a->radial_bins)
+        oadj_add(r0 + 1 + (size_t)ir, v[0]);
+    }
+  }
   *hits += 1;
 }
 
@@ -899,6 +1041,8 @@ static int record_hit(const lmc_o_handle *h, ophoton *ph, double **tallies, uint
     const double denom = v3dot(d, normal);
     const double t = v3dot(v3sub(v3make(0, 0, z_plane), xn), normal) / denom;
     const v3 hit = v3add(xn, v3scale(d, t));
+    if (t_adj)
+      oadj_hit(h, t);
     const double correction = v3norm(v3sub(hit, xf));
     const double n_local = 1.0 / h->light_speed;
     double optical_path_correction = ph->optical_path;
@@ -1000,10 +1144,14 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
   ph->has_T_prev = 0;
   ph->active_medium = ph->first_medium = ph->last_medium = -1;
   const double n_step = 1.0 / h->light_speed;
+  if (t_adj)
+    memset(t_adj->score, 0, sizeof(t_adj->score));
 
   while (ph->alive) {
     const omedium *cur = layer_medium(h, ph->current_layer);
     double step = -1 * cur->p.mfp * log(orng_uniform(rng));      /* medium.cpp:123-126 */
+    if (t_adj)
+      oadj_flight_start(h, h->scene.layers[ph->current_layer].medium);
     st->steps++;
     const double dir_x = ph->P.a[2][0], dir_y = ph->P.a[2][1], dir_z = ph->P.a[2][2];
     double new_z = ph->pos.z + dir_z * step;
@@ -1025,11 +1173,17 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
       ph->pos.y += dir_y * step_to_iface;
       const double nudge = (dir_z > 0) ? 1e-12 : -1e-12;
       ph->pos.z = z_iface + nudge;
+      if (t_adj) {
+        t_adj->seg_med = h->scene.layers[ph->current_layer].medium;
+        t_adj->seg_len = step_to_iface;
+      }
       if (record_hit(h, ph, tallies, hits)) {
         ph->alive = 0;
         ph->fate = LMC_O_FATE_DETECTED;
         break;
       }
+      if (t_adj)
+        oadj_segment_done(h, h->scene.layers[ph->current_layer].medium, step_to_iface);
       const int new_layer = layer_index_at(h, ph->pos.z);
       if (new_layer >= h->scene.n_layers) {
         ph->alive = 0;
@@ -1056,6 +1210,11 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
     ph->pos.z += dir_z * step;
     if (ph->pos.z > ph->penetration_depth)
       ph->penetration_depth = ph->pos.z;
+    const int last_seg_med = h->scene.layers[ph->current_layer].medium;
+    if (t_adj) {
+      t_adj->seg_med = last_seg_med;
+      t_adj->seg_len = step;
+    }
 
     if (record_hit(h, ph, tallies, hits)) {                     /* :403-408 */
       ph->alive = 0;
@@ -1072,6 +1231,8 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
     const int med_idx = h->scene.layers[scatter_layer].medium;  /* :423-426 */
     const omedium *sm = &h->media[med_idx];
     ph->active_medium = med_idx;
+    if (t_adj)
+      oadj_flight_scatter(h, last_seg_med, step);
 
     const double theta = ophase_sample_theta(&h->phase[sm->phase], orng_uniform(rng));  /* :429 */
     cplx S2, S1;
@@ -1099,6 +1260,8 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
     }
     const double cos_theta = cos(theta), sin_theta = sin(theta);     /* :438-453 */
     const double cos_phi = cos(phi), sin_phi = sin(phi);
+    if (t_adj)
+      oadj_scatter(h, &h->phase[sm->phase], med_idx, cos_theta);
     {
       double A[3][3] = {{cos_theta * cos_phi, cos_theta * sin_phi, -sin_theta},
                         {-sin_phi, cos_phi, 0},
@@ -1335,6 +1498,53 @@ int lmc_oracle_run(lmc_o_handle *h, uint64_t seed, uint64_t begin, uint64_t coun
     stats->roulette += local.roulette; stats->cap += local.cap; stats->draws += local.draws;
   }
   return 0;
+}
+
+static int oadj_layout(const lmc_o_handle *h, const lmc_o_adjoint *a, oadj *A)
+{
+  memset(A, 0, sizeof(*A));
+  A->a = a;
+  A->K = 4 * h->scene.n_media;
+  A->sensors0 = h->sensors;
+  size_t n = 0;
+  if (a->radial_sensor >= 0) {
+    if (a->radial_sensor >= h->scene.n_sensors ||
+        h->sensors[a->radial_sensor].p.kind != LMC_O_SENSOR_PLANAR_FLUENCE ||
+        a->radial_bins < 1 || !(a->radial_max > 0))
+      return -1;
+    A->radial_off = 0;
+    n = 1 + (size_t)a->radial_bins;
+  }
+  for (int si = 0; si < h->scene.n_sensors; ++si) {
+    const osensor *s = &h->sensors[si];
+    if (s->p.kind != LMC_O_SENSOR_FARFIELD_CBS)
+      continue;
+    A->cbs_off[si] = n;
+    n += 2 * (size_t)s->N_t * s->N_theta * s->N_phi;
+  }
+  A->n_out = n;
+  return 0;
+}
+
+size_t lmc_oracle_adjoint_outputs(const lmc_o_handle *h, const lmc_o_adjoint *a)
+{
+  oadj A;
+  return oadj_layout(h, a, &A) == 0 ? A.n_out : 0;
+}
+
+int lmc_oracle_run_adjoint(lmc_o_handle *h, uint64_t seed, uint64_t begin, uint64_t count, int rng,
+                           int max_events, int track_reverse, double **tallies, uint64_t *hits,
+                           const lmc_o_adjoint *a, double *out, lmc_o_stats *stats)
+{
+  oadj A;
+  if (oadj_layout(h, a, &A) != 0)
+    return -3;
+  A.out = out;
+  t_adj = &A;
+  const int rc = lmc_oracle_run(h, seed, begin, count, rng, max_events, track_reverse, tallies, hits,
+                                NULL, stats);
+  t_adj = NULL;
+  return rc;
 }
 
 int lmc_oracle_phase_table(const lmc_o_handle *h, int medium, int *n, const double **values,

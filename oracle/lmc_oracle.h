@@ -151,6 +151,29 @@ int lmc_oracle_run(lmc_o_handle *h, uint64_t seed, uint64_t begin, uint64_t coun
                    int max_events, int track_reverse, double **tallies, uint64_t *hits,
                    lmc_o_record *records, lmc_o_stats *stats);
 
+/* Likelihood-ratio derivatives of selected outputs with respect to each medium's
+ * parameters, in the order (mu_a, mu_s, mean_free_path, HG g) per medium:
+ * K = 4 n_media.  Outputs (n_out doubles per row):
+ *   [radial sensor]   total S0 of the PlanarFluence sensor's time-integrated grid,
+ *                     then radial_bins bins of the same S0 by hit radius
+ *                     sqrt(x^2+y^2) < radial_max                (if radial_sensor >= 0)
+ *   [each FarFieldCBS] S0 coherent then S0 incoherent, [N_t][N_theta][N_phi] each
+ * out has (1 + K) rows: row 0 the outputs, row 1 + k their derivative for param k.
+ * The estimator: every hit contributes v * (1, s_1..s_K), s = the photon's score,
+ * the derivative of log(path density x weight) accumulated over its history:
+ * free flights (exponential with mean mean_free_path, crossings rescaled by the
+ * mu_t ratio), albedo factors mu_s/mu_t and HG angle densities. */
+typedef struct lmc_o_adjoint {
+  int radial_sensor;
+  int radial_bins;
+  double radial_max;
+} lmc_o_adjoint;
+
+size_t lmc_oracle_adjoint_outputs(const lmc_o_handle *h, const lmc_o_adjoint *a);
+int lmc_oracle_run_adjoint(lmc_o_handle *h, uint64_t seed, uint64_t begin, uint64_t count, int rng,
+                           int max_events, int track_reverse, double **tallies, uint64_t *hits,
+                           const lmc_o_adjoint *a, double *out, lmc_o_stats *stats);
+
 /* Tables the oracle built (for table parity): theta sampling table of a medium's
  * phase function (values/cdf of n_div+1), and amplitude tables (n complex). */
 int lmc_oracle_phase_table(const lmc_o_handle *h, int medium, int *n, const double **values,

@@ -100,6 +100,13 @@ class Stats(C.Structure):
                  "draws")]
 
 
+class Adjoint(C.Structure):
+    _fields_ = [("radial_sensor", C.c_int), ("radial_bins", C.c_int), ("radial_max", C.c_double)]
+
+
+ADJ_PARAMS = ("mu_a", "mu_s", "mfp", "g")      # per medium, in this order
+
+
 _lib = None
 
 
@@ -117,6 +124,13 @@ def lib():
         L.lmc_oracle_run.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_int,
                                      C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_double)),
                                      C.POINTER(C.c_uint64), C.c_void_p, C.POINTER(Stats)]
+        L.lmc_oracle_adjoint_outputs.restype = C.c_size_t
+        L.lmc_oracle_adjoint_outputs.argtypes = [C.c_void_p, C.POINTER(Adjoint)]
+        L.lmc_oracle_run_adjoint.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64,
+                                             C.c_int, C.c_int, C.c_int,
+                                             C.POINTER(C.POINTER(C.c_double)),
+                                             C.POINTER(C.c_uint64), C.POINTER(Adjoint),
+                                             C.POINTER(C.c_double), C.POINTER(Stats)]
         L.lmc_oracle_phase_table.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                              C.POINTER(C.POINTER(C.c_double)),
                                              C.POINTER(C.POINTER(C.c_double))]
@@ -291,6 +305,39 @@ class Oracle:
         stats = {n: int(getattr(st, n)) for n, _ in Stats._fields_}
         return OracleResult([t.reshape(s) for t, s in zip(tallies, self.shapes)],
                             hits[: len(tallies)], rec, stats)
+
+    def run_adjoint(self, n_photons: int, seed: int, radial_sensor: int = -1,
+                    radial_bins: int = 100, radial_max: float = 5.0, begin: int = 0,
+                    rng: str = "philox_u53", max_events: int | None = None,
+                    track_reverse: bool | None = None):
+        """Tallies plus the likelihood-ratio outputs: returns (OracleResult, out) with
+        out[0] the outputs (radial total + profile, then S0 coherent / incoherent of
+        each FarFieldCBS sensor) and out[1 + 4 m + j] their derivative with respect
+        to parameter j = (mu_a, mu_s, mfp, g) of medium m."""
+        max_events = int(self.spec.get("max_events", 1000) if max_events is None else max_events)
+        if track_reverse is None:
+            track_reverse = bool(self.spec.get("track_reverse_paths", True))
+        a = Adjoint(radial_sensor, radial_bins, radial_max)
+        n_out = lib().lmc_oracle_adjoint_outputs(self._h, C.byref(a))
+        if n_out == 0:
+            raise ValueError("no adjoint outputs (radial sensor must be a PlanarFluenceSensor)")
+        K = 4 * self._scene.n_media
+        out = np.zeros((1 + K, n_out), dtype=np.float64)
+        tallies = [np.zeros(int(np.prod(s)), dtype=np.float64) for s in self.shapes]
+        ptrs = (C.POINTER(C.c_double) * max(1, len(tallies)))()
+        for i, t in enumerate(tallies):
+            ptrs[i] = t.ctypes.data_as(C.POINTER(C.c_double))
+        hits = np.zeros(max(1, len(tallies)), dtype=np.uint64)
+        st = Stats()
+        rc = lib().lmc_oracle_run_adjoint(self._h, seed, begin, n_photons, RNG[rng], max_events,
+                                          int(bool(track_reverse)), ptrs,
+                                          hits.ctypes.data_as(C.POINTER(C.c_uint64)), C.byref(a),
+                                          out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st))
+        if rc != 0:
+            raise ValueError(f"oracle adjoint run failed ({rc})")
+        stats = {n: int(getattr(st, n)) for n, _ in Stats._fields_}
+        return OracleResult([t.reshape(s) for t, s in zip(tallies, self.shapes)],
+                            hits[: len(tallies)], None, stats), out
 
     def phase_table(self, medium: int):
         n = C.c_int()
