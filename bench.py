@@ -33,6 +33,10 @@ sys.path.insert(0, REPO)
 
 FLOP_PER_EVENT = 300        # FP32 flops per scattering event (add/mul = 1, FMA = 2)
 METRIC = "photons/s"
+# DRAM bytes (read + write) per photon of one transport launch on bilayer_rgd_mie in
+# FP32: 166.07 MB for a 2 M-photon launch in one ncu capture
+# (profiles/transport_kernel_bilayer_rgd_mie.md); traffic grows with photons.
+TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": 166.07e6 / 2e6}
 
 
 def parse():
@@ -51,6 +55,8 @@ def parse():
     ap.add_argument("--block-size", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--batch-photons", type=int, default=0)
+    ap.add_argument("--variant-steps", type=int, default=2,
+                    help="timed steps of the FP64 and FP32+adjoint variants (0: skip them)")
     return ap.parse_args()
 
 
@@ -262,12 +268,19 @@ def run_ours(args):
     photons_done = sum(s["photons"] for s in stats)
     assert photons_done == P * args.steps, (photons_done, P * args.steps)
 
-    # roofline: the transport kernel is FP32/SFU issue-bound; measured FMA peak
+    # roofline: the transport kernel is FP32/SFU issue-bound; measured FMA peak.
+    # achieved = algorithmic flops of its launches / their own CUDA-event time
     peak_tflops, _ = N.probe_fp32_peak(200000)
-    achieved_tflops = events * FLOP_PER_EVENT / (kernel_ms * 1e-3) / 1e12
-    launches = 0
-    nb = max(1, math.ceil(P / (8 << 20)))
-    launches = args.steps * nb * 2        # one transport + one tally kernel per batch
+    transport_ms = sum(s["transport_ms"] for s in stats)
+    transport_launches = sum(s["transport_launches"] for s in stats)
+    achieved_tflops = events * FLOP_PER_EVENT / (transport_ms * 1e-3) / 1e12
+    per_photon = TRAFFIC_BYTES_PER_PHOTON.get(spec["name"]) if args.precision == "fp32" else None
+    traffic = per_photon * P / max(1, transport_launches // args.steps) if per_photon else None
+    launches = 2 * transport_launches     # one transport + one tally kernel per batch
+
+    variants = {}
+    if args.variant_steps > 0:
+        variants = measure_variants(args, spec, local, stream, flush, world, rank, dist)
 
     # end-to-end through the public API: host tally arrays, copies inside
     e2e = None
@@ -324,13 +337,87 @@ def run_ours(args):
                              "peak": peak_tflops, "unit": "TFLOP/s",
                              "frac": achieved_tflops / peak_tflops,
                              "peak_source": "measured: FFMA probe (lmc_probe_fp32_peak) on this GPU",
-                             "flop_per_event": FLOP_PER_EVENT, "traffic": None},
+                             "flop_per_event": FLOP_PER_EVENT,
+                             "kernel": "transport_kernel", "launches": transport_launches,
+                             "ms_per_launch": transport_ms / max(1, transport_launches),
+                             "traffic": traffic,
+                             "traffic_source": "ncu dram bytes per photon x photons per launch"
+                                               if traffic else None},
+                "variants": variants,
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     run.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def measure_variants(args, spec, local, stream, flush, world, rank, dist):
+    """The two other arms of the headline metric on this GPU: the same workload in
+    FP64 throughout, and FP32 transport with the likelihood-ratio derivatives of the
+    differentiable configuration (HG bilayer, 1e7 photons, radial fluence profile of
+    100 bins to 5 mm, CBS cone).  photons/s from the device time of the runs."""
+    import torch
+
+    import luminis_mc_b200 as lm
+    from luminis_mc_b200 import workloads as W
+    from luminis_mc_b200.adjoint import AdjointTransport
+    from luminis_mc_b200.device import DeviceRun
+
+    def max_ms(ms):
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    out = {}
+    P = int(spec["n_photons"])
+    cfg, _, keep = W.build(lm, spec)
+    run = DeviceRun(cfg, device=f"cuda:{local}")
+    ms = 0.0
+    for k in range(1 + args.variant_steps):
+        flush.zero_()
+        st, _ = run.run(P, int(spec["seed"]), begin=(k * world + rank) * P, precision="fp64",
+                        stream=stream.cuda_stream)
+        if k >= 1:
+            ms += st["kernel_ms"]
+    run.close()
+    ms = max_ms(ms)
+    out["fp64"] = {"value": P * world * args.variant_steps / (ms * 1e-3), "unit": "photons/s",
+                   "workload": spec["name"], "steps": args.variant_steps}
+
+    aspec = W.bilayer_hg(10_000_000, 2024)
+    acfg, _, akeep = W.build(lm, aspec)
+    PA = int(aspec["n_photons"])
+    run = DeviceRun(acfg, device=f"cuda:{local}")
+    ms = 0.0
+    for k in range(1 + args.variant_steps):
+        flush.zero_()
+        st, _ = run.run(PA, 2024, begin=(k * world + rank) * PA, precision="fp32",
+                        stream=stream.cuda_stream)
+        if k >= 1:
+            ms += st["kernel_ms"]
+    run.close()
+    ms = max_ms(ms)
+    out["fp32_differentiable_workload"] = {
+        "value": PA * world * args.variant_steps / (ms * 1e-3), "unit": "photons/s",
+        "workload": "bilayer_hg (differentiable), no derivatives", "steps": args.variant_steps}
+    tr = AdjointTransport(acfg, radial_sensor=1, radial_bins=100, radial_max=5.0,
+                          device=f"cuda:{local}")
+    ms = 0.0
+    for k in range(1 + args.variant_steps):
+        flush.zero_()
+        _, _, st = tr.run(PA, 2024, precision="fp32", begin=(k * world + rank) * PA,
+                          stream=stream.cuda_stream)
+        if k >= 1:
+            ms += st["kernel_ms"]
+    tr.close()
+    ms = max_ms(ms)
+    out["fp32_adjoint"] = {"value": PA * world * args.variant_steps / (ms * 1e-3),
+                           "unit": "photons/s", "workload": "bilayer_hg (differentiable)",
+                           "parameters": 8, "outputs": "total + 100 radial bins + CBS S0 cone",
+                           "steps": args.variant_steps}
+    return out
 
 
 def main():

@@ -174,7 +174,9 @@ typedef struct lmc_stats {
   uint64_t photons, events, steps, detected, escaped, stack, roulette, cap, draws;
   uint64_t hits[LMC_MAX_SENSORS];   /* Sensor::hits increments                         */
   uint32_t error_flags;             /* device error word (0 = none)                    */
-  float kernel_ms;                  /* transport kernel time, CUDA events              */
+  float kernel_ms;                  /* whole run on the device (all launches), CUDA events */
+  float transport_ms;               /* sum of the transport kernel launches alone       */
+  uint32_t transport_launches;      /* transport kernel launches (queue batches)        */
 } lmc_stats;
 
 typedef struct lmc_handle lmc_handle;
@@ -233,6 +235,41 @@ LMC_API size_t lmc_last_error(char *buf, size_t len);
 LMC_API lmc_status lmc_run_noalloc(const lmc_scene *scene, uint64_t seed, uint64_t photon_begin,
                                    uint64_t n_photons, const lmc_run_opts *opts, double *d_tallies,
                                    lmc_stats *stats);
+
+/* ---- likelihood-ratio derivatives ("adjoint") --------------------------------------- */
+/* Derivatives of selected outputs with respect to every medium's parameters
+ * (mu_a, mu_s, mean_free_path, HG g), K = 4 n_media, estimated in the same transport
+ * pass by the likelihood-ratio (score) method: every hit contributes v * (1, s_1..s_K),
+ * s = d log(path density x weight) / d param accumulated over the photon's flights,
+ * albedo factors and HG angle draws.  Running per-photon sums; no path is stored.
+ * No counterpart in the reference (config "Differentiable" of the task). */
+typedef struct lmc_adjoint_opts {
+  int radial_sensor;           /* PlanarFluenceSensor: total S0 of its time-integrated
+                                  grid + radial S0 profile by hit radius; -1: none    */
+  int radial_bins;             /* 1..512                                              */
+  double radial_max;           /* profile covers r in [0, radial_max)                 */
+} lmc_adjoint_opts;
+
+/* Outputs per row (n_out doubles): [total, radial_bins bins] when radial_sensor >= 0,
+ * then for each FarFieldCBSSensor S0 coherent and S0 incoherent, [N_t][N_theta][N_phi]
+ * each.  The buffer holds (1 + n_params) rows: the outputs, then d outputs / d param k
+ * for k = 4 medium + (0 mu_a, 1 mu_s, 2 mean_free_path, 3 g).  Needs every sensor plane
+ * at z <= 0 and at most 4 media. */
+LMC_API lmc_status lmc_adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a, size_t *n_out,
+                                      int *n_params);
+
+/* lmc_run that also ADDS the outputs and their derivatives into d_adjoint (device,
+ * (1 + n_params) x n_out doubles). */
+LMC_API lmc_status lmc_run_adjoint(lmc_handle *h, uint64_t seed, uint64_t photon_begin,
+                                   uint64_t n_photons, const lmc_run_opts *opts,
+                                   const lmc_adjoint_opts *a, double *d_tallies, double *d_adjoint,
+                                   lmc_stats *stats);
+
+/* Backward pass: d_grad_params[k] = sum_j d_adjoint[(1 + k) n_out + j] * d_grad_out[j]
+ * (all device pointers; enqueued on `stream`, NULL = legacy default stream). */
+LMC_API lmc_status lmc_adjoint_contract(const double *d_adjoint, const double *d_grad_out,
+                                        size_t n_out, int n_params, double *d_grad_params,
+                                        void *stream);
 
 /* ---- set-up physics (host), the constructors' work -------------------------------- */
 

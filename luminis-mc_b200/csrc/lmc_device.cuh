@@ -22,6 +22,8 @@ struct Medium {
   const int *guide_d;                    // kGuideBuckets + 1 entries
   const double4 *amp_d;                  // (s1.re, s1.im, s2.re, s2.im) per node
   const float4 *amp_f;
+  double mu_s;                           // scattering coefficient (likelihood-ratio scores)
+  float mu_s_f, pad_s;
 };
 
 struct Layer {
@@ -95,6 +97,13 @@ enum QueueR {
   kQRBasic = 16               // fields every entry carries
 };
 
+// Likelihood-ratio ("adjoint") runs append the photon's score, one R per parameter
+// (mu_a, mu_s, mean free path, HG g of each medium), after the R fields above.
+constexpr int kQScore = kQRFields;
+constexpr int kAdjMaxMedia = 4;
+constexpr int kAdjMaxK = 4 * kAdjMaxMedia;
+constexpr int kAdjMaxRadialBins = 512;
+
 struct Queue {
   unsigned long long cap;
   uint32_t *u32;                         // [kQU32Fields][cap]
@@ -118,6 +127,13 @@ struct RunParams {
   Queue queue;                           // used by the queued kernel pair
   unsigned int cbs_mask;                 // sensors whose hits need the CBS fields
   unsigned int pad;
+  // likelihood-ratio outputs: (1 + adj_K) rows of adj_n_out doubles; row 0 the
+  // outputs, row 1 + k their derivative for parameter k = 4 medium + (mu_a, mu_s, mfp, g)
+  double *adj_out;
+  unsigned long long adj_n_out;
+  int adj_K, adj_radial_sensor, adj_radial_bins, adj_pad;
+  double adj_radial_max;
+  unsigned long long adj_cbs_off[LMC_MAX_SENSORS];
 };
 
 }  // namespace dev

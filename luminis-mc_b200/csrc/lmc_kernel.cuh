@@ -230,6 +230,110 @@ struct Counters {
   uint32_t events, steps, draws;
 };
 
+// ------------------------------------------------------- likelihood-ratio score
+// Score of a photon history: d/d(param) of log(path density x weight), summed over
+// its free flights, albedo factors and HG angle draws (the estimator of
+// oracle/lmc_oracle.c, in the same order of operations).  A free flight from medium
+// a draws tau ~ Exp(1), step = mfp_a tau, and every interface rescales the remaining
+// distance by mu_t_old / mu_t_new (src/simulation.cpp:318-382): its optical depth
+// O = sum_i d_i mu_t_i is exponential with mean m_a = mfp_a mu_t_a.  A flight ending
+// in a scatter in medium c has log density log mu_t_c - log m_a - O / m_a; one cut
+// by a sensor hit has log survival -O / m_a.  Parameters k = 4 medium + (mu_a, mu_s,
+// mfp, g).  The running scores live in shared memory, one column per thread.
+template <typename R> __device__ __forceinline__ R med_mus(const Medium &m);
+template <> __device__ __forceinline__ float med_mus<float>(const Medium &m) { return m.mu_s_f; }
+template <> __device__ __forceinline__ double med_mus<double>(const Medium &m) { return m.mu_s; }
+template <typename R> __device__ __forceinline__ R med_g(const Medium &m);
+template <> __device__ __forceinline__ float med_g<float>(const Medium &m) { return m.hg_g_f; }
+template <> __device__ __forceinline__ double med_g<double>(const Medium &m) { return m.hg_g; }
+
+template <typename R> struct Flight {
+  R *score;                    // this thread's column: score[k * kBlock]
+  R m, O, seg_len;             // m_a; depth of completed segments; current segment length
+  int a, cross, seg_med;       // start medium; crossed an interface; current segment's medium
+  __device__ __forceinline__ R &operator[](int k) const { return score[k * kBlock]; }
+};
+
+template <typename R>
+__device__ __forceinline__ void flight_start(const Scene &sc, Flight<R> &f, int med)
+{
+  const Medium &m = sc.media[med];
+  f.a = med;
+  f.m = med_mfp<R>(m) * med_mut<R>(m);
+  f.O = R(0);
+  f.cross = 0;
+}
+
+template <typename R>
+__device__ __forceinline__ void flight_segment_done(const Scene &sc, Flight<R> &f, int med, R d)
+{
+  f[4 * med + 0] -= d / f.m;
+  f[4 * med + 1] -= d / f.m;
+  f.O += d * med_mut<R>(sc.media[med]);
+  f.cross = 1;
+}
+
+template <typename R>
+__device__ __forceinline__ void flight_scatter(const Scene &sc, Flight<R> &f, int c, R d)
+{
+  const int a = f.a;
+  const R mfp_a = med_mfp<R>(sc.media[a]);
+  if (!f.cross) {
+    f[4 * a + 2] += (d / mfp_a - R(1)) / mfp_a;
+    return;
+  }
+  const R mt_a = med_mut<R>(sc.media[a]), mt_c = med_mut<R>(sc.media[c]);
+  f[4 * c + 0] -= d / f.m;
+  f[4 * c + 1] -= d / f.m;
+  const R O = f.O + d * mt_c;
+  f[4 * c + 0] += R(1) / mt_c;
+  f[4 * c + 1] += R(1) / mt_c;
+  f[4 * a + 0] += O / (f.m * mt_a) - R(1) / mt_a;
+  f[4 * a + 1] += O / (f.m * mt_a) - R(1) / mt_a;
+  f[4 * a + 2] += O / (mfp_a * f.m) - R(1) / mfp_a;
+}
+
+// Albedo and HG terms of a scatter in medium c with sampled cos(theta).
+template <typename R>
+__device__ __forceinline__ void flight_event(const Scene &sc, Flight<R> &f, int c, R cos_theta)
+{
+  const Medium &m = sc.media[c];
+  const R mt = med_mut<R>(m);
+  if (mt > R(0)) {
+    f[4 * c + 0] += R(-1) / mt;
+    f[4 * c + 1] += R(1) / med_mus<R>(m) - R(1) / mt;
+  }
+  if (m.theta_kind == LMC_THETA_HG) {
+    const R g = med_g<R>(m);
+    f[4 * c + 3] += R(-2) * g / (R(1) - g * g) -
+                    R(3) * (g - cos_theta) / (R(1) + g * g - R(2) * g * cos_theta);
+  }
+}
+
+// Score k of a sensor crossing at fraction t of the current segment.
+template <typename R>
+__device__ __forceinline__ R flight_hit_score(const Scene &sc, const Flight<R> &f, R t, int k)
+{
+  R v = f[k];
+  const R d = t * f.seg_len;
+  const int a = f.a;
+  const R mfp_a = med_mfp<R>(sc.media[a]);
+  if (!f.cross) {
+    if (k == 4 * a + 2)
+      v += (d / mfp_a) / mfp_a;
+    return v;
+  }
+  const int sm = f.seg_med;
+  if (k == 4 * sm + 0 || k == 4 * sm + 1)
+    v -= d / f.m;
+  const R O = f.O + d * med_mut<R>(sc.media[sm]);
+  if (k == 4 * a + 0 || k == 4 * a + 1)
+    v += O / (f.m * med_mut<R>(sc.media[a]));
+  if (k == 4 * a + 2)
+    v += O / (mfp_a * f.m);
+  return v;
+}
+
 template <typename R> __device__ __forceinline__ int layer_index_at(const Scene &sc, R z)
 {                                                          // src/sample.cpp:221-235
   if (z < R(0))
@@ -610,12 +714,34 @@ __device__ __forceinline__ double hit_launch_time(const Scene &sc, const RunPara
   return emission_time<R>(sc.laser, rp, ((unsigned long long)h.p_hi << 32) | h.p_lo);
 }
 
+// Likelihood-ratio outputs of one hit contribution v: row 0 += v, row 1 + k +=
+// v * score_k.  Global atomics (FarFieldCBS bins), or the block's shared-memory copy
+// of the radial outputs (rows of adj_radial_bins + 1 doubles).
+template <typename R>
+__device__ __forceinline__ void adj_add_global(const RunParams &rp, unsigned long long idx, double v,
+                                               const R *hs)
+{
+  atomicAdd(rp.adj_out + idx, v);
+  for (int k = 0; k < rp.adj_K; ++k)
+    atomicAdd(rp.adj_out + (unsigned long long)(1 + k) * rp.adj_n_out + idx, v * (double)hs[k]);
+}
+
+template <typename R>
+__device__ __forceinline__ void adj_add_shared(const RunParams &rp, double *s_rad, int idx, double v,
+                                               const R *hs)
+{
+  const int row = rp.adj_radial_bins + 1;
+  atomicAdd(s_rad + idx, v);
+  for (int k = 0; k < rp.adj_K; ++k)
+    atomicAdd(s_rad + (1 + k) * row + idx, v * (double)hs[k]);
+}
+
 // FarFieldCBSSensor::process_hit (src/detector.cpp:1231-1310) and the far-field
 // fluence sensor (same binning, reverse field zero).  exp(i k L) multiplies E_f
 // and E_r alike and cancels in every Stokes parameter, so it is not formed.
-template <typename R>
+template <typename R, bool kAdj>
 __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor &s,
-                             const HitData<R> &h, lmc_record *rec)
+                             const HitData<R> &h, lmc_record *rec, int si, const R *hs)
 {
   const double t_launch = (s.dt > 0) ? hit_launch_time<R>(sc, rp, h) : 0.0;
   const int t_idx = time_bin(s, t_launch + h.opath);
@@ -686,13 +812,23 @@ __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor 
     add4(base, P, t_idx * tstride + cell, c0, c1, c2, c3);
     add4(base + 4 * P, P, t_idx * tstride + cell, i0, i1, i2, i3);
   }
+  if (kAdj && s.kind == LMC_SENSOR_FARFIELD_CBS) {     // S0 coherent, S0 incoherent
+    const unsigned long long o = rp.adj_cbs_off[si];
+    adj_add_global<R>(rp, o + cell, c0, hs);
+    adj_add_global<R>(rp, o + P + cell, i0, hs);
+    if (t_idx >= 1) {
+      adj_add_global<R>(rp, o + t_idx * tstride + cell, c0, hs);
+      adj_add_global<R>(rp, o + P + t_idx * tstride + cell, i0, hs);
+    }
+  }
   return true;
 }
 
 // PlanarFluenceSensor::process_hit (src/detector.cpp:780-841): lab-frame Stokes
 // with E_x negated; exp(i k L) cancels and is not formed.
-template <typename R>
-__device__ bool hit_fluence(const Scene &sc, const RunParams &rp, const Sensor &s, const HitData<R> &h)
+template <typename R, bool kAdj>
+__device__ bool hit_fluence(const Scene &sc, const RunParams &rp, const Sensor &s, const HitData<R> &h,
+                            int si, const R *hs, double *s_rad)
 {
   int t_idx = -1;
   if (s.dt > 0) {
@@ -720,6 +856,15 @@ __device__ bool hit_fluence(const Scene &sc, const RunParams &rp, const Sensor &
   if (s.dt > 0)
     add4(base, s.plane_stride, t_idx * tstride + cell, q0, q1, q2, q3);
   add4(base, s.plane_stride, cell, q0, q1, q2, q3);
+  if (kAdj && si == rp.adj_radial_sensor) {            // total S0 and its radial profile
+    adj_add_shared<R>(rp, s_rad, 0, q0, hs);
+    const double r = sqrt((double)h.hx * (double)h.hx + (double)h.hy * (double)h.hy);
+    if (r < rp.adj_radial_max) {
+      const int ir = (int)(r / (rp.adj_radial_max / rp.adj_radial_bins));
+      if (ir >= 0 && ir < rp.adj_radial_bins)
+        adj_add_shared<R>(rp, s_rad, 1 + ir, q0, hs);
+    }
+  }
   return true;
 }
 
@@ -751,9 +896,9 @@ __device__ bool hit_field(const Scene &sc, const RunParams &rp, const Sensor &s,
 
 // process_hit of every sensor in `mask` (all on the plane of this hit), in
 // insertion order, as SensorsGroup::record_hit calls them (src/detector.cpp:244-265).
-template <typename R>
+template <typename R, bool kAdj>
 __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData<R> &h,
-                             unsigned mask, unsigned long long *hits)
+                             unsigned mask, unsigned long long *hits, const R *hs, double *s_rad)
 {
   lmc_record *rec = rp.records ? rp.records + ((((unsigned long long)h.p_hi << 32) | h.p_lo) -
                                                rp.photon_begin)
@@ -764,11 +909,11 @@ __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData
     const Sensor &s = sc.sensors[si];
     bool counted;
     if (s.kind == LMC_SENSOR_PLANAR_FLUENCE)
-      counted = hit_fluence<R>(sc, rp, s, h);
+      counted = hit_fluence<R, kAdj>(sc, rp, s, h, si, hs, s_rad);
     else if (s.kind == LMC_SENSOR_PLANAR_FIELD)
       counted = hit_field<R>(sc, rp, s, h);
     else
-      counted = hit_farfield<R>(sc, rp, s, h, rec);
+      counted = hit_farfield<R, kAdj>(sc, rp, s, h, rec, si, hs);
     if (counted) {
       atomicAdd(hits + si, 1ull);
       if (rec) {
@@ -842,8 +987,9 @@ __device__ __forceinline__ void fill_hit(const Photon<R> &ph, const Side<R> &sid
 
 // Append a hit to the queue (warp-aggregated slot).  Only the fields the
 // sensors in `mask` read are written.
-template <typename R>
-__device__ __forceinline__ void enqueue_hit(const RunParams &rp, const Photon<R> &ph, const Side<R> &side,
+template <typename R, bool kAdj>
+__device__ __forceinline__ void enqueue_hit(const Scene &sc, const RunParams &rp, const Photon<R> &ph,
+                                            const Side<R> &side, const Flight<R> &fl, R t,
                                             R hx, R hy, R hz, double opath, unsigned mask)
 {
   const unsigned active = __activemask();
@@ -896,14 +1042,17 @@ __device__ __forceinline__ void enqueue_hit(const RunParams &rp, const Photon<R>
       r[(kQT + 2 * qd + 1) * C + slot] = ph.T[qd].im;
     }
   }
+  if (kAdj)
+    for (int k = 0; k < rp.adj_K; ++k)
+      r[(kQScore + k) * C + slot] = flight_hit_score<R>(sc, fl, t, k);
 }
 
 // SensorsGroup::record_hit (src/detector.cpp:178-270) for the step (x0,y0,z0) -> pos.
 // kQueue: hits are appended to the queue for the tally kernel; otherwise they are
 // processed here.  Returns whether an absorbing sensor took the photon.
-template <typename R, bool kQueue>
+template <typename R, bool kQueue, bool kAdj>
 __device__ __forceinline__ bool record_hit(const Scene &sc, const RunParams &rp, Photon<R> &ph,
-                                           const Side<R> &side, R x0, R y0, R z0,
+                                           const Side<R> &side, const Flight<R> &fl, R x0, R y0, R z0,
                                            unsigned long long *s_hits)
 {
   const R z1 = z0, z2 = ph.pz;
@@ -933,11 +1082,11 @@ __device__ __forceinline__ bool record_hit(const Scene &sc, const RunParams &rp,
     }
     if (mask) {
       if (kQueue) {
-        enqueue_hit<R>(rp, ph, side, hx, hy, hz, opath, mask);
+        enqueue_hit<R, kAdj>(sc, rp, ph, side, fl, t, hx, hy, hz, opath, mask);
       } else {
         HitData<R> h;
         fill_hit<R>(ph, side, hx, hy, hz, opath, h);
-        process_hits<R>(sc, rp, h, mask, s_hits);
+        process_hits<R, false>(sc, rp, h, mask, s_hits, nullptr, nullptr);
       }
     }
   }
@@ -994,9 +1143,10 @@ constexpr int kMaxRejectionTrials = 1 << 16;
 
 // One loop iteration of run_photon (src/simulation.cpp:297-614).  Returns the
 // photon's fate (kAlive if it continues).
-template <typename R, bool kQueue>
+template <typename R, bool kQueue, bool kAdj>
 __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, Photon<R> &ph,
-                                          Side<R> &side, Counters &cnt, unsigned long long *s_hits)
+                                          Side<R> &side, Flight<R> &fl, Counters &cnt,
+                                          unsigned long long *s_hits)
 {
   rng_prefetch<R>(ph.rng, rp);
   {
@@ -1004,6 +1154,8 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
     const Medium &cm = sc.media[sc.layers[ph.layer].medium];
     R step = -med_mfp<R>(cm) * m_log(uniform<R>(ph.rng, rp));
     cnt.steps++;
+    if (kAdj)
+      flight_start<R>(sc, fl, sc.layers[ph.layer].medium);
     const R dx = ph.P[6], dy = ph.P[7], dz = ph.P[8];
     // Move to the next interface (src/simulation.cpp:318-382) or by the whole
     // step (:389-400), testing the sensor planes after each move (:355, :403).
@@ -1035,14 +1187,20 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
         if (ph.pz > ph.pen)
           ph.pen = ph.pz;
       }
+      if (kAdj) {
+        fl.seg_med = sc.layers[ph.layer].medium;
+        fl.seg_len = s_move;
+      }
       if (sc.n_planes > 0 && fabs(ph.pz - z0) >= R(1e-12)) {
         const R zlo = z0 < ph.pz ? z0 : ph.pz, zhi = z0 < ph.pz ? ph.pz : z0;
         if (sc_plane<R>(sc, 0) <= zhi && sc_plane<R>(sc, sc.n_planes - 1) >= zlo &&
-            record_hit<R, kQueue>(sc, rp, ph, side, x0, y0, z0, s_hits))
+            record_hit<R, kQueue, kAdj>(sc, rp, ph, side, fl, x0, y0, z0, s_hits))
           return kDetected;
       }
       if (!at_iface)
         break;
+      if (kAdj)
+        flight_segment_done<R>(sc, fl, fl.seg_med, s_move);
       const int nl = layer_index_at<R>(sc, ph.pz);
       if (nl >= sc.n_layers)
         return kStack;
@@ -1058,6 +1216,8 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   ph.layer = layer_index_at<R>(sc, ph.pz);
   const int med_idx = sc.layers[ph.layer].medium;
   const Medium &m = sc.media[med_idx];
+  if (kAdj)
+    flight_scatter<R>(sc, fl, fl.seg_med, fl.seg_len);
 
   const R theta = sample_theta<R>(m, uniform<R>(ph.rng, rp));  // :429
   Cx<R> S2, S1;
@@ -1084,6 +1244,8 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   }
   R st, ct;
   m_sincos(theta, &st, &ct);
+  if (kAdj)
+    flight_event<R>(sc, fl, med_idx, ct);
   // frame update P <- A(theta, phi) P (src/simulation.cpp:438-453); P_{n-1} <- old P
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
@@ -1193,13 +1355,18 @@ __device__ __forceinline__ void load_scene(unsigned char *s_raw, const Scene *g_
 
 // kMinBlocks > 1 asks the compiler to fit that many 256-thread blocks per SM
 // (register cap 65536 / (256 kMinBlocks)); lmc_run picks the variant.
-template <typename R, bool kQueue, int kMinBlocks>
+// kAdj: likelihood-ratio run; the scores take adj_K * kBlock R of dynamic shared
+// memory (queued mode only).
+template <typename R, bool kQueue, int kMinBlocks, bool kAdj = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
   __shared__ __align__(16) unsigned char s_raw[sizeof(Scene)];
   __shared__ Side<R> side;
   __shared__ unsigned long long s_hits[LMC_MAX_SENSORS];
   __shared__ unsigned long long s_fate[7];
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  Flight<R> fl;
+  fl.score = reinterpret_cast<R *>(s_dyn) + threadIdx.x;
   load_scene(s_raw, g_scene);
   if (threadIdx.x < LMC_MAX_SENSORS)
     s_hits[threadIdx.x] = 0;
@@ -1223,6 +1390,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
         const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
         if (idx < rp.n_photons) {
           init_photon<R>(sc, rp, ph, side, rp.photon_begin + idx);
+          if (kAdj)
+            for (int k = 0; k < rp.adj_K; ++k)
+              fl[k] = R(0);
           alive = true;
         } else {
           done = true;
@@ -1232,7 +1402,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
     if (__all_sync(kFull, done))
       break;
     if (alive) {
-      const int fate = event_step<R, kQueue>(sc, rp, ph, side, cnt, s_hits);
+      const int fate = event_step<R, kQueue, kAdj>(sc, rp, ph, side, fl, cnt, s_hits);
       if (fate != kAlive) {
         alive = false;
         cnt.draws += ph.rng.draw;
@@ -1275,14 +1445,21 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
 }
 
 // Tally kernel: one thread per queued hit runs the sensors' process_hit.
-template <typename R>
+// kAdj: also the likelihood-ratio outputs; the radial ones are summed per block in
+// (1 + adj_K) * (adj_radial_bins + 1) doubles of dynamic shared memory.
+template <typename R, bool kAdj = false>
 __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
   __shared__ __align__(16) unsigned char s_raw[sizeof(Scene)];
   __shared__ unsigned long long s_hits[LMC_MAX_SENSORS];
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  double *s_rad = reinterpret_cast<double *>(s_dyn);
+  const int rad_n = (kAdj && rp.adj_radial_sensor >= 0) ? (1 + rp.adj_K) * (rp.adj_radial_bins + 1) : 0;
   load_scene(s_raw, g_scene);
   if (threadIdx.x < LMC_MAX_SENSORS)
     s_hits[threadIdx.x] = 0;
+  for (int j = threadIdx.x; j < rad_n; j += blockDim.x)
+    s_rad[j] = 0.0;
   __syncthreads();
   const Scene &sc = *reinterpret_cast<const Scene *>(s_raw);
   const Queue &q = rp.queue;
@@ -1325,11 +1502,45 @@ __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__
       for (int qd = 0; qd < 4; ++qd)
         h.T[qd] = {r[(kQT + 2 * qd) * C + i], r[(kQT + 2 * qd + 1) * C + i]};
     }
-    process_hits<R>(sc, rp, h, mask, s_hits);
+    R hs[kAdj ? kAdjMaxK : 1];
+    if (kAdj)
+      for (int k = 0; k < rp.adj_K; ++k)
+        hs[k] = r[(kQScore + k) * C + i];
+    process_hits<R, kAdj>(sc, rp, h, mask, s_hits, hs, s_rad);
   }
   __syncthreads();
   if (threadIdx.x < LMC_MAX_SENSORS && s_hits[threadIdx.x])
     atomicAdd(&rp.scratch->hits[threadIdx.x], s_hits[threadIdx.x]);
+  if (kAdj && rad_n) {                   // radial outputs sit at offset 0 of every row
+    const int row = rp.adj_radial_bins + 1;
+    for (int j = threadIdx.x; j < rad_n; j += blockDim.x)
+      if (s_rad[j] != 0.0)
+        atomicAdd(rp.adj_out + (unsigned long long)(j / row) * rp.adj_n_out + (j % row), s_rad[j]);
+  }
+}
+
+// Backward contraction of the likelihood-ratio outputs: grad[k] = sum_j
+// J[(1 + k) n_out + j] g[j].  One block per parameter, fixed-order tree reduction,
+// so the result does not depend on scheduling.
+__global__ void __launch_bounds__(kBlock) adjoint_contract_kernel(const double *__restrict__ J,
+                                                                  const double *__restrict__ g,
+                                                                  unsigned long long n_out,
+                                                                  double *__restrict__ grad)
+{
+  __shared__ double s[kBlock];
+  const double *row = J + (unsigned long long)(1 + blockIdx.x) * n_out;
+  double acc = 0.0;
+  for (unsigned long long j = threadIdx.x; j < n_out; j += blockDim.x)
+    acc = fma(row[j], g[j], acc);
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    grad[blockIdx.x] = s[0];
 }
 
 }  // namespace dev

@@ -57,6 +57,7 @@ struct lmc_handle {
   int sm_count = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> kev;          // per transport launch: start, end
   double *d_host_tally = nullptr;        // staging for lmc_run_host
   size_t host_tally_cap = 0;
   void *d_queue = nullptr;               // hit queue (queued mode), grown on demand
@@ -352,6 +353,8 @@ lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
     d.amp_n = M.amp_n;
     d.amp_inv_dx = 1.0 / M.amp_dtheta;
     d.amp_inv_dx_f = (float)d.amp_inv_dx;
+    d.mu_s = M.mu_s;
+    d.mu_s_f = (float)M.mu_s;
     MedOff &o = mo[i];
     o = MedOff{0, 0, 0, 0, 0, 0};
     if (M.theta_kind == LMC_THETA_TABLE || M.theta_kind == LMC_THETA_TABLE_COS) {
@@ -431,6 +434,8 @@ void lmc_destroy(lmc_handle *h)
   cudaFree(h->d_scratch);
   cudaFree(h->d_host_tally);
   cudaFree(h->d_queue);
+  for (cudaEvent_t e : h->kev)
+    cudaEventDestroy(e);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -456,8 +461,50 @@ lmc_status lmc_tally_layout(const lmc_handle *h, int sensor, size_t *offset, siz
   return LMC_OK;
 }
 
-lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
-                   const lmc_run_opts *opts, double *d_tallies, lmc_stats *stats)
+// Layout of the likelihood-ratio outputs of a handle (lmc_adjoint_layout).
+static lmc_status adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a, size_t *n_out,
+                                 unsigned long long cbs_off[LMC_MAX_SENSORS])
+{
+  using namespace lmc;
+  if (!h || !a)
+    return fail(LMC_ERR_INVALID, "handle and adjoint options must not be null");
+  if (!h->queued)
+    return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs need every sensor plane at z <= 0");
+  if (h->scene.n_media > dev::kAdjMaxMedia)
+    return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs support at most 4 media");
+  for (int i = 0; i < h->scene.n_media; ++i) {
+    const dev::Medium &m = h->scene.media[i];
+    if (!(m.mu_t > 0) || !(m.mu_s > 0))
+      return fail(LMC_ERR_INVALID, "likelihood-ratio outputs need mu_s > 0 in every medium");
+  }
+  size_t n = 0;
+  if (a->radial_sensor >= 0) {
+    if (a->radial_sensor >= h->scene.n_sensors ||
+        h->scene.sensors[a->radial_sensor].kind != LMC_SENSOR_PLANAR_FLUENCE)
+      return fail(LMC_ERR_INVALID, "radial_sensor must be a PlanarFluenceSensor");
+    if (a->radial_bins < 1 || a->radial_bins > dev::kAdjMaxRadialBins || !(a->radial_max > 0))
+      return fail(LMC_ERR_INVALID, "radial_bins must be in [1, 512] and radial_max > 0");
+    n = 1 + (size_t)a->radial_bins;
+  }
+  for (int i = 0; i < LMC_MAX_SENSORS; ++i)
+    cbs_off[i] = 0;
+  for (int i = 0; i < h->scene.n_sensors; ++i) {
+    const dev::Sensor &s = h->scene.sensors[i];
+    if (s.kind != LMC_SENSOR_FARFIELD_CBS)
+      continue;
+    cbs_off[i] = n;
+    n += 2 * (size_t)s.N_t * s.N_theta * s.N_phi;
+  }
+  if (n == 0)
+    return fail(LMC_ERR_INVALID, "no likelihood-ratio outputs: no radial sensor and no FarFieldCBSSensor");
+  *n_out = n;
+  return LMC_OK;
+}
+
+// lmc_run and lmc_run_adjoint (adj == nullptr: plain run).
+static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
+                           const lmc_run_opts *opts, const lmc_adjoint_opts *adj, double *d_adj,
+                           double *d_tallies, lmc_stats *stats)
 {
   using namespace lmc;
   if (!h || !opts)
@@ -489,16 +536,44 @@ lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t
   const int block = opts->block_size > 0 ? opts->block_size : dev::kBlock;
   if (block % 32 != 0 || block > dev::kBlock)
     return fail(LMC_ERR_INVALID, "block_size must be a multiple of 32 and at most 256");
+  const size_t rbytes = fp32 ? sizeof(float) : sizeof(double);
+  size_t dyn_transport = 0, dyn_tally = 0;
+  if (adj) {
+    size_t n_out = 0;
+    const lmc_status ls = adjoint_layout(h, adj, &n_out, rp.adj_cbs_off);
+    if (ls != LMC_OK)
+      return ls;
+    if (!d_adj)
+      return fail(LMC_ERR_INVALID, "device adjoint buffer must not be null");
+    rp.adj_out = d_adj;
+    rp.adj_n_out = n_out;
+    rp.adj_K = 4 * h->scene.n_media;
+    rp.adj_radial_sensor = adj->radial_sensor;
+    rp.adj_radial_bins = adj->radial_bins;
+    rp.adj_radial_max = adj->radial_max;
+    dyn_transport = (size_t)rp.adj_K * dev::kBlock * rbytes;
+    if (adj->radial_sensor >= 0)
+      dyn_tally = (size_t)(1 + rp.adj_K) * (adj->radial_bins + 1) * sizeof(double);
+  }
   // binary32 queued transport: a 2-block (<=128 registers) and a 3-block (<=85
   // registers, some spills) variant; blocks_per_sm >= 3 selects the latter
-  const bool three = fp32 && h->queued && opts->blocks_per_sm >= 3;
-  const void *tk = fp32 ? (h->queued ? (three ? (const void *)dev::transport_kernel<float, true, 3>
-                                              : (const void *)dev::transport_kernel<float, true, 2>)
-                                     : (const void *)dev::transport_kernel<float, false, 1>)
-                        : (h->queued ? (const void *)dev::transport_kernel<double, true, 1>
-                                     : (const void *)dev::transport_kernel<double, false, 1>);
+  const bool three = fp32 && h->queued && opts->blocks_per_sm >= 3 && !adj;
+  const void *tk =
+      adj ? (fp32 ? (const void *)dev::transport_kernel<float, true, 2, true>
+                  : (const void *)dev::transport_kernel<double, true, 1, true>)
+          : fp32 ? (h->queued ? (three ? (const void *)dev::transport_kernel<float, true, 3>
+                                       : (const void *)dev::transport_kernel<float, true, 2>)
+                              : (const void *)dev::transport_kernel<float, false, 1>)
+                 : (h->queued ? (const void *)dev::transport_kernel<double, true, 1>
+                              : (const void *)dev::transport_kernel<double, false, 1>);
+  if (adj) {
+    LMC_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_transport));
+    const void *tl = fp32 ? (const void *)dev::tally_kernel<float, true>
+                          : (const void *)dev::tally_kernel<double, true>;
+    LMC_CUDA(cudaFuncSetAttribute(tl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_tally));
+  }
   int per_sm = 0;
-  LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tk, block, 0));
+  LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tk, block, dyn_transport));
   if (opts->blocks_per_sm > 0)
     per_sm = std::min(per_sm, opts->blocks_per_sm);
   per_sm = std::max(per_sm, 1);
@@ -510,9 +585,8 @@ lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t
     batch = std::min<unsigned long long>(batch, n_photons);
     const unsigned long long planes = std::max(1, h->scene.n_planes);
     const unsigned long long cap = batch * planes + batch / 16 + 1024;
-    const size_t rbytes = fp32 ? sizeof(float) : sizeof(double);
     const size_t need = (size_t)cap * (dev::kQU32Fields * 4 + dev::kQF64Fields * 8 +
-                                       dev::kQRFields * rbytes) + 3 * 256;
+                                       (dev::kQRFields + (size_t)rp.adj_K) * rbytes) + 3 * 256;
     if (h->queue_bytes < need) {
       cudaFree(h->d_queue);
       h->d_queue = nullptr;
@@ -532,6 +606,14 @@ lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t
     o += align((size_t)cap * dev::kQF64Fields * 8);
     rp.queue.r = q + o;
   }
+  if (stats && n_photons > 0) {           // one event pair per transport launch
+    const size_t need_ev = 2 * (size_t)((n_photons + batch - 1) / batch);
+    while (h->kev.size() < need_ev) {
+      cudaEvent_t e = nullptr;
+      LMC_CUDA(cudaEventCreate(&e));
+      h->kev.push_back(e);
+    }
+  }
   LMC_CUDA(cudaEventRecord(h->ev0, stream));
   for (unsigned long long done = 0; done < n_photons; done += batch) {
     const unsigned long long nb = std::min(batch, n_photons - done);
@@ -542,7 +624,15 @@ lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t
     const int grid = (int)std::max<unsigned long long>(
         1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * per_sm,
                                            (nb + block - 1) / block));
-    if (fp32) {
+    const size_t pair = 2 * (size_t)(done / batch);
+    if (stats)
+      LMC_CUDA(cudaEventRecord(h->kev[pair], stream));
+    if (adj) {
+      if (fp32)
+        dev::transport_kernel<float, true, 2, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
+      else
+        dev::transport_kernel<double, true, 1, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
+    } else if (fp32) {
       if (h->queued && three)
         dev::transport_kernel<float, true, 3><<<grid, block, 0, stream>>>(h->d_scene, rp);
       else if (h->queued)
@@ -556,14 +646,22 @@ lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t
         dev::transport_kernel<double, false, 1><<<grid, block, 0, stream>>>(h->d_scene, rp);
     }
     LMC_CUDA(cudaGetLastError());
+    if (stats)
+      LMC_CUDA(cudaEventRecord(h->kev[pair + 1], stream));
     if (h->queued && h->scene.n_sensors > 0) {
       const int tgrid = (int)std::max<unsigned long long>(
           1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * 8,
                                              (rp.queue.cap + dev::kBlock - 1) / dev::kBlock));
-      if (fp32)
+      if (adj) {
+        if (fp32)
+          dev::tally_kernel<float, true><<<tgrid, dev::kBlock, dyn_tally, stream>>>(h->d_scene, rp);
+        else
+          dev::tally_kernel<double, true><<<tgrid, dev::kBlock, dyn_tally, stream>>>(h->d_scene, rp);
+      } else if (fp32) {
         dev::tally_kernel<float><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
-      else
+      } else {
         dev::tally_kernel<double><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
+      }
       LMC_CUDA(cudaGetLastError());
     }
   }
@@ -582,9 +680,60 @@ lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t
     float ms = 0.f;
     LMC_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     stats->kernel_ms = ms;
+    const size_t launches = batch ? (size_t)((n_photons + batch - 1) / batch) : 0;
+    double tms = 0.0;
+    for (size_t b = 0; b < launches; ++b) {
+      float d = 0.f;
+      LMC_CUDA(cudaEventElapsedTime(&d, h->kev[2 * b], h->kev[2 * b + 1]));
+      tms += d;
+    }
+    stats->transport_ms = (float)tms;
+    stats->transport_launches = (uint32_t)launches;
     if (sc.error_flags)
       return fail(LMC_ERR_KERNEL, "transport kernel raised error flags " + std::to_string(sc.error_flags));
   }
+  return LMC_OK;
+}
+
+lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
+                   const lmc_run_opts *opts, double *d_tallies, lmc_stats *stats)
+{
+  return run_impl(h, seed, photon_begin, n_photons, opts, nullptr, nullptr, d_tallies, stats);
+}
+
+lmc_status lmc_adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a, size_t *n_out,
+                              int *n_params)
+{
+  unsigned long long off[LMC_MAX_SENSORS];
+  size_t n = 0;
+  const lmc_status st = adjoint_layout(h, a, &n, off);
+  if (st != LMC_OK)
+    return st;
+  if (n_out)
+    *n_out = n;
+  if (n_params)
+    *n_params = 4 * h->scene.n_media;
+  return LMC_OK;
+}
+
+lmc_status lmc_run_adjoint(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
+                           const lmc_run_opts *opts, const lmc_adjoint_opts *adj, double *d_tallies,
+                           double *d_adjoint, lmc_stats *stats)
+{
+  if (!adj)
+    return lmc::fail(LMC_ERR_INVALID, "adjoint options must not be null");
+  return run_impl(h, seed, photon_begin, n_photons, opts, adj, d_adjoint, d_tallies, stats);
+}
+
+lmc_status lmc_adjoint_contract(const double *d_adjoint, const double *d_grad_out, size_t n_out,
+                                int n_params, double *d_grad_params, void *stream)
+{
+  using namespace lmc;
+  if (!d_adjoint || !d_grad_out || !d_grad_params || n_out == 0 || n_params < 1)
+    return fail(LMC_ERR_INVALID, "lmc_adjoint_contract: null buffer or empty sizes");
+  dev::adjoint_contract_kernel<<<n_params, dev::kBlock, 0, static_cast<cudaStream_t>(stream)>>>(
+      d_adjoint, d_grad_out, n_out, d_grad_params);
+  LMC_CUDA(cudaGetLastError());
   return LMC_OK;
 }
 
@@ -852,6 +1001,8 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     d.amp_n = M.amp_n;
     d.amp_inv_dx = 1.0 / M.amp_dtheta;
     d.amp_inv_dx_f = (float)d.amp_inv_dx;
+    d.mu_s = M.mu_s;
+    d.mu_s_f = (float)M.mu_s;
     const int nt = (M.theta_kind == LMC_THETA_TABLE || M.theta_kind == LMC_THETA_TABLE_COS) ? M.theta_n : 0;
     DeriveArgs a;
     std::memset(&a, 0, sizeof(a));

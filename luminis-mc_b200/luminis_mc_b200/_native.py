@@ -73,7 +73,8 @@ class Stats(C.Structure):
                 ("detected", C.c_uint64), ("escaped", C.c_uint64), ("stack", C.c_uint64),
                 ("roulette", C.c_uint64), ("cap", C.c_uint64), ("draws", C.c_uint64),
                 ("hits", C.c_uint64 * MAX_SENSORS), ("error_flags", C.c_uint32),
-                ("kernel_ms", C.c_float)]
+                ("kernel_ms", C.c_float), ("transport_ms", C.c_float),
+                ("transport_launches", C.c_uint32)]
 
     def as_dict(self) -> dict:
         d = {n: int(getattr(self, n)) for n in
@@ -81,7 +82,13 @@ class Stats(C.Structure):
               "draws", "error_flags")}
         d["hits"] = [int(x) for x in self.hits]
         d["kernel_ms"] = float(self.kernel_ms)
+        d["transport_ms"] = float(self.transport_ms)
+        d["transport_launches"] = int(self.transport_launches)
         return d
+
+
+class AdjointOpts(C.Structure):
+    _fields_ = [("radial_sensor", C.c_int), ("radial_bins", C.c_int), ("radial_max", C.c_double)]
 
 
 class PhaseParams(C.Structure):
@@ -101,7 +108,8 @@ RECORD_FIELDS = [("photon", "<u8"), ("events", "<u4"), ("draws", "<u4"), ("fate"
 # Every symbol the header declares (checked by the CPU test suite).
 EXPORTED = ["lmc_create", "lmc_destroy", "lmc_tally_layout", "lmc_run", "lmc_run_host",
             "lmc_last_error", "lmc_mie", "lmc_sampling_table", "lmc_phase_cross_section",
-            "lmc_amplitude_table", "lmc_probe_fp32_peak", "lmc_run_noalloc"]
+            "lmc_amplitude_table", "lmc_probe_fp32_peak", "lmc_run_noalloc",
+            "lmc_adjoint_layout", "lmc_run_adjoint", "lmc_adjoint_contract"]
 
 _lib = None
 
@@ -151,6 +159,14 @@ def lib():
     L.lmc_run_noalloc.argtypes = [C.POINTER(SceneDesc), C.c_uint64, C.c_uint64, C.c_uint64,
                                   C.POINTER(RunOpts), vp, C.POINTER(Stats)]
     L.lmc_run_noalloc.restype = C.c_int
+    L.lmc_adjoint_layout.argtypes = [vp, C.POINTER(AdjointOpts), C.POINTER(C.c_size_t),
+                                     C.POINTER(C.c_int)]
+    L.lmc_adjoint_layout.restype = C.c_int
+    L.lmc_run_adjoint.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(RunOpts),
+                                  C.POINTER(AdjointOpts), vp, vp, C.POINTER(Stats)]
+    L.lmc_run_adjoint.restype = C.c_int
+    L.lmc_adjoint_contract.argtypes = [vp, vp, C.c_size_t, C.c_int, vp, vp]
+    L.lmc_adjoint_contract.restype = C.c_int
     _lib = L
     return L
 
