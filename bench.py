@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--batch-photons", type=int, default=0)
     ap.add_argument("--variant-steps", type=int, default=2,
                     help="timed steps of the FP64 and FP32+adjoint variants (0: skip them)")
+    ap.add_argument("--precision-report", action="store_true",
+                    help="instead of timing: FP32 tallies against FP64 on the same random "
+                         "numbers, per sensor, for the named workloads")
     return ap.parse_args()
 
 
@@ -420,8 +423,60 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
     return out
 
 
+def precision_report(args):
+    """Per sensor: FP32 transport (u24 stream) against FP64 transport on the same u24
+    numbers (stream_format=1), i.e. precision error alone, next to the Monte Carlo
+    noise of the same tally (FP64 on two independent seeds).  One JSON line per
+    workload."""
+    import numpy as np
+    import torch
+
+    import luminis_mc_b200 as lm
+    from luminis_mc_b200 import workloads as W
+    from luminis_mc_b200.device import DeviceRun
+
+    torch.cuda.set_device(0)
+    cases = [("mie_cbs_small", W.mie_cbs_small(1_000_000, 12345)),
+             ("bilayer_rgd_mie", W.bilayer_rgd_mie(10_000_000, 12345)),
+             ("mie_long_paths_linear", W.mie_long_paths(200_000, 12345)),
+             ("mie_long_paths_circular", W.mie_long_paths(200_000, 12345, circular=True))]
+    for name, spec in cases:
+        cfg, _, keep = W.build(lm, spec)
+        n, seed = int(spec["n_photons"]), int(spec["seed"])
+        res = {}
+        for key, prec, fmt, sd in (("fp32", "fp32", 0, seed), ("fp64", "fp64", 1, seed),
+                                   ("fp64_other_seed", "fp64", 1, seed + 1)):
+            run = DeviceRun(cfg)
+            st, _ = run.run(n, sd, precision=prec, stream_format=fmt)
+            res[key] = ([t.copy() for t in run.host_tallies()], st)
+            run.close()
+        sensors = []
+        for i, s in enumerate(spec["sensors"]):
+            a, b, c = res["fp32"][0][i], res["fp64"][0][i], res["fp64_other_seed"][0][i]
+            comps = []
+            for q in range(b.shape[0]):
+                bq = b[q].ravel()
+                scale = float(np.abs(bq).max()) or 1.0
+                l2 = float(np.linalg.norm(bq)) or 1.0
+                comps.append({
+                    "max_abs_err_of_max": float(np.abs(a[q].ravel() - bq).max()) / scale,
+                    "rel_l2_err": float(np.linalg.norm(a[q].ravel() - bq)) / l2,
+                    "rel_l2_mc_noise": float(np.linalg.norm(c[q].ravel() - bq)) / l2,
+                    "total_rel_err": float(abs(a[q].sum() - bq.sum()) / (abs(bq.sum()) or 1.0))})
+            sensors.append({"sensor": s["kind"], "components": comps})
+        line = {"workload": name, "photons": n, "seed": seed,
+                "events_fp32": res["fp32"][1]["events"], "events_fp64": res["fp64"][1]["events"],
+                "hits_fp32": res["fp32"][1]["hits"][:len(spec["sensors"])],
+                "hits_fp64": res["fp64"][1]["hits"][:len(spec["sensors"])],
+                "sensors": sensors}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.precision_report:
+        precision_report(args)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
     else:

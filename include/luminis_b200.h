@@ -152,6 +152,9 @@ typedef struct lmc_run_opts {
   void *records;                /* optional device array of n_photons lmc_record       */
   void *stream;                 /* cudaStream_t to launch on; NULL: the handle's own   */
   uint64_t batch_photons;       /* photons per transport batch (hit-queue mode); 0: 8M */
+  int stream_format;            /* 0: u24 for FP32, u53 for FP64; 1: u24 for both (an FP64
+                                   run on the FP32 run's numbers: precision alone)      */
+  int pad;
 } lmc_run_opts;
 
 /* Final state of one photon, written when opts.records is set (the same layout as

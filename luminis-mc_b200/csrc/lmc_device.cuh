@@ -134,6 +134,8 @@ struct RunParams {
   int adj_K, adj_radial_sensor, adj_radial_bins, adj_pad;
   double adj_radial_max;
   unsigned long long adj_cbs_off[LMC_MAX_SENSORS];
+  int stream_u24;                        // binary64 transport drawing u24 values
+  int pad2;
 };
 
 }  // namespace dev

@@ -126,10 +126,15 @@ __device__ __noinline__ uint4 philox_block(uint32_t block, uint32_t p_lo, uint32
   return make_uint4(c0, c1, c2, c3);
 }
 
-// log2(draws per block): u24 takes one 32-bit word per draw, u53 two.
-template <typename R> struct DrawsPerBlock;
-template <> struct DrawsPerBlock<float> { static constexpr uint32_t kLog2 = 2; };
-template <> struct DrawsPerBlock<double> { static constexpr uint32_t kLog2 = 1; };
+// log2(draws per block): u24 takes one 32-bit word per draw, u53 two.  binary32
+// transport always draws u24; binary64 transport draws u53, or u24 when the run asks
+// for it (the same numbers as a binary32 run, to measure precision alone).
+template <typename R> __device__ __forceinline__ uint32_t draw_log2(const RunParams &rp);
+template <> __device__ __forceinline__ uint32_t draw_log2<float>(const RunParams &) { return 2u; }
+template <> __device__ __forceinline__ uint32_t draw_log2<double>(const RunParams &rp)
+{
+  return rp.stream_u24 ? 2u : 1u;
+}
 
 __device__ __forceinline__ void rng_reset(Rng &g, unsigned long long index)
 {
@@ -142,7 +147,7 @@ __device__ __forceinline__ void rng_reset(Rng &g, unsigned long long index)
 // Make sure the block after the current one is generated (call while converged).
 template <typename R> __device__ __forceinline__ void rng_prefetch(Rng &g, const RunParams &rp)
 {
-  constexpr uint32_t L = DrawsPerBlock<R>::kLog2;
+  const uint32_t L = draw_log2<R>(rp);
   if (!(g.state & 1u)) {
     const uint4 b = philox_block(g.draw >> L, g.p_lo, g.p_hi, rp.key0, rp.key1);
     g.c0 = b.x; g.c1 = b.y; g.c2 = b.z; g.c3 = b.w;
@@ -160,8 +165,8 @@ template <typename R> __device__ __forceinline__ void rng_prefetch(Rng &g, const
 template <typename R> __device__ __forceinline__ void rng_words(Rng &g, const RunParams &rp,
                                                                 uint32_t &lo, uint32_t &hi)
 {
-  constexpr uint32_t L = DrawsPerBlock<R>::kLog2;
-  constexpr uint32_t M = (1u << L) - 1u;
+  const uint32_t L = draw_log2<R>(rp);
+  const uint32_t M = (1u << L) - 1u;
   if (!(g.state & 1u)) {                    // look-ahead exhausted inside one event
     const uint4 b = philox_block(g.draw >> L, g.p_lo, g.p_hi, rp.key0, rp.key1);
     g.c0 = b.x; g.c1 = b.y; g.c2 = b.z; g.c3 = b.w;
@@ -195,6 +200,8 @@ template <> __device__ __forceinline__ double uniform<double>(Rng &g, const RunP
 {
   uint32_t lo, hi;
   rng_words<double>(g, rp, lo, hi);
+  if (rp.stream_u24)                          // exactly the binary32 run's value
+    return (double)(__uint2float_rn(2u * (lo >> 9) + 1u) * 5.9604644775390625e-8f);
   const unsigned long long w = ((unsigned long long)hi << 32) | lo;
   return __ull2double_rn(2ull * (w >> 12) + 1ull) * 1.1102230246251565e-16;   // 2^-53
 }

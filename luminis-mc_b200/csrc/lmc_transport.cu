@@ -533,6 +533,9 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   rp.scratch = h->d_scratch;
   rp.cbs_mask = h->cbs_mask;
   const bool fp32 = opts->precision == LMC_PRECISION_FP32;
+  if (opts->stream_format != 0 && opts->stream_format != 1)
+    return fail(LMC_ERR_INVALID, "stream_format must be 0 or 1");
+  rp.stream_u24 = (!fp32 && opts->stream_format == 1) ? 1 : 0;
   const int block = opts->block_size > 0 ? opts->block_size : dev::kBlock;
   if (block % 32 != 0 || block > dev::kBlock)
     return fail(LMC_ERR_INVALID, "block_size must be a multiple of 32 and at most 256");
@@ -1054,6 +1057,9 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
   rp.scratch = d_counters;
   rp.cbs_mask = cbs_mask;
   const bool fp32 = opts->precision == LMC_PRECISION_FP32;
+  if (opts->stream_format != 0 && opts->stream_format != 1)
+    return fail(LMC_ERR_INVALID, "stream_format must be 0 or 1");
+  rp.stream_u24 = (!fp32 && opts->stream_format == 1) ? 1 : 0;
   const int block = dev::kBlock;
   const void *tk = fp32 ? (queued ? (const void *)dev::transport_kernel<float, true, 2>
                                   : (const void *)dev::transport_kernel<float, false, 1>)

@@ -205,7 +205,8 @@ class Transport:
             pass
 
     def opts(self, precision="fp32", max_events=None, track_reverse_paths=None, block_size=0,
-             blocks_per_sm=0, records_ptr=None, stream=None, batch_photons=0) -> N.RunOpts:
+             blocks_per_sm=0, records_ptr=None, stream=None, batch_photons=0,
+             stream_format=0) -> N.RunOpts:
         if precision not in N.PRECISION:
             raise ValueError("precision must be 'fp32' or 'fp64'")
         c = self.config
@@ -219,6 +220,7 @@ class Transport:
         o.records = records_ptr
         o.stream = stream
         o.batch_photons = int(batch_photons)
+        o.stream_format = int(stream_format)
         return o
 
     def run_host(self, tallies: np.ndarray, n_photons: int, seed: int, begin: int = 0,

@@ -203,3 +203,21 @@ def test_device_then_host_run_on_one_handle(cuda):
     for d, h in zip(run.host_tallies(), run.transport.split(host)):
         np.testing.assert_allclose(d, 2 * h, rtol=FP64_RTOL, atol=FP64_RTOL * np.abs(h).max())
     run.close()
+
+
+@pytest.mark.parametrize("spec", list(small_specs())[:3], ids=lambda s: s["name"])
+def test_fp64_on_the_u24_stream_replays_the_oracle(spec, cuda):
+    """stream_format=1: binary64 transport on the binary32 run's numbers (u24) is the
+    oracle's binary64 replay of that stream, so FP32-vs-FP64 comparisons on it measure
+    precision alone."""
+    cfg, _, keep = W.build(lm, spec)
+    run = DeviceRun(cfg)
+    n = cfg.n_photons
+    stats, rec = run.run(n, cfg.seed, precision="fp64", records=True, stream_format=1)
+    ref = O.Oracle(spec).run(n, cfg.seed, rng="philox_u24", records=True)
+    same, worst = _compare_records(rec, ref.records, FP64_RTOL)
+    assert same.all(), f"{(~same).sum()} photons differ in events/draws/fate"
+    for f, e in worst.items():
+        assert e < FP64_RTOL, f"{f}: {e}"
+    assert stats["draws"] == ref.stats["draws"]
+    run.close()
