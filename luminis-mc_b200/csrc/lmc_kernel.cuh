@@ -89,22 +89,28 @@ template <> __device__ __forceinline__ double sc_top<double>(const Scene &s) { r
 
 // ------------------------------------------------------------------------ RNG
 // Philox4x32-10 (Salmon et al., SC'11); stream contract in luminis_b200.h.
-// Each photon keeps the block holding its next draw (`cur`) and the block after
-// it (`nxt`).  The look-ahead block is generated by rng_prefetch() at the top of
-// every event, where the whole warp is converged, instead of at the draw that
-// empties the current block; lanes sit at different stream positions, so a
-// refill on demand would run the ten Philox rounds at almost every draw site
-// with a few lanes active.
-struct Rng {
+// A photon's stream is generated a Philox block (4 words) at a time into a ring of
+// kRing words; draw d reads word d (u24) or words 2d, 2d+1 (u53).  The transport
+// kernel keeps the ring in shared memory (one column per thread) and tops it up at
+// the top of every event, where the warp is converged, so the azimuth rejection
+// loop -- whose trial count differs from lane to lane -- finds its numbers already
+// generated instead of running the ten Philox rounds with a few lanes active.
+constexpr uint32_t kRing = 16;
+
+template <int kStride> struct RngT {
   uint32_t p_lo, p_hi;
   uint32_t draw;               // draws consumed (stream position)
-  uint32_t c0, c1, c2, c3;     // block (draw >> log2(per block))
-  uint32_t n0, n1, n2, n3;     // the block after it
-  uint32_t state;              // bit 0: cur valid, bit 1: nxt valid
+  uint32_t filled;             // words generated so far (a multiple of 4)
+  uint32_t *ring;              // kRing words, kStride apart
+  __device__ __forceinline__ uint32_t &word(uint32_t w) const
+  {
+    return ring[(w & (kRing - 1u)) * kStride];
+  }
 };
+using Rng = RngT<kBlock>;
 
-// One copy of the ten rounds (called from three places; keeping a single copy
-// keeps the event loop small enough for the instruction cache).
+// One copy of the ten rounds (a call keeps the event loop small enough for the
+// instruction cache).
 __device__ __noinline__ uint4 philox_block(uint32_t block, uint32_t p_lo, uint32_t p_hi,
                                            uint32_t key0, uint32_t key1)
 {
@@ -126,77 +132,69 @@ __device__ __noinline__ uint4 philox_block(uint32_t block, uint32_t p_lo, uint32
   return make_uint4(c0, c1, c2, c3);
 }
 
-// log2(draws per block): u24 takes one 32-bit word per draw, u53 two.  binary32
-// transport always draws u24; binary64 transport draws u53, or u24 when the run asks
-// for it (the same numbers as a binary32 run, to measure precision alone).
-template <typename R> __device__ __forceinline__ uint32_t draw_log2(const RunParams &rp);
-template <> __device__ __forceinline__ uint32_t draw_log2<float>(const RunParams &) { return 2u; }
-template <> __device__ __forceinline__ uint32_t draw_log2<double>(const RunParams &rp)
+// Words per draw: u24 takes one 32-bit word, u53 two.  binary32 transport always
+// draws u24; binary64 transport draws u53, or u24 when the run asks for it (the
+// same numbers as a binary32 run, to measure precision alone).
+template <typename R> __device__ __forceinline__ uint32_t words_per_draw(const RunParams &rp);
+template <> __device__ __forceinline__ uint32_t words_per_draw<float>(const RunParams &) { return 1u; }
+template <> __device__ __forceinline__ uint32_t words_per_draw<double>(const RunParams &rp)
 {
-  return rp.stream_u24 ? 2u : 1u;
+  return rp.stream_u24 ? 1u : 2u;
 }
 
-__device__ __forceinline__ void rng_reset(Rng &g, unsigned long long index)
+template <int S> __device__ __forceinline__ void rng_reset(RngT<S> &g, unsigned long long index)
 {
   g.p_lo = (uint32_t)index;
   g.p_hi = (uint32_t)(index >> 32);
   g.draw = 0;
-  g.state = 0;
+  g.filled = 0;
 }
 
-// Make sure the block after the current one is generated (call while converged).
-template <typename R> __device__ __forceinline__ void rng_prefetch(Rng &g, const RunParams &rp)
+// Generate the next block into the ring (words filled .. filled + 3).
+template <int S> __device__ __forceinline__ void rng_fill(RngT<S> &g, const RunParams &rp)
 {
-  const uint32_t L = draw_log2<R>(rp);
-  if (!(g.state & 1u)) {
-    const uint4 b = philox_block(g.draw >> L, g.p_lo, g.p_hi, rp.key0, rp.key1);
-    g.c0 = b.x; g.c1 = b.y; g.c2 = b.z; g.c3 = b.w;
-    g.state |= 1u;
-  }
-  if (!(g.state & 2u)) {
-    const uint4 b = philox_block((g.draw >> L) + 1u, g.p_lo, g.p_hi, rp.key0, rp.key1);
-    g.n0 = b.x; g.n1 = b.y; g.n2 = b.z; g.n3 = b.w;
-    g.state |= 2u;
-  }
+  const uint4 b = philox_block(g.filled >> 2, g.p_lo, g.p_hi, rp.key0, rp.key1);
+  g.word(g.filled) = b.x;
+  g.word(g.filled + 1u) = b.y;
+  g.word(g.filled + 2u) = b.z;
+  g.word(g.filled + 3u) = b.w;
+  g.filled += 4u;
 }
 
-// Next word of the stream: slot `draw & (per block - 1)` of the current block;
-// moving past the block's end promotes the look-ahead block.
-template <typename R> __device__ __forceinline__ void rng_words(Rng &g, const RunParams &rp,
-                                                                uint32_t &lo, uint32_t &hi)
+// Top the ring up (call while converged): up to two blocks, as long as a whole
+// block fits behind the words not yet consumed.
+template <typename R, int S> __device__ __forceinline__ void rng_prefetch(RngT<S> &g, const RunParams &rp)
 {
-  const uint32_t L = draw_log2<R>(rp);
-  const uint32_t M = (1u << L) - 1u;
-  if (!(g.state & 1u)) {                    // look-ahead exhausted inside one event
-    const uint4 b = philox_block(g.draw >> L, g.p_lo, g.p_hi, rp.key0, rp.key1);
-    g.c0 = b.x; g.c1 = b.y; g.c2 = b.z; g.c3 = b.w;
-    g.state |= 1u;
-  }
-  const uint32_t slot = g.draw & M;
-  if (L == 2) {
-    lo = slot == 0u ? g.c0 : slot == 1u ? g.c1 : slot == 2u ? g.c2 : g.c3;
-    hi = 0u;
-  } else {
-    lo = slot == 0u ? g.c0 : g.c2;
-    hi = slot == 0u ? g.c1 : g.c3;
-  }
+  const uint32_t used = g.draw * words_per_draw<R>(rp);
+#pragma unroll 1
+  for (int i = 0; i < 2; ++i)
+    if (g.filled + 4u <= used + kRing)
+      rng_fill(g, rp);
+}
+
+// Words of the next draw; generates a block only if the ring ran dry.
+template <typename R, int S> __device__ __forceinline__ void rng_words(RngT<S> &g, const RunParams &rp,
+                                                                       uint32_t &lo, uint32_t &hi)
+{
+  const uint32_t wpd = words_per_draw<R>(rp);
+  const uint32_t w0 = g.draw * wpd;
+  if (w0 + wpd > g.filled)
+    rng_fill(g, rp);
+  lo = g.word(w0);
+  hi = wpd == 2u ? g.word(w0 + 1u) : 0u;
   g.draw++;
-  if ((g.draw & M) == 0u) {                 // current block used up
-    g.c0 = g.n0; g.c1 = g.n1; g.c2 = g.n2; g.c3 = g.n3;
-    g.state = (g.state & 2u) ? 1u : 0u;
-  }
 }
 
-template <typename R> __device__ __forceinline__ R uniform(Rng &g, const RunParams &rp);
+template <typename R, int S> __device__ __forceinline__ R uniform(RngT<S> &g, const RunParams &rp);
 
-template <> __device__ __forceinline__ float uniform<float>(Rng &g, const RunParams &rp)   // "u24"
+template <> __device__ __forceinline__ float uniform<float, kBlock>(Rng &g, const RunParams &rp)   // "u24"
 {
   uint32_t w, unused;
   rng_words<float>(g, rp, w, unused);
   return __uint2float_rn(2u * (w >> 9) + 1u) * 5.9604644775390625e-8f;   // 2^-24
 }
 
-template <> __device__ __forceinline__ double uniform<double>(Rng &g, const RunParams &rp)  // "u53"
+template <> __device__ __forceinline__ double uniform<double, kBlock>(Rng &g, const RunParams &rp)  // "u53"
 {
   uint32_t lo, hi;
   rng_words<double>(g, rp, lo, hi);
@@ -204,6 +202,23 @@ template <> __device__ __forceinline__ double uniform<double>(Rng &g, const RunP
     return (double)(__uint2float_rn(2u * (lo >> 9) + 1u) * 5.9604644775390625e-8f);
   const unsigned long long w = ((unsigned long long)hi << 32) | lo;
   return __ull2double_rn(2ull * (w >> 12) + 1ull) * 1.1102230246251565e-16;   // 2^-53
+}
+
+template <> __device__ __forceinline__ float uniform<float, 1>(RngT<1> &g, const RunParams &rp)
+{
+  uint32_t w, unused;
+  rng_words<float>(g, rp, w, unused);
+  return __uint2float_rn(2u * (w >> 9) + 1u) * 5.9604644775390625e-8f;
+}
+
+template <> __device__ __forceinline__ double uniform<double, 1>(RngT<1> &g, const RunParams &rp)
+{
+  uint32_t lo, hi;
+  rng_words<double>(g, rp, lo, hi);
+  if (rp.stream_u24)
+    return (double)(__uint2float_rn(2u * (lo >> 9) + 1u) * 5.9604644775390625e-8f);
+  const unsigned long long w = ((unsigned long long)hi << 32) | lo;
+  return __ull2double_rn(2ull * (w >> 12) + 1ull) * 1.1102230246251565e-16;
 }
 
 // --------------------------------------------------------------------- photon
@@ -216,9 +231,6 @@ template <typename R> struct Photon {
   R pen;                       // penetration depth (records only)
   uint32_t events;
   int layer, last_med;
-  R rn[3];                     // position of the newest scatter (r_n)
-  R Pn1[9];                    // frame before the newest scatter (P_{n-1})
-  Cx<R> T[4];                  // matrix_T_raw: normalised interior Jones product
   Rng rng;
   __device__ __forceinline__ unsigned long long index() const
   {
@@ -226,10 +238,17 @@ template <typename R> struct Photon {
   }
 };
 
-// Per-thread CBS state that only a detection reads, in shared memory.
+// Per-thread CBS state, in shared memory (one column per thread): the reverse
+// path reads it only at a detection, and keeping it out of registers lets more
+// warps share an SM.  Lives in dynamic shared memory (the binary64 layout exceeds
+// the 48 KB static limit).
 template <typename R> struct Side {
   R first[12][kBlock];         // r_1 (3), then P1 rows m_1, n_1, s_1 (9)
   R last[6][kBlock];           // S2, S1 (re, im) and cos, sin(phi) of the newest scatter
+  R pn1[9][kBlock];            // frame before the newest scatter (P_{n-1})
+  R rn[3][kBlock];             // position of the newest scatter (r_n)
+  R T[8][kBlock];              // matrix_T_raw: normalised interior Jones product (re, im)
+  uint32_t ring[kRing][kBlock];  // the photon's generated Philox words (see RngT)
   int first_med[kBlock];
 };
 
@@ -563,8 +582,8 @@ __device__ __forceinline__ float exit_theta(float sx, float sy, float sz)
 // ---------------------------------------------------------------- source
 // Laser::emit_photon's random part (src/laser.cpp:11-28, :42-75, :77-99): launch
 // x, y and emission time, drawn from the photon's stream starting at draw 0.
-template <typename R>
-__device__ void source_sample(const Laser &L, Rng &g, const RunParams &rp, double &x, double &y,
+template <typename R, int S>
+__device__ void source_sample(const Laser &L, RngT<S> &g, const RunParams &rp, double &x, double &y,
                               double &t)
 {
   x = L.pos[0];
@@ -610,7 +629,9 @@ __device__ __noinline__ double emission_time(const Laser &L, RunParams rp, unsig
 {
   if (L.temporal == 0)
     return L.time_offset * 1e-3;
-  Rng g;
+  uint32_t words[kRing];                  // a private ring (local memory; rare path)
+  RngT<1> g;
+  g.ring = words;
   rng_reset(g, index);
   double x, y, t;
   source_sample<R>(L, g, rp, x, y, t);
@@ -978,18 +999,18 @@ __device__ __forceinline__ void fill_hit(const Photon<R> &ph, const Side<R> &sid
   for (int j = 0; j < 9; ++j) {
     h.P[j] = ph.P[j];
     h.P1[j] = side.first[3 + j][tid];
-    h.Pn1[j] = ph.Pn1[j];
+    h.Pn1[j] = side.pn1[j][tid];
   }
   h.Em = ph.Em;
   h.En = ph.En;
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     h.r1[j] = side.first[j][tid];
-    h.rn[j] = ph.rn[j];
+    h.rn[j] = side.rn[j][tid];
   }
 #pragma unroll
   for (int q = 0; q < 4; ++q)
-    h.T[q] = ph.T[q];
+    h.T[q] = {side.T[2 * q][tid], side.T[2 * q + 1][tid]};
 }
 
 // Append a hit to the queue (warp-aggregated slot).  Only the fields the
@@ -1036,17 +1057,17 @@ __device__ __forceinline__ void enqueue_hit(const Scene &sc, const RunParams &rp
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       r[(kQR1 + j) * C + slot] = side.first[j][tid];
-      r[(kQRn + j) * C + slot] = ph.rn[j];
+      r[(kQRn + j) * C + slot] = side.rn[j][tid];
     }
 #pragma unroll
     for (int j = 0; j < 9; ++j) {
       r[(kQP1 + j) * C + slot] = side.first[3 + j][tid];
-      r[(kQPn1 + j) * C + slot] = ph.Pn1[j];
+      r[(kQPn1 + j) * C + slot] = side.pn1[j][tid];
     }
 #pragma unroll
     for (int qd = 0; qd < 4; ++qd) {
-      r[(kQT + 2 * qd) * C + slot] = ph.T[qd].re;
-      r[(kQT + 2 * qd + 1) * C + slot] = ph.T[qd].im;
+      r[(kQT + 2 * qd) * C + slot] = side.T[2 * qd][tid];
+      r[(kQT + 2 * qd + 1) * C + slot] = side.T[2 * qd + 1][tid];
     }
   }
   if (kAdj)
@@ -1125,14 +1146,14 @@ __device__ void init_photon(const Scene &sc, const RunParams &rp, Photon<R> &ph,
   ph.events = 0;
   ph.layer = layer_index_at<R>(sc, ph.pz);
   ph.last_med = 0;
-  ph.rn[0] = ph.px; ph.rn[1] = ph.py; ph.rn[2] = ph.pz;
+  const int tid = threadIdx.x;                              // r_1 = r_n = launch, P1 = Pn1 = P0
+  side.rn[0][tid] = ph.px; side.rn[1][tid] = ph.py; side.rn[2][tid] = ph.pz;
 #pragma unroll
   for (int j = 0; j < 9; ++j)
-    ph.Pn1[j] = ph.P[j];
+    side.pn1[j][tid] = ph.P[j];
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
-    ph.T[q] = {R(q == 0 || q == 3 ? 1 : 0), R(0)};
-  const int tid = threadIdx.x;                              // r_1 = launch, P1 = P0
+  for (int q = 0; q < 8; ++q)
+    side.T[q][tid] = R(q == 0 || q == 6 ? 1 : 0);
   side.first[0][tid] = ph.px; side.first[1][tid] = ph.py; side.first[2][tid] = ph.pz;
 #pragma unroll
   for (int j = 0; j < 9; ++j)
@@ -1254,12 +1275,15 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   if (kAdj)
     flight_event<R>(sc, fl, med_idx, ct);
   // frame update P <- A(theta, phi) P (src/simulation.cpp:438-453); P_{n-1} <- old P
+  if (rp.track_reverse) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < 9; ++j)
+      side.pn1[j][tid] = ph.P[j];
+  }
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     const R mj = ph.P[j], nj = ph.P[3 + j], sj = ph.P[6 + j];
-    ph.Pn1[j] = mj;
-    ph.Pn1[3 + j] = nj;
-    ph.Pn1[6 + j] = sj;
     ph.P[j] = ct * cp * mj + ct * sp * nj - st * sj;
     ph.P[3 + j] = -sp * mj + cp * nj;
     ph.P[6 + j] = st * cp * mj + st * sp * nj + ct * sj;
@@ -1286,7 +1310,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
         side.first[3 + j][tid] = ph.P[j];
       side.first_med[tid] = med_idx;
     }
-    ph.rn[0] = ph.px; ph.rn[1] = ph.py; ph.rn[2] = ph.pz;
+    side.rn[0][tid] = ph.px; side.rn[1][tid] = ph.py; side.rn[2][tid] = ph.pz;
     ph.last_med = med_idx;
     if (evt >= 3) {
       // T <- normalise(J_{n-1} T), J_{n-1} = diag(S2, S1) R(phi) of the previous event
@@ -1294,16 +1318,19 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
       const Cx<R> pS1 = {side.last[2][tid], side.last[3][tid]};
       const R pc = side.last[4][tid], ps = side.last[5][tid];
       const Cx<R> B00 = cscale(pS2, pc), B01 = cscale(pS2, ps), B10 = cscale(pS1, -ps), B11 = cscale(pS1, pc);
-      Cx<R> t0 = cadd(cmul(B00, ph.T[0]), cmul(B01, ph.T[2]));
-      Cx<R> t1 = cadd(cmul(B00, ph.T[1]), cmul(B01, ph.T[3]));
-      Cx<R> t2 = cadd(cmul(B10, ph.T[0]), cmul(B11, ph.T[2]));
-      Cx<R> t3 = cadd(cmul(B10, ph.T[1]), cmul(B11, ph.T[3]));
+      const Cx<R> T0 = {side.T[0][tid], side.T[1][tid]}, T1 = {side.T[2][tid], side.T[3][tid]};
+      const Cx<R> T2 = {side.T[4][tid], side.T[5][tid]}, T3 = {side.T[6][tid], side.T[7][tid]};
+      Cx<R> t0 = cadd(cmul(B00, T0), cmul(B01, T2));
+      Cx<R> t1 = cadd(cmul(B00, T1), cmul(B01, T3));
+      Cx<R> t2 = cadd(cmul(B10, T0), cmul(B11, T2));
+      Cx<R> t3 = cadd(cmul(B10, T1), cmul(B11, T3));
       const R frob = m_sqrt(cnorm(t0) + cnorm(t1) + cnorm(t2) + cnorm(t3));
       if (frob > tiny<R>()) {
         const R inv = R(1) / frob;
         t0 = cscale(t0, inv); t1 = cscale(t1, inv); t2 = cscale(t2, inv); t3 = cscale(t3, inv);
       }
-      ph.T[0] = t0; ph.T[1] = t1; ph.T[2] = t2; ph.T[3] = t3;
+      side.T[0][tid] = t0.re; side.T[1][tid] = t0.im; side.T[2][tid] = t1.re; side.T[3][tid] = t1.im;
+      side.T[4][tid] = t2.re; side.T[5][tid] = t2.im; side.T[6][tid] = t3.re; side.T[7][tid] = t3.im;
     }
     if (evt >= 2) {
       side.last[0][tid] = S2.re; side.last[1][tid] = S2.im;
@@ -1346,7 +1373,7 @@ __device__ void write_record(const Scene &sc, const RunParams &rp, const Photon<
     r.n[j] = ph.P[3 + j];
     r.dir[j] = ph.P[6 + j];
     r.r1[j] = side.first[j][tid];
-    r.rn[j] = ph.rn[j];
+    r.rn[j] = side.rn[j][tid];
   }
   r.E[0] = ph.Em.re; r.E[1] = ph.Em.im; r.E[2] = ph.En.re; r.E[3] = ph.En.im;
 }
@@ -1362,18 +1389,24 @@ __device__ __forceinline__ void load_scene(unsigned char *s_raw, const Scene *g_
 
 // kMinBlocks > 1 asks the compiler to fit that many 256-thread blocks per SM
 // (register cap 65536 / (256 kMinBlocks)); lmc_run picks the variant.
-// kAdj: likelihood-ratio run; the scores take adj_K * kBlock R of dynamic shared
-// memory (queued mode only).
+// Dynamic shared memory of a transport block: the Side arrays, then (kAdj) the
+// likelihood-ratio scores, adj_K * kBlock R.
+template <typename R> __host__ __device__ constexpr size_t side_bytes()
+{
+  return (sizeof(Side<R>) + 15) & ~size_t(15);
+}
+
+// kAdj: likelihood-ratio run (queued mode only).
 template <typename R, bool kQueue, int kMinBlocks, bool kAdj = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
   __shared__ __align__(16) unsigned char s_raw[sizeof(Scene)];
-  __shared__ Side<R> side;
   __shared__ unsigned long long s_hits[LMC_MAX_SENSORS];
   __shared__ unsigned long long s_fate[7];
   extern __shared__ __align__(16) unsigned char s_dyn[];
+  Side<R> &side = *reinterpret_cast<Side<R> *>(s_dyn);
   Flight<R> fl;
-  fl.score = reinterpret_cast<R *>(s_dyn) + threadIdx.x;
+  fl.score = reinterpret_cast<R *>(s_dyn + side_bytes<R>()) + threadIdx.x;
   load_scene(s_raw, g_scene);
   if (threadIdx.x < LMC_MAX_SENSORS)
     s_hits[threadIdx.x] = 0;
@@ -1384,6 +1417,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
   const unsigned lane = threadIdx.x & 31u;
   Counters cnt = {0, 0, 0};
   Photon<R> ph;
+  ph.rng.ring = &side.ring[0][threadIdx.x];
   bool alive = false, done = false;
   for (;;) {
     const unsigned need = __ballot_sync(kFull, !alive && !done);

@@ -540,7 +540,8 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   if (block % 32 != 0 || block > dev::kBlock)
     return fail(LMC_ERR_INVALID, "block_size must be a multiple of 32 and at most 256");
   const size_t rbytes = fp32 ? sizeof(float) : sizeof(double);
-  size_t dyn_transport = 0, dyn_tally = 0;
+  size_t dyn_transport = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
+  size_t dyn_tally = 0;
   if (adj) {
     size_t n_out = 0;
     const lmc_status ls = adjoint_layout(h, adj, &n_out, rp.adj_cbs_off);
@@ -554,13 +555,13 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     rp.adj_radial_sensor = adj->radial_sensor;
     rp.adj_radial_bins = adj->radial_bins;
     rp.adj_radial_max = adj->radial_max;
-    dyn_transport = (size_t)rp.adj_K * dev::kBlock * rbytes;
+    dyn_transport += (size_t)rp.adj_K * dev::kBlock * rbytes;
     if (adj->radial_sensor >= 0)
       dyn_tally = (size_t)(1 + rp.adj_K) * (adj->radial_bins + 1) * sizeof(double);
   }
-  // binary32 queued transport: a 2-block (<=128 registers) and a 3-block (<=85
-  // registers, some spills) variant; blocks_per_sm >= 3 selects the latter
-  const bool three = fp32 && h->queued && opts->blocks_per_sm >= 3 && !adj;
+  // binary32 queued transport: a 3-block (<=85 registers, the default) and a
+  // 2-block (<=128 registers) variant; blocks_per_sm == 1 or 2 selects the latter
+  const bool three = fp32 && h->queued && !adj && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
   const void *tk =
       adj ? (fp32 ? (const void *)dev::transport_kernel<float, true, 2, true>
                   : (const void *)dev::transport_kernel<double, true, 1, true>)
@@ -569,8 +570,8 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
                               : (const void *)dev::transport_kernel<float, false, 1>)
                  : (h->queued ? (const void *)dev::transport_kernel<double, true, 1>
                               : (const void *)dev::transport_kernel<double, false, 1>);
+  LMC_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_transport));
   if (adj) {
-    LMC_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_transport));
     const void *tl = fp32 ? (const void *)dev::tally_kernel<float, true>
                           : (const void *)dev::tally_kernel<double, true>;
     LMC_CUDA(cudaFuncSetAttribute(tl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_tally));
@@ -637,16 +638,16 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
         dev::transport_kernel<double, true, 1, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
     } else if (fp32) {
       if (h->queued && three)
-        dev::transport_kernel<float, true, 3><<<grid, block, 0, stream>>>(h->d_scene, rp);
+        dev::transport_kernel<float, true, 3><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
       else if (h->queued)
-        dev::transport_kernel<float, true, 2><<<grid, block, 0, stream>>>(h->d_scene, rp);
+        dev::transport_kernel<float, true, 2><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
       else
-        dev::transport_kernel<float, false, 1><<<grid, block, 0, stream>>>(h->d_scene, rp);
+        dev::transport_kernel<float, false, 1><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
     } else {
       if (h->queued)
-        dev::transport_kernel<double, true, 1><<<grid, block, 0, stream>>>(h->d_scene, rp);
+        dev::transport_kernel<double, true, 1><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
       else
-        dev::transport_kernel<double, false, 1><<<grid, block, 0, stream>>>(h->d_scene, rp);
+        dev::transport_kernel<double, false, 1><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
     }
     LMC_CUDA(cudaGetLastError());
     if (stats)
@@ -1065,8 +1066,10 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
                                   : (const void *)dev::transport_kernel<float, false, 1>)
                         : (queued ? (const void *)dev::transport_kernel<double, true, 1>
                                   : (const void *)dev::transport_kernel<double, false, 1>);
+  const size_t dyn_transport = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
+  LMC_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_transport));
   int per_sm = 0;
-  LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tk, block, 0));
+  LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tk, block, dyn_transport));
   per_sm = std::max(per_sm, 1);
   unsigned long long batch = n_photons;
   if (queued && n_photons > 0) {
@@ -1095,14 +1098,14 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
         1ull, std::min<unsigned long long>((unsigned long long)sm_count * per_sm, (nb + block - 1) / block));
     if (fp32) {
       if (queued)
-        dev::transport_kernel<float, true, 2><<<grid, block, 0, stream>>>(d_scene, rp);
+        dev::transport_kernel<float, true, 2><<<grid, block, dyn_transport, stream>>>(d_scene, rp);
       else
-        dev::transport_kernel<float, false, 1><<<grid, block, 0, stream>>>(d_scene, rp);
+        dev::transport_kernel<float, false, 1><<<grid, block, dyn_transport, stream>>>(d_scene, rp);
     } else {
       if (queued)
-        dev::transport_kernel<double, true, 1><<<grid, block, 0, stream>>>(d_scene, rp);
+        dev::transport_kernel<double, true, 1><<<grid, block, dyn_transport, stream>>>(d_scene, rp);
       else
-        dev::transport_kernel<double, false, 1><<<grid, block, 0, stream>>>(d_scene, rp);
+        dev::transport_kernel<double, false, 1><<<grid, block, dyn_transport, stream>>>(d_scene, rp);
     }
     LMC_CUDA(cudaGetLastError());
     if (queued && s->n_sensors > 0) {
