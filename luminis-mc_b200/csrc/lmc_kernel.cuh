@@ -185,40 +185,36 @@ template <typename R, int S> __device__ __forceinline__ void rng_words(RngT<S> &
   g.draw++;
 }
 
-template <typename R, int S> __device__ __forceinline__ R uniform(RngT<S> &g, const RunParams &rp);
-
-template <> __device__ __forceinline__ float uniform<float, kBlock>(Rng &g, const RunParams &rp)   // "u24"
+// The uniform value of a draw's word(s): "u24" (2 (x >> 9) + 1) 2^-24 or "u53"
+// (2 (w >> 12) + 1) 2^-53 of the 64-bit word hi:lo; binary64 on the u24 stream
+// returns exactly the binary32 run's value.
+template <typename R> __device__ __forceinline__ R words_uniform(const RunParams &rp, uint32_t lo, uint32_t hi);
+template <> __device__ __forceinline__ float words_uniform<float>(const RunParams &, uint32_t w, uint32_t)
 {
-  uint32_t w, unused;
-  rng_words<float>(g, rp, w, unused);
   return __uint2float_rn(2u * (w >> 9) + 1u) * 5.9604644775390625e-8f;   // 2^-24
 }
-
-template <> __device__ __forceinline__ double uniform<double, kBlock>(Rng &g, const RunParams &rp)  // "u53"
+template <> __device__ __forceinline__ double words_uniform<double>(const RunParams &rp, uint32_t lo, uint32_t hi)
 {
-  uint32_t lo, hi;
-  rng_words<double>(g, rp, lo, hi);
-  if (rp.stream_u24)                          // exactly the binary32 run's value
+  if (rp.stream_u24)
     return (double)(__uint2float_rn(2u * (lo >> 9) + 1u) * 5.9604644775390625e-8f);
   const unsigned long long w = ((unsigned long long)hi << 32) | lo;
   return __ull2double_rn(2ull * (w >> 12) + 1ull) * 1.1102230246251565e-16;   // 2^-53
 }
 
-template <> __device__ __forceinline__ float uniform<float, 1>(RngT<1> &g, const RunParams &rp)
-{
-  uint32_t w, unused;
-  rng_words<float>(g, rp, w, unused);
-  return __uint2float_rn(2u * (w >> 9) + 1u) * 5.9604644775390625e-8f;
-}
-
-template <> __device__ __forceinline__ double uniform<double, 1>(RngT<1> &g, const RunParams &rp)
+template <typename R, int S> __device__ __forceinline__ R uniform(RngT<S> &g, const RunParams &rp)
 {
   uint32_t lo, hi;
-  rng_words<double>(g, rp, lo, hi);
-  if (rp.stream_u24)
-    return (double)(__uint2float_rn(2u * (lo >> 9) + 1u) * 5.9604644775390625e-8f);
-  const unsigned long long w = ((unsigned long long)hi << 32) | lo;
-  return __ull2double_rn(2ull * (w >> 12) + 1ull) * 1.1102230246251565e-16;
+  rng_words<R>(g, rp, lo, hi);
+  return words_uniform<R>(rp, lo, hi);
+}
+
+// Draw g.draw + k without consuming it; the caller has checked that the ring holds it.
+template <typename R, int S> __device__ __forceinline__ R peek_uniform(const RngT<S> &g, const RunParams &rp,
+                                                                       uint32_t k)
+{
+  const uint32_t wpd = words_per_draw<R>(rp);
+  const uint32_t w0 = (g.draw + k) * wpd;
+  return words_uniform<R>(rp, g.word(w0), wpd == 2u ? g.word(w0 + 1u) : 0u);
 }
 
 // --------------------------------------------------------------------- photon
@@ -1259,16 +1255,50 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   const R c = R(2) * (s2sq - s1sq) * e12;
   const R diff = a - b;
   const R Fmax = R(0.5) * (a + b) + R(0.5) * m_sqrt(diff * diff + c * c);
-  R cp, sp;
-  for (int trial = 0;; ++trial) {
-    if (trial == kMaxRejectionTrials)
-      return kError;
-    const R u1 = uniform<R>(ph.rng, rp);
-    m_sincospi(R(2) * u1, &sp, &cp);
-    const R F = a * cp * cp + b * sp * sp + c * cp * sp;
-    const R Fc = F > R(0) ? F : R(0);
-    if (uniform<R>(ph.rng, rp) * Fmax <= Fc)
-      break;
+  // The first kSpecTrials trials are evaluated together, from numbers the ring
+  // already holds, and the first accepted one is taken with only the draws up to it
+  // consumed: the same phi and the same stream position as trial-by-trial
+  // rejection, without a loop whose trip count differs from lane to lane.  Lanes
+  // that reject them all (or whose ring is short, at a photon's first event)
+  // continue one trial at a time.
+  R cp = R(1), sp = R(0);
+  int trial = 0;
+  {
+    constexpr int kSpec = sizeof(R) == 4 ? 3 : 2;
+    const uint32_t wpd = words_per_draw<R>(rp);
+    if (ph.rng.filled >= (ph.rng.draw + 2u * kSpec) * wpd) {
+      bool acc = false;
+      uint32_t take = 2u * kSpec;
+#pragma unroll
+      for (int t = 0; t < kSpec; ++t) {
+        const R u1 = peek_uniform<R>(ph.rng, rp, 2u * t);
+        const R u2 = peek_uniform<R>(ph.rng, rp, 2u * t + 1u);
+        R st_, ct_;
+        m_sincospi(R(2) * u1, &st_, &ct_);
+        const R F = a * ct_ * ct_ + b * st_ * st_ + c * ct_ * st_;
+        const R Fc = F > R(0) ? F : R(0);
+        if (!acc && u2 * Fmax <= Fc) {
+          cp = ct_;
+          sp = st_;
+          take = 2u * t + 2u;
+          acc = true;
+        }
+      }
+      ph.rng.draw += take;
+      trial = acc ? -1 : kSpec;
+    }
+  }
+  if (trial >= 0) {
+    for (;; ++trial) {
+      if (trial == kMaxRejectionTrials)
+        return kError;
+      const R u1 = uniform<R>(ph.rng, rp);
+      m_sincospi(R(2) * u1, &sp, &cp);
+      const R F = a * cp * cp + b * sp * sp + c * cp * sp;
+      const R Fc = F > R(0) ? F : R(0);
+      if (uniform<R>(ph.rng, rp) * Fmax <= Fc)
+        break;
+    }
   }
   R st, ct;
   m_sincos(theta, &st, &ct);
