@@ -1262,6 +1262,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   // that reject them all (or whose ring is short, at a photon's first event)
   // continue one trial at a time.
   R cp = R(1), sp = R(0);
+  R Facc = R(1);                 // F(phi) of the accepted trial (> 0: u > 0 accepted it)
   int trial = 0;
   {
     constexpr int kSpec = sizeof(R) == 4 ? 3 : 2;
@@ -1280,6 +1281,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
         if (!acc && u2 * Fmax <= Fc) {
           cp = ct_;
           sp = st_;
+          Facc = F;
           take = 2u * t + 2u;
           acc = true;
         }
@@ -1296,6 +1298,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
       m_sincospi(R(2) * u1, &sp, &cp);
       const R F = a * cp * cp + b * sp * sp + c * cp * sp;
       const R Fc = F > R(0) ? F : R(0);
+      Facc = F;
       if (uniform<R>(ph.rng, rp) * Fmax <= Fc)
         break;
     }
@@ -1318,13 +1321,11 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
     ph.P[3 + j] = -sp * mj + cp * nj;
     ph.P[6 + j] = st * cp * mj + st * sp * nj + ct * sj;
   }
-  // Jones update E <- (S R(phi)) E / sqrt(F) (src/simulation.cpp:456-492)
+  // Jones update E <- (S R(phi)) E / sqrt(F) (src/simulation.cpp:456-492); F(phi)
+  // is the density the rejection step just evaluated (the same quadratic form)
   {
     const Cx<R> Em = ph.Em, En = ph.En;
-    const R pc = cp * cp, ps = sp * sp;
-    const R F = e1sq * (s2sq * pc + s1sq * ps) + e2sq * (s2sq * ps + s1sq * pc) +
-                R(2) * e12 * (s2sq - s1sq) * sp * cp;
-    const R inv = R(1) / m_sqrt(F);
+    const R inv = R(1) / m_sqrt(Facc);
     const Cx<R> T00 = cscale(S2, cp * inv), T01 = cscale(S2, sp * inv);
     const Cx<R> T10 = cscale(S1, -sp * inv), T11 = cscale(S1, cp * inv);
     ph.Em = cadd(cmul(T00, Em), cmul(T01, En));

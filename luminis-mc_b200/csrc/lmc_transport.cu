@@ -568,7 +568,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
           : fp32 ? (h->queued ? (three ? (const void *)dev::transport_kernel<float, true, 3>
                                        : (const void *)dev::transport_kernel<float, true, 2>)
                               : (const void *)dev::transport_kernel<float, false, 1>)
-                 : (h->queued ? (const void *)dev::transport_kernel<double, true, 1>
+                 : (h->queued ? (const void *)dev::transport_kernel<double, true, 2>
                               : (const void *)dev::transport_kernel<double, false, 1>);
   LMC_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_transport));
   if (adj) {
@@ -645,7 +645,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
         dev::transport_kernel<float, false, 1><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
     } else {
       if (h->queued)
-        dev::transport_kernel<double, true, 1><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
+        dev::transport_kernel<double, true, 2><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
       else
         dev::transport_kernel<double, false, 1><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
     }
