@@ -563,7 +563,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   // 2-block (<=128 registers) variant; blocks_per_sm == 1 or 2 selects the latter
   const bool three = fp32 && h->queued && !adj && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
   const void *tk =
-      adj ? (fp32 ? (const void *)dev::transport_kernel<float, true, 2, true>
+      adj ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, true>
                   : (const void *)dev::transport_kernel<double, true, 1, true>)
           : fp32 ? (h->queued ? (three ? (const void *)dev::transport_kernel<float, true, 3>
                                        : (const void *)dev::transport_kernel<float, true, 2>)
@@ -633,7 +633,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
       LMC_CUDA(cudaEventRecord(h->kev[pair], stream));
     if (adj) {
       if (fp32)
-        dev::transport_kernel<float, true, 2, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
+        dev::transport_kernel<float, true, 3, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
       else
         dev::transport_kernel<double, true, 1, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
     } else if (fp32) {
