@@ -8,12 +8,15 @@ tallies and hit counts:
                            ("pin" build: -O2 -ffp-contract=off)
   ref_philox_<scene>.npz   the reference with the Philox replay seam
                            (oracle/replay_rng.cpp), the stream the GPU draws
+  ref_farfield_fluence_small.npz  the far-field fluence definition applied to the
+                           reference's own PhotonRecordSensor records (replay build)
   stat_ref_<scene>.npz     R independent-seed replicas of the unmodified reference
                            (its own RNG): per-bin mean and variance of tally / N,
                            the statistical oracle for other random streams
 
     python tests/golden/make_golden.py        (needs oracle/_ref; run `make -C oracle ref`)
     python tests/golden/make_golden.py stat   (the replica fixtures only)
+    python tests/golden/make_golden.py farfield  (far-field fluence from reference records)
 
 The fixtures pin the oracle (tests/test_oracle_golden.py) and the GPU path
 (tests/test_gpu_golden.py) without the reference present at test time.
@@ -123,6 +126,101 @@ def stat_main():
         print("wrote", run_stat_reference(spec["name"]))
 
 
+FF_GRID = {"theta_max": 1.5707963267948966, "phi_max": 2 * 3.141592653589793, "len_t": 20.0,
+           "d_theta": 3.141592653589793 / 36, "d_phi": 2 * 3.141592653589793 / 12, "d_t": 2.0}
+
+
+def farfield_scene():
+    """bilayer_small with one absorbing sensor at z = 0: a FarFieldFluenceSensor for
+    this library and the oracle, a PhotonRecordSensor for the reference (which has no
+    far-field fluence class); the photon histories are the same."""
+    spec = W.bilayer_rgd_mie(2000, 77)
+    spec["name"] = "farfield_fluence_small"
+    spec["sensors"] = [dict(FF_GRID, kind="farfield_fluence")]
+    return spec
+
+
+def bin_farfield_fluence(records, grid):
+    """The far-field fluence definition applied to the reference's own photon records
+    (PhotonRecordSensor at z = 0): forward-field Stokes of each exiting photon, lab
+    frame projection E_x = E_m m_x + E_n n_x, E_y = E_m m_y + E_n n_y (the FarFieldCBS
+    incoherent part with a zero reverse field), binned on theta = acos(-s_z),
+    phi = atan2(s_y, s_x) in [0, 2 pi), time-integrated bin 0 plus bin
+    floor(t / dt) + 1 of the arrival time."""
+    import math
+    n_t = 1 if grid["d_t"] == 0 else int(math.ceil(grid["len_t"] / grid["d_t"])) + 1
+    n_th = int(math.ceil(grid["theta_max"] / grid["d_theta"]))
+    n_ph = int(math.ceil(grid["phi_max"] / grid["d_phi"]))
+    out = np.zeros((4, n_t, n_th, n_ph))
+    for r in records:
+        if grid["d_t"] > 0:
+            a = r["arrival"]
+            if a < 0 or a >= grid["len_t"]:
+                continue
+            ti = int(a / grid["d_t"]) + 1
+            if ti >= n_t:
+                continue
+        else:
+            ti = 0
+        sx, sy, sz = r["dir"]
+        theta = math.acos(-sz)
+        phi = math.atan2(sy, sx)
+        if phi < 0:
+            phi += 2.0 * math.pi
+        it, jp = int(theta / grid["d_theta"]), int(phi / grid["d_phi"])
+        if not (0 <= it < n_th and 0 <= jp < n_ph):
+            continue
+        w = math.sqrt(r["weight"])
+        em, en = r["Em"] * w, r["En"] * w
+        ex = em * r["m"][0] + en * r["n"][0]
+        ey = em * r["m"][1] + en * r["n"][1]
+        v = (abs(ex) ** 2 + abs(ey) ** 2, abs(ex) ** 2 - abs(ey) ** 2,
+             2.0 * (ex * ey.conjugate()).real, 2.0 * (ex * ey.conjugate()).imag)
+        for t in ((0, ti) if ti >= 1 else (0,)):
+            out[:, t, it, jp] += v
+    return out
+
+
+def run_farfield_reference():
+    """The reference (replay build, Philox u53) with a PhotonRecordSensor at z = 0;
+    returns its records as plain dicts."""
+    code = f"""
+import sys, glob, ctypes, pickle
+sys.path.insert(0, {REPO!r}); sys.path.insert(0, {os.path.join(REPO, 'luminis-mc_b200')!r})
+from tests.golden.make_golden import farfield_scene
+from luminis_mc_b200 import workloads as W
+from oracle import pyoracle as O
+lm = O.reference_module("replay"); lm.set_log_level(lm.LogLevel.off)
+so = ctypes.CDLL(glob.glob({os.path.join(REPO, 'oracle', '_ref', 'replay', 'luminis_mc', '_core*.so')!r})[0])
+so.lmc_replay_set_format(0)
+spec = farfield_scene()
+spec["sensors"] = []
+cfg, hs, keep = W.build(lm, spec, n_threads=1)
+rec = cfg.detector.add_detector(lm.PhotonRecordSensor(0.0, True))
+lm.run_simulation_parallel(cfg)
+out = []
+for r in rec.recorded_photons:
+    d = r.direction; m = r.m; n = r.n; E = r.polarization_forward
+    out.append(dict(arrival=r.arrival_time, weight=r.weight, dir=(d.x, d.y, d.z), m=(m.x, m.y, m.z),
+                    n=(n.x, n.y, n.z), Em=complex(E.m), En=complex(E.n)))
+pickle.dump(out, open(sys.argv[1], "wb"))
+"""
+    import pickle
+    tmp = os.path.join(HERE, "_tmp_records.pkl")
+    subprocess.run([sys.executable, "-c", code, tmp], check=True)
+    recs = pickle.load(open(tmp, "rb"))
+    os.unlink(tmp)
+    return recs
+
+
+def farfield_main():
+    recs = run_farfield_reference()
+    t = bin_farfield_fluence(recs, FF_GRID)
+    path = os.path.join(HERE, "ref_farfield_fluence_small.npz")
+    np.savez_compressed(path, sensor0=t, records=np.int64(len(recs)))
+    print("wrote", path, len(recs), "records")
+
+
 def run_flavour(flavour, scene_name, fmt=None):
     """Run one scene in a fresh interpreter (each reference flavour is a module
     named luminis_mc) and return {sensor index: tally, 'hits': [...]}."""
@@ -173,5 +271,7 @@ def main():
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "stat":
         stat_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "farfield":
+        farfield_main()
     else:
         main()

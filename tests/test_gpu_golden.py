@@ -28,3 +28,17 @@ def test_gpu_fp64_reproduces_reference_golden(spec, cuda):
         np.testing.assert_allclose(t, ref, rtol=tol, atol=tol * np.abs(ref).max())
         assert stats["hits"][i] == g["hits"][i]
     run.close()
+
+
+def test_gpu_farfield_fluence_matches_reference_records(cuda):
+    """FarFieldFluence (no reference class) against its definition applied to the
+    reference's own photon records (tests/golden/ref_farfield_fluence_small.npz)."""
+    from tests.golden.make_golden import farfield_scene
+    spec = farfield_scene()
+    ref = np.load(os.path.join(GOLDEN, "ref_farfield_fluence_small.npz"))["sensor0"]
+    cfg, _, keep = W.build(lm, spec)
+    run = DeviceRun(cfg)
+    run.run(spec["n_photons"], spec["seed"], precision="fp64")
+    got = run.host_tallies()[0]
+    np.testing.assert_allclose(got, ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
+    run.close()

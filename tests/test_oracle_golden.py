@@ -122,3 +122,16 @@ def test_stream_contract():
         assert O.stream_uniform(123, 7, j, "u24") == (2 * (x[j] >> 9) + 1) * 2.0 ** -24
     u = [O.stream_uniform(5, p, d, "u24") for p in range(50) for d in range(40)]
     assert 0.0 < min(u) and max(u) < 1.0
+
+
+def test_farfield_fluence_pinned_by_reference_records():
+    """The reference has no far-field fluence class: its definition (forward-field
+    Stokes binned on exit angles) applied to the reference's own PhotonRecordSensor
+    records on the Philox stream (tests/golden/ref_farfield_fluence_small.npz) equals
+    the oracle's FarFieldFluence tally of the same photons."""
+    from tests.golden.make_golden import farfield_scene
+    spec = farfield_scene()
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden",
+                               "ref_farfield_fluence_small.npz"))["sensor0"]
+    got = O.Oracle(spec).run(spec["n_photons"], spec["seed"], rng="philox_u53").tallies[0]
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
