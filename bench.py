@@ -359,7 +359,10 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
     """The two other arms of the headline metric on this GPU: the same workload in
     FP64 throughout, and FP32 transport with the likelihood-ratio derivatives of the
     differentiable configuration (HG bilayer, 1e7 photons, radial fluence profile of
-    100 bins to 5 mm, CBS cone).  photons/s from the device time of the runs."""
+    100 bins to 5 mm, CBS cone); and the batched sweep of 256 Mie media in one launch
+    (plain, replayed from a CUDA graph, and as one launch per medium).  photons/s from
+    the device time of the runs."""
+    import numpy as np
     import torch
 
     import luminis_mc_b200 as lm
@@ -420,6 +423,52 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
                            "unit": "photons/s", "workload": "bilayer_hg (differentiable)",
                            "parameters": 8, "outputs": "total + 100 radial bins + CBS S0 cone",
                            "steps": args.variant_steps}
+
+    # batched sweep: 256 single-layer Mie media (seeded radius, mu_s, mu_a, photon counts
+    # log-uniform 1e5..1e7) in one launch, against one launch per medium
+    from luminis_mc_b200.sweep import SweepRun
+    from luminis_mc_b200.simulation import Transport
+    _, _, _, counts = W.mie_sweep_parameters()
+    sspecs = [W.mie_sweep(i, seed=2026) for i in range(len(counts))]
+    scfgs = [W.build(lm, sp)[0] for sp in sspecs]
+    sw = SweepRun(scfgs, device=f"cuda:{local}")
+    sw.set_photons(counts)
+    total = int(counts.sum())
+    sw.run(2026 + rank * 7919, precision="fp32", stream=stream.cuda_stream)   # grows the queue
+    flush.zero_()
+    st = sw.run(2027 + rank * 7919, precision="fp32", stream=stream.cuda_stream)
+    sweep_ms = max_ms(st["kernel_ms"])
+    g = sw.capture(2028 + rank * 7919, precision="fp32")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.zero_()
+    e0.record(stream)
+    g.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    graph_ms = max_ms(e0.elapsed_time(e1))
+    del g
+    sw.close()
+    trs = [Transport(c) for c in scfgs]
+    bufs = [torch.zeros(max(t.tally_size, 1), dtype=torch.float64, device=f"cuda:{local}")
+            for t in trs]
+    offs = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    flush.zero_()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for t, b, n, o in zip(trs, bufs, counts, offs):
+        t.run_device(b.data_ptr(), int(n), 2027 + rank * 7919, int(o), want_stats=False,
+                     precision="fp32", stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = max_ms(e0.elapsed_time(e1))
+    for t in trs:
+        t.close()
+    out["sweep_256_media"] = {
+        "value": total * world / (sweep_ms * 1e-3), "unit": "photons/s", "precision": "fp32",
+        "photons": total, "media": len(counts), "graph_replay": total * world / (graph_ms * 1e-3),
+        "sequential_launches": total * world / (seq_ms * 1e-3),
+        "workload": "256 single-layer Mie media, FarFieldCBS 100x1 each, seeded draws "
+                    "(numpy default_rng(2026))"}
     return out
 
 

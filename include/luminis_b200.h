@@ -48,6 +48,7 @@ extern "C" {
 #define LMC_MAX_LAYERS 16
 #define LMC_MAX_MEDIA 16
 #define LMC_MAX_SENSORS 8
+#define LMC_MAX_SWEEP_SCENES 4096
 
 typedef enum lmc_status {
   LMC_OK = 0,
@@ -238,6 +239,34 @@ LMC_API size_t lmc_last_error(char *buf, size_t len);
 LMC_API lmc_status lmc_run_noalloc(const lmc_scene *scene, uint64_t seed, uint64_t photon_begin,
                                    uint64_t n_photons, const lmc_run_opts *opts, double *d_tallies,
                                    lmc_stats *stats);
+
+/* ---- sweeps: many independent scenes in one launch ------------------------------------ */
+/* A parameter sweep of the reference is a sequence of run_simulation_parallel calls, one
+ * per scene (src/simulation.cpp:105-249).  A sweep handle transports all of them in one
+ * persistent launch: photons are numbered across the scenes in order, scene s owning
+ * [P_s, P_s + n_s) with P_s = n_0 + ... + n_{s-1}, and photon g draws the stream of
+ * (seed, g).  Scene s's tallies therefore equal those of lmc_run(seed, P_s, n_s) on a
+ * handle of that scene alone.  Every scene must put every sensor plane at z <= 0. */
+LMC_API lmc_status lmc_create_sweep(const lmc_scene *scenes, int n_scenes, lmc_handle **out);
+
+/* Sensor `sensor` of scene `scene` in the sweep's tally buffer (scene = -1: total size in
+ * *count); dims as lmc_tally_layout. */
+LMC_API lmc_status lmc_sweep_layout(const lmc_handle *h, int scene, int sensor, size_t *offset,
+                                    size_t *count, int dims[4]);
+
+/* Photons per scene for the following lmc_run_sweep calls (n_scenes counts; synchronous:
+ * set them before capturing lmc_run_sweep in a CUDA graph). */
+LMC_API lmc_status lmc_sweep_set_photons(lmc_handle *h, const uint64_t *n_photons);
+
+/* Transport every scene's photons and ADD their contributions into d_tallies (size from
+ * lmc_sweep_layout(-1)).  With stats == NULL the call only enqueues work on opts->stream
+ * (no host synchronisation, no allocation once the hit queue has grown): it can be
+ * captured in a CUDA graph after one uncaptured call of the same size. */
+LMC_API lmc_status lmc_run_sweep(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts,
+                                 double *d_tallies, lmc_stats *stats);
+
+/* Sensor hit counts of the last lmc_run_sweep, [n_scenes][LMC_MAX_SENSORS] (synchronises). */
+LMC_API lmc_status lmc_sweep_hits(lmc_handle *h, uint64_t *hits);
 
 /* ---- likelihood-ratio derivatives ("adjoint") --------------------------------------- */
 /* Derivatives of selected outputs with respect to every medium's parameters

@@ -55,7 +55,7 @@ struct Laser {
 struct __align__(16) Scene {
   int n_layers, n_interfaces, n_media, n_sensors, n_planes, top_is_inf;
   int need_phase;                        // a PlanarField sensor needs exp(i k L)
-  int pad;
+  unsigned cbs_mask;                     // sensors whose hits need the CBS fields
   double top;                            // z_max of the last layer
   double n_step;                         // 1 / light_speed = 1 / (1 / n_host)
   double interfaces[LMC_MAX_LAYERS];
@@ -82,7 +82,7 @@ struct Scratch {
 // Hit queue: one entry per (photon, crossed sensor plane) whose sensors pass their
 // filters, written by the transport kernel and consumed by the tally kernel.
 // Struct-of-arrays, `cap` entries per field.
-enum QueueU32 { kQPhotonLo = 0, kQPhotonHi, kQEvents, kQMask, kQMedia, kQU32Fields };
+enum QueueU32 { kQPhotonLo = 0, kQPhotonHi, kQEvents, kQMask, kQMedia, kQScene, kQU32Fields };
 enum QueueF64 { kQWeight = 0, kQOpath, kQF64Fields };
 enum QueueR {
   kQHit = 0,                  // 3: hit point
@@ -135,7 +135,11 @@ struct RunParams {
   double adj_radial_max;
   unsigned long long adj_cbs_off[LMC_MAX_SENSORS];
   int stream_u24;                        // binary64 transport drawing u24 values
-  int pad2;
+  int n_scenes;                          // sweep: scenes in the launch
+  // sweep: photon g belongs to scene s with sweep_prefix[s] <= g < sweep_prefix[s + 1];
+  // hit counts per scene and sensor in sweep_hits[s * LMC_MAX_SENSORS + sensor]
+  const unsigned long long *sweep_prefix;
+  unsigned long long *sweep_hits;
 };
 
 }  // namespace dev

@@ -227,6 +227,7 @@ template <typename R> struct Photon {
   R pen;                       // penetration depth (records only)
   uint32_t events;
   int layer, last_med;
+  int scene;                   // sweep: the photon's scene
   Rng rng;
   __device__ __forceinline__ unsigned long long index() const
   {
@@ -1036,6 +1037,7 @@ __device__ __forceinline__ void enqueue_hit(const Scene &sc, const RunParams &rp
   q.u32[kQEvents * C + slot] = ph.events;
   q.u32[kQMask * C + slot] = mask;
   q.u32[kQMedia * C + slot] = (uint32_t)side.first_med[tid] | ((uint32_t)ph.last_med << 16);
+  q.u32[kQScene * C + slot] = (uint32_t)ph.scene;
   q.f64[kQWeight * C + slot] = ph.w;
   q.f64[kQOpath * C + slot] = opath;
   R *r = static_cast<R *>(q.r);
@@ -1049,7 +1051,7 @@ __device__ __forceinline__ void enqueue_hit(const Scene &sc, const RunParams &rp
   r[(kQE + 1) * C + slot] = ph.Em.im;
   r[(kQE + 2) * C + slot] = ph.En.re;
   r[(kQE + 3) * C + slot] = ph.En.im;
-  if (mask & rp.cbs_mask) {
+  if (mask & sc.cbs_mask) {
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       r[(kQR1 + j) * C + slot] = side.first[j][tid];
@@ -1140,6 +1142,7 @@ __device__ void init_photon(const Scene &sc, const RunParams &rp, Photon<R> &ph,
   ph.pen = R(0);
   ph.opath = 0.0;
   ph.events = 0;
+  ph.scene = 0;
   ph.layer = layer_index_at<R>(sc, ph.pz);
   ph.last_med = 0;
   const int tid = threadIdx.x;                              // r_1 = r_n = launch, P1 = Pn1 = P0
@@ -1427,24 +1430,41 @@ template <typename R> __host__ __device__ constexpr size_t side_bytes()
   return (sizeof(Side<R>) + 15) & ~size_t(15);
 }
 
-// kAdj: likelihood-ratio run (queued mode only).
-template <typename R, bool kQueue, int kMinBlocks, bool kAdj = false>
+// Scene of global photon g in a sweep: the s with prefix[s] <= g < prefix[s + 1].
+__device__ __forceinline__ int sweep_scene(const RunParams &rp, unsigned long long g)
+{
+  int lo = 0, hi = rp.n_scenes - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (rp.sweep_prefix[mid] <= g)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// kAdj: likelihood-ratio run (queued mode only).  kSweep: g_scene is an array of
+// rp.n_scenes scenes read from global memory (L1-cached), photon g belongs to scene
+// sweep_scene(g), and each lane follows its own photon's scene.
+template <typename R, bool kQueue, int kMinBlocks, bool kAdj = false, bool kSweep = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
-  __shared__ __align__(16) unsigned char s_raw[sizeof(Scene)];
+  __shared__ __align__(16) unsigned char s_raw[kSweep ? 16 : sizeof(Scene)];
   __shared__ unsigned long long s_hits[LMC_MAX_SENSORS];
   __shared__ unsigned long long s_fate[7];
   extern __shared__ __align__(16) unsigned char s_dyn[];
   Side<R> &side = *reinterpret_cast<Side<R> *>(s_dyn);
   Flight<R> fl;
   fl.score = reinterpret_cast<R *>(s_dyn + side_bytes<R>()) + threadIdx.x;
-  load_scene(s_raw, g_scene);
+  if (!kSweep)
+    load_scene(s_raw, g_scene);
   if (threadIdx.x < LMC_MAX_SENSORS)
     s_hits[threadIdx.x] = 0;
   if (threadIdx.x < 7)
     s_fate[threadIdx.x] = 0;
   __syncthreads();
-  const Scene &sc = *reinterpret_cast<const Scene *>(s_raw);
+  const Scene *scp = kSweep ? g_scene : reinterpret_cast<const Scene *>(s_raw);
   const unsigned lane = threadIdx.x & 31u;
   Counters cnt = {0, 0, 0};
   Photon<R> ph;
@@ -1461,7 +1481,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
       if (!alive && !done) {
         const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
         if (idx < rp.n_photons) {
-          init_photon<R>(sc, rp, ph, side, rp.photon_begin + idx);
+          int si = 0;
+          if (kSweep) {
+            si = sweep_scene(rp, rp.photon_begin + idx);
+            scp = g_scene + si;
+          }
+          init_photon<R>(*scp, rp, ph, side, rp.photon_begin + idx);
+          ph.scene = si;
           if (kAdj)
             for (int k = 0; k < rp.adj_K; ++k)
               fl[k] = R(0);
@@ -1474,13 +1500,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
     if (__all_sync(kFull, done))
       break;
     if (alive) {
-      const int fate = event_step<R, kQueue, kAdj>(sc, rp, ph, side, fl, cnt, s_hits);
+      const int fate = event_step<R, kQueue, kAdj>(*scp, rp, ph, side, fl, cnt, s_hits);
       if (fate != kAlive) {
         alive = false;
         cnt.draws += ph.rng.draw;
         atomicAdd(&s_fate[fate], 1ull);
         if (rp.records)
-          write_record<R>(sc, rp, ph, side, fate);
+          write_record<R>(*scp, rp, ph, side, fate);
         if (fate == kError)
           atomicOr(&rp.scratch->error_flags, (unsigned)kErrAborted);
         if (!isfinite(ph.w))
@@ -1519,21 +1545,24 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
 // Tally kernel: one thread per queued hit runs the sensors' process_hit.
 // kAdj: also the likelihood-ratio outputs; the radial ones are summed per block in
 // (1 + adj_K) * (adj_radial_bins + 1) doubles of dynamic shared memory.
-template <typename R, bool kAdj = false>
+// kSweep: each entry carries its scene (an index into the g_scene array) and hit
+// counts go to rp.sweep_hits.
+template <typename R, bool kAdj = false, bool kSweep = false>
 __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
-  __shared__ __align__(16) unsigned char s_raw[sizeof(Scene)];
+  __shared__ __align__(16) unsigned char s_raw[kSweep ? 16 : sizeof(Scene)];
   __shared__ unsigned long long s_hits[LMC_MAX_SENSORS];
   extern __shared__ __align__(16) unsigned char s_dyn[];
   double *s_rad = reinterpret_cast<double *>(s_dyn);
   const int rad_n = (kAdj && rp.adj_radial_sensor >= 0) ? (1 + rp.adj_K) * (rp.adj_radial_bins + 1) : 0;
-  load_scene(s_raw, g_scene);
+  if (!kSweep)
+    load_scene(s_raw, g_scene);
   if (threadIdx.x < LMC_MAX_SENSORS)
     s_hits[threadIdx.x] = 0;
   for (int j = threadIdx.x; j < rad_n; j += blockDim.x)
     s_rad[j] = 0.0;
   __syncthreads();
-  const Scene &sc = *reinterpret_cast<const Scene *>(s_raw);
+  const Scene &sc0 = *reinterpret_cast<const Scene *>(s_raw);
   const Queue &q = rp.queue;
   const unsigned long long C = q.cap;
   const unsigned long long count = *(volatile unsigned long long *)&rp.scratch->queue_count;
@@ -1541,6 +1570,8 @@ __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__
   const R *r = static_cast<const R *>(q.r);
   for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
        i += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned scene = kSweep ? q.u32[kQScene * C + i] : 0u;
+    const Scene &sc = kSweep ? g_scene[scene] : sc0;
     HitData<R> h;
     h.p_lo = q.u32[kQPhotonLo * C + i];
     h.p_hi = q.u32[kQPhotonHi * C + i];
@@ -1559,7 +1590,7 @@ __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__
       h.P[j] = r[(kQP + j) * C + i];
     h.Em = {r[(kQE + 0) * C + i], r[(kQE + 1) * C + i]};
     h.En = {r[(kQE + 2) * C + i], r[(kQE + 3) * C + i]};
-    if (mask & rp.cbs_mask) {
+    if (mask & sc.cbs_mask) {
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
         h.r1[j] = r[(kQR1 + j) * C + i];
@@ -1578,7 +1609,9 @@ __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__
     if (kAdj)
       for (int k = 0; k < rp.adj_K; ++k)
         hs[k] = r[(kQScore + k) * C + i];
-    process_hits<R, kAdj>(sc, rp, h, mask, s_hits, hs, s_rad);
+    process_hits<R, kAdj>(sc, rp, h, mask,
+                          kSweep ? rp.sweep_hits + (unsigned long long)scene * LMC_MAX_SENSORS : s_hits,
+                          hs, s_rad);
   }
   __syncthreads();
   if (threadIdx.x < LMC_MAX_SENSORS && s_hits[threadIdx.x])

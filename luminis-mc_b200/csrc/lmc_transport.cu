@@ -64,6 +64,21 @@ struct lmc_handle {
   size_t queue_bytes = 0;
   unsigned cbs_mask = 0;                 // sensors that need the CBS fields of a hit
   bool queued = false;                   // every sensor plane at z <= 0: queued kernel pair
+  int max_planes = 0;                    // most sensor planes of any scene
+  // sweep handles (lmc_create_sweep): n_scenes scenes in one device array
+  bool sweep = false;
+  int n_scenes = 1;
+  struct SceneLayout {
+    size_t tally_base = 0;
+    int n_sensors = 0;
+    size_t off[LMC_MAX_SENSORS] = {}, count[LMC_MAX_SENSORS] = {};
+    int dims[LMC_MAX_SENSORS][4] = {};
+  };
+  std::vector<lmc::dev::Scene> scenes;   // host copies (device table pointers inside)
+  std::vector<SceneLayout> layouts;
+  unsigned long long *d_prefix = nullptr;      // n_scenes + 1 photon offsets
+  unsigned long long *d_sweep_hits = nullptr;  // n_scenes x LMC_MAX_SENSORS, last run
+  unsigned long long total_photons = 0;        // photons of one sweep run
 };
 
 namespace lmc {
@@ -213,35 +228,27 @@ void fill_sensor(const lmc_sensor_desc &S, dev::Sensor &d, size_t &count, int di
 
 using lmc::fail;
 
-extern "C" {
+namespace lmc {
+namespace {
 
-size_t lmc_last_error(char *buf, size_t len)
+// Host half of a scene: the device Scene (table pointers patched later), its
+// sensor layout and its tables appended to a shared arena.
+struct MedOff { size_t tvd, tcd, tcs, gd, ad, af; };
+struct SceneBuild {
+  dev::Scene sc;
+  size_t tally_doubles = 0;
+  size_t sensor_off[LMC_MAX_SENSORS] = {};
+  size_t sensor_count[LMC_MAX_SENSORS] = {};
+  int sensor_dims[LMC_MAX_SENSORS][4] = {};
+  unsigned cbs_mask = 0;
+  bool queued = false;
+  MedOff mo[LMC_MAX_MEDIA] = {};
+};
+
+// tally_base: offset (doubles) of this scene's first sensor in the tally buffer.
+void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned char> &arena, SceneBuild &b)
 {
-  const std::string &e = lmc::last_error();
-  if (buf && len) {
-    const size_t n = std::min(len - 1, e.size());
-    std::memcpy(buf, e.data(), n);
-    buf[n] = 0;
-  }
-  return e.size();
-}
-
-lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
-{
-  using namespace lmc;
-  if (!out)
-    return fail(LMC_ERR_INVALID, "out must not be null");
-  *out = nullptr;
-  const lmc_status v = validate(s);
-  if (v != LMC_OK)
-    return v;
-  int device = 0;
-  LMC_CUDA(cudaGetDevice(&device));
-  lmc_handle *h = new lmc_handle();
-  h->device = device;
-  LMC_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device));
-
-  dev::Scene &sc = h->scene;
+  dev::Scene &sc = b.sc;
   std::memset(&sc, 0, sizeof(sc));
   sc.n_layers = s->n_layers;
   sc.n_media = s->n_media;
@@ -284,7 +291,7 @@ lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
     const lmc_sensor_desc &S = s->sensors[i];
     dev::Sensor &d = sc.sensors[i];
     size_t count = 0;
-    fill_sensor(S, d, count, h->sensor_dims[i]);
+    fill_sensor(S, d, count, b.sensor_dims[i]);
     const double z = (S.kind == LMC_SENSOR_FARFIELD_CBS || S.kind == LMC_SENSOR_FARFIELD_FLUENCE) ? 0.0 : S.z;
     if (S.kind == LMC_SENSOR_PLANAR_FIELD && !d.estimator)
       sc.need_phase = 1;
@@ -297,16 +304,16 @@ lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
       g = (int)planes.size() - 1;
     }
     d.plane = g;
-    d.tally_off = off;
-    h->sensor_off[i] = off;
-    h->sensor_count[i] = count;
+    d.tally_off = tally_base + off;
+    b.sensor_off[i] = off;
+    b.sensor_count[i] = count;
     off += count;
   }
   // sort planes ascending and remap (record_hit walks the map in key order)
   std::vector<int> order(planes.size());
   for (size_t k = 0; k < planes.size(); ++k)
     order[k] = (int)k;
-  std::sort(order.begin(), order.end(), [&](int a, int b) { return planes[a] < planes[b]; });
+  std::sort(order.begin(), order.end(), [&](int a, int c) { return planes[a] < planes[c]; });
   std::vector<int> rank(planes.size());
   for (size_t k = 0; k < order.size(); ++k) {
     rank[order[k]] = (int)k;
@@ -316,28 +323,24 @@ lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
   for (int i = 0; i < s->n_sensors; ++i)
     sc.sensors[i].plane = rank[sc.sensors[i].plane];
   sc.n_planes = (int)planes.size();
-  h->n_sensors = s->n_sensors;
-  h->tally_doubles = off;
+  b.tally_doubles = off;
   // A photon below z = 0 has left the sample, so a plane at z <= 0 is crossed at
   // most once per photon: hits fit a queue of (photons x planes) entries and are
   // tallied by a second kernel.  Planes inside the sample may be crossed any
   // number of times; such scenes tally inside the transport kernel.
-  h->queued = sc.n_planes == 0 || sc.plane_z[sc.n_planes - 1] <= 0.0;
+  b.queued = sc.n_planes == 0 || sc.plane_z[sc.n_planes - 1] <= 0.0;
   for (int i = 0; i < s->n_sensors; ++i)
     if (s->sensors[i].kind == LMC_SENSOR_FARFIELD_CBS)
-      h->cbs_mask |= 1u << i;
+      b.cbs_mask |= 1u << i;
+  sc.cbs_mask = b.cbs_mask;
 
   // table arena: per medium double/float theta tables, guide tables, amplitudes
-  struct Span { size_t off, bytes; };
-  std::vector<unsigned char> arena;
   auto put = [&](const void *src, size_t bytes) -> size_t {
     const size_t o = (arena.size() + 255) & ~size_t(255);
     arena.resize(o + bytes);
     std::memcpy(arena.data() + o, src, bytes);
     return o;
   };
-  struct MedOff { size_t tvd, tcd, tcs, gd, ad, af; };
-  std::vector<MedOff> mo(s->n_media);
   for (int i = 0; i < s->n_media; ++i) {
     const lmc_medium_desc &M = s->media[i];
     dev::Medium &d = sc.media[i];
@@ -355,7 +358,7 @@ lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
     d.amp_inv_dx_f = (float)d.amp_inv_dx;
     d.mu_s = M.mu_s;
     d.mu_s_f = (float)M.mu_s;
-    MedOff &o = mo[i];
+    MedOff &o = b.mo[i];
     o = MedOff{0, 0, 0, 0, 0, 0};
     if (M.theta_kind == LMC_THETA_TABLE || M.theta_kind == LMC_THETA_TABLE_COS) {
       const int n = M.theta_n;
@@ -383,28 +386,14 @@ lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
     o.ad = put(ad.data(), ad.size() * sizeof(double4));
     o.af = put(af.data(), af.size() * sizeof(float4));
   }
-  h->arena_bytes = arena.size();
-  cudaError_t e = cudaMalloc(&h->d_arena, std::max<size_t>(h->arena_bytes, 256));
-  if (e == cudaSuccess)
-    e = cudaMemcpy(h->d_arena, arena.data(), arena.size(), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = cudaMalloc(&h->d_scene, sizeof(dev::Scene));
-  if (e == cudaSuccess)
-    e = cudaMalloc(&h->d_scratch, sizeof(dev::Scratch));
-  if (e == cudaSuccess)
-    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess)
-    e = cudaEventCreate(&h->ev0);
-  if (e == cudaSuccess)
-    e = cudaEventCreate(&h->ev1);
-  if (e != cudaSuccess) {
-    lmc_destroy(h);
-    return fail(LMC_ERR_CUDA, std::string("lmc_create: ") + cudaGetErrorString(e));
-  }
-  unsigned char *base = static_cast<unsigned char *>(h->d_arena);
-  for (int i = 0; i < s->n_media; ++i) {
-    dev::Medium &d = sc.media[i];
-    const MedOff &o = mo[i];
+}
+
+// Device table pointers of a built scene, given the device copy of the arena.
+void patch_tables(SceneBuild &b, unsigned char *base)
+{
+  for (int i = 0; i < b.sc.n_media; ++i) {
+    dev::Medium &d = b.sc.media[i];
+    const MedOff &o = b.mo[i];
     if (d.theta_n) {
       d.th_val_d = reinterpret_cast<const double *>(base + o.tvd);
       d.th_cdf_d = reinterpret_cast<const double *>(base + o.tcd);
@@ -414,7 +403,79 @@ lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
     d.amp_d = reinterpret_cast<const double4 *>(base + o.ad);
     d.amp_f = reinterpret_cast<const float4 *>(base + o.af);
   }
-  e = cudaMemcpy(h->d_scene, &sc, sizeof(sc), cudaMemcpyHostToDevice);
+}
+
+// Device allocations shared by lmc_create and lmc_create_sweep: arena, scenes,
+// scratch, stream and events.
+cudaError_t alloc_handle(lmc_handle *h, const std::vector<unsigned char> &arena, size_t n_scenes)
+{
+  h->arena_bytes = arena.size();
+  cudaError_t e = cudaMalloc(&h->d_arena, std::max<size_t>(h->arena_bytes, 256));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(h->d_arena, arena.data(), arena.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMalloc(&h->d_scene, n_scenes * sizeof(dev::Scene));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&h->d_scratch, sizeof(dev::Scratch));
+  if (e == cudaSuccess)
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&h->ev0);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&h->ev1);
+  return e;
+}
+
+}  // namespace
+}  // namespace lmc
+
+extern "C" {
+
+size_t lmc_last_error(char *buf, size_t len)
+{
+  const std::string &e = lmc::last_error();
+  if (buf && len) {
+    const size_t n = std::min(len - 1, e.size());
+    std::memcpy(buf, e.data(), n);
+    buf[n] = 0;
+  }
+  return e.size();
+}
+
+lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
+{
+  using namespace lmc;
+  if (!out)
+    return fail(LMC_ERR_INVALID, "out must not be null");
+  *out = nullptr;
+  const lmc_status v = validate(s);
+  if (v != LMC_OK)
+    return v;
+  int device = 0;
+  LMC_CUDA(cudaGetDevice(&device));
+  lmc_handle *h = new lmc_handle();
+  h->device = device;
+  LMC_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device));
+  std::vector<unsigned char> arena;
+  SceneBuild b;
+  build_scene(s, 0, arena, b);
+  h->n_sensors = s->n_sensors;
+  h->tally_doubles = b.tally_doubles;
+  h->queued = b.queued;
+  h->cbs_mask = b.cbs_mask;
+  h->max_planes = b.sc.n_planes;
+  for (int i = 0; i < LMC_MAX_SENSORS; ++i) {
+    h->sensor_off[i] = b.sensor_off[i];
+    h->sensor_count[i] = b.sensor_count[i];
+    for (int k = 0; k < 4; ++k)
+      h->sensor_dims[i][k] = b.sensor_dims[i][k];
+  }
+  cudaError_t e = alloc_handle(h, arena, 1);
+  if (e == cudaSuccess) {
+    patch_tables(b, static_cast<unsigned char *>(h->d_arena));
+    h->scene = b.sc;
+    e = cudaMemcpy(h->d_scene, &h->scene, sizeof(h->scene), cudaMemcpyHostToDevice);
+  }
   if (e != cudaSuccess) {
     lmc_destroy(h);
     return fail(LMC_ERR_CUDA, std::string("lmc_create: ") + cudaGetErrorString(e));
@@ -434,6 +495,8 @@ void lmc_destroy(lmc_handle *h)
   cudaFree(h->d_scratch);
   cudaFree(h->d_host_tally);
   cudaFree(h->d_queue);
+  cudaFree(h->d_prefix);
+  cudaFree(h->d_sweep_hits);
   for (cudaEvent_t e : h->kev)
     cudaEventDestroy(e);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -515,13 +578,22 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     return fail(LMC_ERR_INVALID, "unknown precision");
   if (opts->max_events < 0)
     return fail(LMC_ERR_INVALID, "max_events must be non-negative");
-  for (int i = 0; i < h->scene.n_sensors; ++i)
-    if (h->scene.sensors[i].kind == LMC_SENSOR_FARFIELD_CBS && !opts->track_reverse_paths)
-      return fail(LMC_ERR_INVALID, "FarFieldCBSSensor needs track_reverse_paths (the reference "
-                                   "dereferences null species pointers without it)");
+  const bool sw = h->sweep;
+  if (sw && adj)
+    return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs are not available for sweeps");
+  for (int k = 0; k < h->n_scenes; ++k) {
+    const dev::Scene &scn = sw ? h->scenes[k] : h->scene;
+    for (int i = 0; i < scn.n_sensors; ++i)
+      if (scn.sensors[i].kind == LMC_SENSOR_FARFIELD_CBS && !opts->track_reverse_paths)
+        return fail(LMC_ERR_INVALID, "FarFieldCBSSensor needs track_reverse_paths (the reference "
+                                     "dereferences null species pointers without it)");
+  }
   LMC_CUDA(cudaSetDevice(h->device));
   cudaStream_t stream = opts->stream ? static_cast<cudaStream_t>(opts->stream) : h->stream;
   LMC_CUDA(cudaMemsetAsync(h->d_scratch, 0, sizeof(dev::Scratch), stream));
+  if (sw)
+    LMC_CUDA(cudaMemsetAsync(h->d_sweep_hits, 0,
+                             sizeof(unsigned long long) * h->n_scenes * LMC_MAX_SENSORS, stream));
   dev::RunParams rp;
   std::memset(&rp, 0, sizeof(rp));
   rp.key0 = (uint32_t)seed;
@@ -536,6 +608,11 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   if (opts->stream_format != 0 && opts->stream_format != 1)
     return fail(LMC_ERR_INVALID, "stream_format must be 0 or 1");
   rp.stream_u24 = (!fp32 && opts->stream_format == 1) ? 1 : 0;
+  if (sw) {
+    rp.n_scenes = h->n_scenes;
+    rp.sweep_prefix = h->d_prefix;
+    rp.sweep_hits = h->d_sweep_hits;
+  }
   const int block = opts->block_size > 0 ? opts->block_size : dev::kBlock;
   if (block % 32 != 0 || block > dev::kBlock)
     return fail(LMC_ERR_INVALID, "block_size must be a multiple of 32 and at most 256");
@@ -563,7 +640,9 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   // 2-block (<=128 registers) variant; blocks_per_sm == 1 or 2 selects the latter
   const bool three = fp32 && h->queued && !adj && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
   const void *tk =
-      adj ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, true>
+      sw ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, false, true>
+                 : (const void *)dev::transport_kernel<double, true, 2, false, true>)
+      : adj ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, true>
                   : (const void *)dev::transport_kernel<double, true, 1, true>)
           : fp32 ? (h->queued ? (three ? (const void *)dev::transport_kernel<float, true, 3>
                                        : (const void *)dev::transport_kernel<float, true, 2>)
@@ -587,7 +666,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   if (h->queued && n_photons > 0) {
     batch = opts->batch_photons ? opts->batch_photons : (8ull << 20);
     batch = std::min<unsigned long long>(batch, n_photons);
-    const unsigned long long planes = std::max(1, h->scene.n_planes);
+    const unsigned long long planes = std::max(1, h->max_planes);
     const unsigned long long cap = batch * planes + batch / 16 + 1024;
     const size_t need = (size_t)cap * (dev::kQU32Fields * 4 + dev::kQF64Fields * 8 +
                                        (dev::kQRFields + (size_t)rp.adj_K) * rbytes) + 3 * 256;
@@ -631,7 +710,12 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     const size_t pair = 2 * (size_t)(done / batch);
     if (stats)
       LMC_CUDA(cudaEventRecord(h->kev[pair], stream));
-    if (adj) {
+    if (sw) {
+      if (fp32)
+        dev::transport_kernel<float, true, 3, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
+      else
+        dev::transport_kernel<double, true, 2, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
+    } else if (adj) {
       if (fp32)
         dev::transport_kernel<float, true, 3, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
       else
@@ -652,11 +736,16 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     LMC_CUDA(cudaGetLastError());
     if (stats)
       LMC_CUDA(cudaEventRecord(h->kev[pair + 1], stream));
-    if (h->queued && h->scene.n_sensors > 0) {
+    if (h->queued && h->tally_doubles > 0) {
       const int tgrid = (int)std::max<unsigned long long>(
           1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * 8,
                                              (rp.queue.cap + dev::kBlock - 1) / dev::kBlock));
-      if (adj) {
+      if (sw) {
+        if (fp32)
+          dev::tally_kernel<float, false, true><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
+        else
+          dev::tally_kernel<double, false, true><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
+      } else if (adj) {
         if (fp32)
           dev::tally_kernel<float, true><<<tgrid, dev::kBlock, dyn_tally, stream>>>(h->d_scene, rp);
         else
@@ -702,7 +791,148 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
 lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
                    const lmc_run_opts *opts, double *d_tallies, lmc_stats *stats)
 {
+  if (h && h->sweep)
+    return lmc::fail(LMC_ERR_INVALID, "a sweep handle runs through lmc_run_sweep");
   return run_impl(h, seed, photon_begin, n_photons, opts, nullptr, nullptr, d_tallies, stats);
+}
+
+lmc_status lmc_create_sweep(const lmc_scene *scenes, int n_scenes, lmc_handle **out)
+{
+  using namespace lmc;
+  if (!out || !scenes)
+    return fail(LMC_ERR_INVALID, "scenes and out must not be null");
+  *out = nullptr;
+  if (n_scenes < 1 || n_scenes > LMC_MAX_SWEEP_SCENES)
+    return fail(LMC_ERR_INVALID, "n_scenes must be in [1, " + std::to_string(LMC_MAX_SWEEP_SCENES) + "]");
+  for (int k = 0; k < n_scenes; ++k) {
+    const lmc_status v = validate(scenes + k);
+    if (v != LMC_OK)
+      return fail(v, "scene " + std::to_string(k) + ": " + last_error());
+  }
+  int device = 0;
+  LMC_CUDA(cudaGetDevice(&device));
+  lmc_handle *h = new lmc_handle();
+  h->device = device;
+  h->sweep = true;
+  h->n_scenes = n_scenes;
+  LMC_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device));
+  std::vector<unsigned char> arena;
+  std::vector<SceneBuild> builds(n_scenes);
+  h->layouts.resize(n_scenes);
+  size_t tally = 0;
+  h->queued = true;
+  for (int k = 0; k < n_scenes; ++k) {
+    build_scene(scenes + k, tally, arena, builds[k]);
+    if (!builds[k].queued) {
+      delete h;
+      return fail(LMC_ERR_UNSUPPORTED, "scene " + std::to_string(k) +
+                                           ": a sweep needs every sensor plane at z <= 0");
+    }
+    lmc_handle::SceneLayout &L = h->layouts[k];
+    L.tally_base = tally;
+    L.n_sensors = scenes[k].n_sensors;
+    for (int i = 0; i < LMC_MAX_SENSORS; ++i) {
+      L.off[i] = tally + builds[k].sensor_off[i];
+      L.count[i] = builds[k].sensor_count[i];
+      for (int j = 0; j < 4; ++j)
+        L.dims[i][j] = builds[k].sensor_dims[i][j];
+    }
+    h->max_planes = std::max(h->max_planes, builds[k].sc.n_planes);
+    tally += builds[k].tally_doubles;
+  }
+  h->tally_doubles = tally;
+  h->n_sensors = scenes[0].n_sensors;
+  for (int i = 0; i < LMC_MAX_SENSORS; ++i) {
+    h->sensor_off[i] = h->layouts[0].off[i];
+    h->sensor_count[i] = h->layouts[0].count[i];
+  }
+  cudaError_t e = alloc_handle(h, arena, (size_t)n_scenes);
+  if (e == cudaSuccess)
+    e = cudaMalloc(&h->d_prefix, sizeof(unsigned long long) * (n_scenes + 1));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&h->d_sweep_hits, sizeof(unsigned long long) * n_scenes * LMC_MAX_SENSORS);
+  if (e == cudaSuccess) {
+    h->scenes.resize(n_scenes);
+    for (int k = 0; k < n_scenes; ++k) {
+      patch_tables(builds[k], static_cast<unsigned char *>(h->d_arena));
+      h->scenes[k] = builds[k].sc;
+    }
+    h->scene = h->scenes[0];
+    e = cudaMemcpy(h->d_scene, h->scenes.data(), sizeof(dev::Scene) * n_scenes, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) {
+    std::vector<unsigned long long> zero(n_scenes + 1, 0ull);
+    e = cudaMemcpy(h->d_prefix, zero.data(), sizeof(unsigned long long) * (n_scenes + 1),
+                   cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    lmc_destroy(h);
+    return fail(LMC_ERR_CUDA, std::string("lmc_create_sweep: ") + cudaGetErrorString(e));
+  }
+  *out = h;
+  return LMC_OK;
+}
+
+lmc_status lmc_sweep_layout(const lmc_handle *h, int scene, int sensor, size_t *offset,
+                            size_t *count, int dims[4])
+{
+  using namespace lmc;
+  if (!h || !h->sweep)
+    return fail(LMC_ERR_INVALID, "not a sweep handle");
+  if (scene == -1) {
+    if (count)
+      *count = h->tally_doubles;
+    return LMC_OK;
+  }
+  if (scene < 0 || scene >= h->n_scenes)
+    return fail(LMC_ERR_INVALID, "scene out of range");
+  const lmc_handle::SceneLayout &L = h->layouts[scene];
+  if (sensor < 0 || sensor >= L.n_sensors)
+    return fail(LMC_ERR_INVALID, "sensor out of range");
+  if (offset)
+    *offset = L.off[sensor];
+  if (count)
+    *count = L.count[sensor];
+  if (dims)
+    for (int k = 0; k < 4; ++k)
+      dims[k] = L.dims[sensor][k];
+  return LMC_OK;
+}
+
+lmc_status lmc_sweep_set_photons(lmc_handle *h, const uint64_t *n_photons)
+{
+  using namespace lmc;
+  if (!h || !h->sweep || !n_photons)
+    return fail(LMC_ERR_INVALID, "sweep handle and photon counts must not be null");
+  std::vector<unsigned long long> prefix(h->n_scenes + 1, 0ull);
+  for (int k = 0; k < h->n_scenes; ++k)
+    prefix[k + 1] = prefix[k] + n_photons[k];
+  LMC_CUDA(cudaSetDevice(h->device));
+  LMC_CUDA(cudaStreamSynchronize(h->stream));
+  LMC_CUDA(cudaMemcpy(h->d_prefix, prefix.data(), sizeof(unsigned long long) * (h->n_scenes + 1),
+                      cudaMemcpyHostToDevice));
+  h->total_photons = prefix[h->n_scenes];
+  return LMC_OK;
+}
+
+lmc_status lmc_run_sweep(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts, double *d_tallies,
+                         lmc_stats *stats)
+{
+  if (!h || !h->sweep)
+    return lmc::fail(LMC_ERR_INVALID, "not a sweep handle");
+  return run_impl(h, seed, 0, h->total_photons, opts, nullptr, nullptr, d_tallies, stats);
+}
+
+lmc_status lmc_sweep_hits(lmc_handle *h, uint64_t *hits)
+{
+  using namespace lmc;
+  if (!h || !h->sweep || !hits)
+    return fail(LMC_ERR_INVALID, "sweep handle and output must not be null");
+  LMC_CUDA(cudaSetDevice(h->device));
+  LMC_CUDA(cudaDeviceSynchronize());
+  LMC_CUDA(cudaMemcpy(hits, h->d_sweep_hits, sizeof(unsigned long long) * h->n_scenes * LMC_MAX_SENSORS,
+                      cudaMemcpyDeviceToHost));
+  return LMC_OK;
 }
 
 lmc_status lmc_adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a, size_t *n_out,
@@ -962,6 +1192,7 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     sc.sensors[i].plane = rank[sc.sensors[i].plane];
   sc.n_planes = n_planes;
   const bool queued = n_planes == 0 || sc.plane_z[n_planes - 1] <= 0.0;
+  sc.cbs_mask = cbs_mask;
   if (tally_doubles && !d_tallies)
     return fail(LMC_ERR_INVALID, "device tally buffer must not be null");
 

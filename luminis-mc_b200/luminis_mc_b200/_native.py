@@ -110,7 +110,9 @@ RECORD_FIELDS = [("photon", "<u8"), ("events", "<u4"), ("draws", "<u4"), ("fate"
 EXPORTED = ["lmc_create", "lmc_destroy", "lmc_tally_layout", "lmc_run", "lmc_run_host",
             "lmc_last_error", "lmc_mie", "lmc_sampling_table", "lmc_phase_cross_section",
             "lmc_amplitude_table", "lmc_probe_fp32_peak", "lmc_run_noalloc",
-            "lmc_adjoint_layout", "lmc_run_adjoint", "lmc_adjoint_contract"]
+            "lmc_adjoint_layout", "lmc_run_adjoint", "lmc_adjoint_contract",
+            "lmc_create_sweep", "lmc_sweep_layout", "lmc_sweep_set_photons", "lmc_run_sweep",
+            "lmc_sweep_hits"]
 
 _lib = None
 
@@ -168,6 +170,17 @@ def lib():
     L.lmc_run_adjoint.restype = C.c_int
     L.lmc_adjoint_contract.argtypes = [vp, vp, C.c_size_t, C.c_int, vp, vp]
     L.lmc_adjoint_contract.restype = C.c_int
+    L.lmc_create_sweep.argtypes = [C.POINTER(SceneDesc), C.c_int, C.POINTER(vp)]
+    L.lmc_create_sweep.restype = C.c_int
+    L.lmc_sweep_layout.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_size_t),
+                                   C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
+    L.lmc_sweep_layout.restype = C.c_int
+    L.lmc_sweep_set_photons.argtypes = [vp, C.POINTER(C.c_uint64)]
+    L.lmc_sweep_set_photons.restype = C.c_int
+    L.lmc_run_sweep.argtypes = [vp, C.c_uint64, C.POINTER(RunOpts), vp, C.POINTER(Stats)]
+    L.lmc_run_sweep.restype = C.c_int
+    L.lmc_sweep_hits.argtypes = [vp, C.POINTER(C.c_uint64)]
+    L.lmc_sweep_hits.restype = C.c_int
     _lib = L
     return L
 
