@@ -34,9 +34,9 @@ sys.path.insert(0, REPO)
 FLOP_PER_EVENT = 300        # FP32 flops per scattering event (add/mul = 1, FMA = 2)
 METRIC = "photons/s"
 # DRAM bytes (read + write) per photon of one transport launch on bilayer_rgd_mie in
-# FP32: 166.07 MB for a 2 M-photon launch in one ncu capture
+# FP32: 863.4 MB for an 8 M-photon launch in one ncu capture
 # (profiles/transport_kernel_bilayer_rgd_mie.md); traffic grows with photons.
-TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": 166.07e6 / 2e6}
+TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": 863.42e6 / 8e6}
 
 
 def parse():
