@@ -205,6 +205,8 @@ def build(lm, spec, n_photons=None, seed=None, n_threads=None):
                                            s["d_theta"], s["d_phi"], s.get("d_t", 0.0))
         else:
             raise ValueError(f"unknown sensor kind {kind!r}")
+        if "theta_pp_max" in s:
+            det.theta_pp_max = float(s["theta_pp_max"])
         if "theta_limit" in s:
             det.set_theta_limit(*s["theta_limit"])
         if "phi_limit" in s:

@@ -8,9 +8,8 @@
  * std::complex<double> arithmetic maps onto C99 `double complex`; std::norm is
  * re*re + im*im (what libstdc++ evaluates at -O2 here).
  *
- * Out of scope (rejected at create time): MixtureLayer, estimator-mode
- * FarFieldCBS (process_estimation), PhotonRecord/Statistics sensors, the
- * Absorption recorder.  Planar sensors in estimator mode record nothing, as in
+ * Out of scope (rejected at create time): MixtureLayer, PhotonRecord/Statistics
+ * sensors, the Absorption recorder.  Planar sensors in estimator mode record nothing, as in
  * the reference (their process_estimation bodies are empty,
  * src/detector.cpp:571-700,844-846).
  */
@@ -418,6 +417,7 @@ static double ophase_sample_theta(const ophase *ph, double x)
 typedef struct {
   lmc_o_medium p;
   double mu_t;          /* mu_a + mu_s (src/medium.cpp:61-71) */
+  double I_norm;        /* int_0^pi (|S11|^2 + |S22|^2) sin(theta) dtheta (estimator) */
   dtable S1, S2;
   int phase;
 } omedium;
@@ -511,10 +511,6 @@ static int osensor_init(lmc_o_handle *h, osensor *s, const lmc_o_sensor *p, char
   case LMC_O_SENSOR_FARFIELD_FLUENCE:
     s->p.z = 0.0;                 /* Sensor(0.0, true, estimator): always z=0, absorbing */
     s->p.absorb = 1;
-    if (p->kind == LMC_O_SENSOR_FARFIELD_CBS && s->p.estimator) {
-      snprintf(err, (size_t)err_len, "estimator-mode FarFieldCBSSensor is outside the oracle");
-      return -1;
-    }
     s->N_t = (p->dt == 0) ? 1 : (int)ceil(p->len_t / p->dt) + 1;
     s->N_theta = (int)ceil(p->theta_max_grid / p->dtheta);
     s->N_phi = (int)ceil(p->phi_max_grid / p->dphi);
@@ -1022,6 +1018,200 @@ static void process_hit_field(const osensor *s, double *tally, const ophoton *ph
   *hits += 1;
 }
 
+/* ------------------------------------------------- last-flight CBS estimator */
+/* I_norm = int_0^pi (|S11|^2 + |S22|^2) sin(theta) dtheta, midpoint rule with 2048
+ * points (src/detector.cpp:106-118). */
+static double compute_I_norm(const omedium *md)
+{
+  const int n = 2048;
+  double acc = 0.0;
+  const double dth = M_PI / n;
+  for (int i = 0; i < n; i++) {
+    const double th = (i + 0.5) * dth;
+    cplx S2, S1;
+    omedium_smatrix(md, th, &S2, &S1);
+    acc += (cnrm(S1) + cnrm(S2)) * sin(th);
+  }
+  return acc * dth;
+}
+
+/* Optical depth along a straight ray, layer by layer (src/detector.cpp:52-102). */
+static double optical_depth_to_detector(const lmc_o_handle *h, v3 start, v3 dir, double L_total)
+{
+  double tau = 0.0, traveled = 0.0;
+  v3 p = start;
+  int layer = layer_index_at(h, p.z);
+  if (layer >= h->scene.n_layers)
+    return 0.0;
+  if (h->scene.n_layers == 1)
+    return layer_medium(h, layer)->mu_t * L_total;
+  const double dz = dir.z;
+  while (traveled < L_total - 1e-15) {
+    const double remaining = L_total - traveled;
+    const double mu = layer_medium(h, layer)->mu_t;
+    double seg = remaining;
+    if (fabs(dz) > 1e-15) {
+      double zi;
+      if (find_next_interface(h, p.z, p.z + dz * remaining, &zi)) {
+        const double sd = (zi - p.z) / dz;
+        if (sd > 1e-15 && sd < remaining)
+          seg = sd;
+      }
+    }
+    tau += mu * seg;
+    p.x += dir.x * seg;
+    p.y += dir.y * seg;
+    p.z += dir.z * seg;
+    traveled += seg;
+    if (seg >= remaining - 1e-15)
+      break;
+    const double nudge = (dz > 0) ? 1e-12 : -1e-12;
+    const int next = layer_index_at(h, p.z + nudge);
+    if (next >= h->scene.n_layers)
+      break;
+    layer = next;
+  }
+  return tau;
+}
+
+/* phase_F (src/detector.cpp:1012-1024) */
+static double phase_F(cplx S2, cplx S1, double cos_phi, double sin_phi, cplx Em, cplx En)
+{
+  const double s22 = cnrm(S2), s11 = cnrm(S1);
+  const double Emm = cnrm(Em), Enn = cnrm(En);
+  const double c2 = cos_phi * cos_phi, s2 = sin_phi * sin_phi;
+  return Emm * (s22 * c2 + s11 * s2) + Enn * (s22 * s2 + s11 * c2) +
+         2.0 * creal(Em * conj(En)) * (s22 - s11) * sin_phi * cos_phi;
+}
+
+/* scatter_frame (src/detector.cpp:1027-1045): A(theta, phi) P */
+static m3 scatter_frame(const m3 *P, double theta, double cos_phi, double sin_phi)
+{
+  const double ct = cos(theta), st = sin(theta);
+  const double A[3][3] = {{ct * cos_phi, ct * sin_phi, -st}, {-sin_phi, cos_phi, 0}, {st * cos_phi, st * sin_phi, ct}};
+  m3 out;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; ++k)
+        acc += A[i][k] * P->a[k][j];
+      out.a[i][j] = acc;
+    }
+  return out;
+}
+
+/* apply_scatter_normalized (src/detector.cpp:121-160): (S R(phi)) E / sqrt(F) */
+static void apply_scatter_normalized(cplx S2, cplx S1, double cos_phi, double sin_phi, cplx Em, cplx En,
+                                     cplx *Om, cplx *On)
+{
+  const cplx T00 = S2 * cos_phi, T01 = S2 * sin_phi, T10 = S1 * -sin_phi, T11 = S1 * cos_phi;
+  const double F = phase_F(S2, S1, cos_phi, sin_phi, Em, En);
+  if (F < 1e-300) {
+    *Om = 0.0;
+    *On = 0.0;
+    return;
+  }
+  const double inv = 1.0 / sqrt(F);
+  *Om = inv * (T00 * Em + T01 * En);
+  *On = inv * (T10 * Em + T11 * En);
+}
+
+/* FarFieldCBSSensor::process_estimation (src/detector.cpp:1315-1566): at every
+ * scattering vertex, before the scatter is sampled, the photon is forced toward
+ * the centre of every angular bin (theta, phi) of the grid; the bin receives the
+ * weight w mu_s/mu_t x transmittance x p(Omega) dOmega with p = F / (pi I_norm),
+ * its forward field and, from the second vertex on, its reverse (CBS) field. */
+static void estimate_farfield_cbs(const lmc_o_handle *h, const osensor *s, double *tally,
+                                  const ophoton *ph, int med_idx, uint64_t *hits)
+{
+  const lmc_o_sensor *p = &s->p;
+  if (p->f_events && ((int)ph->events < p->events_min || (int)ph->events > p->events_max))
+    return;
+  const omedium *med = &h->media[med_idx];
+  const double I_norm = med->I_norm;
+  if (I_norm < 1e-300)
+    return;
+  const v3 e1 = m3row(&ph->P0, 0), e2 = m3row(&ph->P0, 1), s_in = m3row(&ph->P0, 2);
+  const v3 e3 = v3scale(s_in, -1.0);
+  const m3 *Pcur = &ph->P;
+  const v3 m_cur = m3row(Pcur, 0), n_cur = m3row(Pcur, 1), s_cur = m3row(Pcur, 2);
+  const double w_scatter = ph->weight * (med->p.mu_s / med->mu_t);
+  if (w_scatter < 1e-300)
+    return;
+  const double th_cap = (p->theta_pp_max > 0.0) ? fmin(p->theta_pp_max, p->theta_max_grid) : p->theta_max_grid;
+  int i_max = (int)(th_cap / p->dtheta);
+  if (i_max > s->N_theta)
+    i_max = s->N_theta;
+  const int multi = ph->events >= 1;
+  cplx pre_m = 0.0, pre_n = 0.0;
+  if (multi) {
+    cplx Tmid[4] = {ph->Traw[0], ph->Traw[1], ph->Traw[2], ph->Traw[3]};
+    if (ph->events >= 2 && ph->has_T_prev) {
+      const cplx *A = ph->Traw_buf, *B = ph->Traw;
+      Tmid[0] = A[0] * B[0] + A[1] * B[2];
+      Tmid[1] = A[0] * B[1] + A[1] * B[3];
+      Tmid[2] = A[2] * B[0] + A[3] * B[2];
+      Tmid[3] = A[2] * B[1] + A[3] * B[3];
+    }
+    reverse_field_prefix(h, &ph->P0, Pcur, Tmid, med_idx, ph->E0m, ph->E0n, &pre_m, &pre_n);
+  }
+  for (int it = 0; it < i_max; ++it) {
+    const double th_det = (it + 0.5) * p->dtheta;
+    const double c_th = cos(th_det), s_th = sin(th_det);
+    const double dOmega_band = cos(it * p->dtheta) - cos((it + 1) * p->dtheta);
+    for (int jp = 0; jp < s->N_phi; ++jp) {
+      const double ph_det = (jp + 0.5) * p->dphi;
+      const double c_ph = cos(ph_det), s_ph = sin(ph_det);
+      const v3 s_out = v3add(v3add(v3scale(e1, s_th * c_ph), v3scale(e2, s_th * s_ph)), v3scale(e3, c_th));
+      /* intersect_plane with the sensor plane z = 0, normal +z (src/detector.cpp:35-47) */
+      const double denom = s_out.z;
+      if (fabs(denom) < 1e-14)
+        continue;
+      const double L = (-ph->pos.z) / denom;
+      if (L <= 0.0)
+        continue;
+      const double Tr = exp(-optical_depth_to_detector(h, ph->pos, s_out, L));
+      if (Tr < 1e-20)
+        continue;
+      const v3 pv = v3cross(s_cur, s_out);
+      const double pn = v3norm(pv);
+      if (pn < 1e-12)
+        continue;
+      const v3 p_hat = v3scale(pv, 1.0 / pn);
+      const double sin_phi = -v3dot(m_cur, p_hat);
+      const double cos_phi = v3dot(n_cur, p_hat);
+      const double th_scat = acos(clamp_pm1(v3dot(s_cur, s_out)));
+      cplx S2, S1;
+      omedium_smatrix(med, th_scat, &S2, &S1);
+      const double F = phase_F(S2, S1, cos_phi, sin_phi, ph->Em, ph->En);
+      if (F < 1e-300)
+        continue;
+      const double prob_bin = (F / (M_PI * I_norm)) * (dOmega_band * p->dphi);
+      const double w_bin = w_scatter * Tr * prob_bin;
+      if (w_bin < 1e-300)
+        continue;
+      const cplx amp = sqrt(w_bin) * cexp(CMPLX(0.0, ph->k * L));
+      const m3 P_exit = scatter_frame(Pcur, th_scat, cos_phi, sin_phi);
+      cplx Efm, Efn;
+      apply_scatter_normalized(S2, S1, cos_phi, sin_phi, ph->Em, ph->En, &Efm, &Efn);
+      const int t_idx = time_bin(s, ph->launch_time + (ph->opticalpath + L) / ph->velocity);
+      if (t_idx < 0)
+        continue;
+      cplx Efx, Efy, Erx = 0.0, Ery = 0.0;
+      project_to_lab(Efm * amp, Efn * amp, &P_exit, &Efx, &Efy);
+      if (multi) {
+        cplx Erm, Ern;
+        reverse_field_suffix(h, &ph->P1, &P_exit, ph->first_medium, pre_m, pre_n, &Erm, &Ern);
+        const v3 qb = v3scale(v3add(s_out, s_in), ph->k);
+        const cplx path_phase = cexp(CMPLX(0.0, v3dot(qb, v3sub(ph->pos, ph->r1))));
+        project_to_lab(Erm * amp * path_phase, Ern * amp * path_phase, &P_exit, &Erx, &Ery);
+      }
+      accumulate_stokes(s, tally, it, jp, t_idx, Efx, Efy, Erx, Ery);
+    }
+  }
+  *hits += 1;
+}
+
 /* SensorsGroup::record_hit, src/detector.cpp:178-270 */
 static int record_hit(const lmc_o_handle *h, ophoton *ph, double **tallies, uint64_t *hits)
 {
@@ -1231,6 +1421,11 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
     const int med_idx = h->scene.layers[scatter_layer].medium;  /* :423-426 */
     const omedium *sm = &h->media[med_idx];
     ph->active_medium = med_idx;
+    for (int si = 0; si < h->scene.n_sensors; ++si) {             /* :419-426 run_estimators */
+      const osensor *es = &h->sensors[si];
+      if (es->p.estimator && es->p.kind == LMC_O_SENSOR_FARFIELD_CBS)
+        estimate_farfield_cbs(h, es, tallies[si], ph, med_idx, &hits[si]);
+    }
     if (t_adj)
       oadj_flight_scatter(h, last_seg_med, step);
 
@@ -1370,12 +1565,14 @@ lmc_o_handle *lmc_oracle_create(const lmc_o_scene *scene, char *err, int err_len
       lmc_oracle_destroy(h);
       return NULL;
     }
-  for (int i = 0; i < scene->n_media; ++i)
+  for (int i = 0; i < scene->n_media; ++i) {
     if (omedium_init(&h->media[i], &scene->media[i]) != 0) {
       snprintf(err, (size_t)err_len, "medium %d: bad parameters", i);
       lmc_oracle_destroy(h);
       return NULL;
     }
+    h->media[i].I_norm = compute_I_norm(&h->media[i]);
+  }
   for (int l = 1; l < scene->n_layers; ++l)                     /* sample.cpp:155-158 */
     h->interfaces[h->n_interfaces++] = scene->layers[l].z_min;
   /* z_layers (detector.hpp:46-48, detector.cpp:166-176): a key per plane within 1e-9 */

@@ -104,6 +104,7 @@ typedef struct lmc_o_sensor {
   double len_x, len_y, len_t, dx, dy, dt;
   /* far-field sensors (len_t and dt above are the time axis) */
   double theta_max_grid, phi_max_grid, dtheta, dphi;
+  double theta_pp_max;                    /* estimator: theta cap of the grid (0: none) */
 } lmc_o_sensor;
 
 typedef struct lmc_o_scene {

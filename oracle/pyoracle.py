@@ -65,7 +65,7 @@ class Sensor(C.Structure):
                 ("len_x", C.c_double), ("len_y", C.c_double), ("len_t", C.c_double),
                 ("dx", C.c_double), ("dy", C.c_double), ("dt", C.c_double),
                 ("theta_max_grid", C.c_double), ("phi_max_grid", C.c_double),
-                ("dtheta", C.c_double), ("dphi", C.c_double)]
+                ("dtheta", C.c_double), ("dphi", C.c_double), ("theta_pp_max", C.c_double)]
 
 
 class Scene(C.Structure):
@@ -223,6 +223,7 @@ def scene_from_spec(spec: dict) -> Scene:
             q.len_t = float(s.get("len_t", 0.0))
             q.dtheta = float(s["d_theta"])
             q.dphi = float(s["d_phi"])
+            q.theta_pp_max = float(s.get("theta_pp_max", 0.0))
             q.dt = float(s.get("d_t", 0.0))
         else:
             q.z = float(s["z"])

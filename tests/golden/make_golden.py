@@ -17,6 +17,7 @@ tallies and hit counts:
     python tests/golden/make_golden.py        (needs oracle/_ref; run `make -C oracle ref`)
     python tests/golden/make_golden.py stat   (the replica fixtures only)
     python tests/golden/make_golden.py farfield  (far-field fluence from reference records)
+    python tests/golden/make_golden.py estimator (estimator-mode FarFieldCBS, Philox stream)
 
 The fixtures pin the oracle (tests/test_oracle_golden.py) and the GPU path
 (tests/test_gpu_golden.py) without the reference present at test time.
@@ -126,6 +127,37 @@ def stat_main():
         print("wrote", run_stat_reference(spec["name"]))
 
 
+def estimator_scenes():
+    """Estimator-mode FarFieldCBS (the reference's last-flight CBS estimate at every
+    scattering vertex): one semi-infinite Mie medium with the cfg-0 grid, and the
+    two-layer slab with time bins, a 2-D angular grid and a theta cap, where the
+    straight rays to the detector cross the interface."""
+    a = W.mie_cbs_small(300, 31)
+    a["name"] = "estimator_mie"
+    a["media"][0].update(mu_a=0.2)
+    a["sensors"] = [dict(a["sensors"][0], estimator=True)]
+    b = W.bilayer_rgd_mie(200, 32)
+    b["name"] = "estimator_bilayer"
+    b["media"][0].update(mu_a=0.5)
+    b["media"][1].update(mu_a=0.5)
+    b["sensors"] = [{"kind": "farfield_cbs", "theta_max": 0.2, "phi_max": 2 * W.PI, "len_t": 12.0,
+                     "d_theta": 0.01, "d_phi": W.PI / 2, "d_t": 2.0, "estimator": True,
+                     "theta_pp_max": 0.15},
+                    {"kind": "planar_fluence", "z": 0.0, "len_x": 4.0, "len_y": 4.0, "len_t": 0.0,
+                     "dx": 0.5, "dy": 0.5, "d_t": 0.0, "absorb": True}]
+    return [a, b]
+
+
+def estimator_main():
+    meta = {}
+    for spec in estimator_scenes():
+        name = spec["name"]
+        np.savez_compressed(os.path.join(HERE, f"ref_philox_{name}.npz"),
+                            **run_flavour("replay", name, fmt=0, source="estimator_scenes"))
+        meta[name] = {"n_photons": spec["n_photons"], "seed": spec["seed"]}
+    print("wrote", meta)
+
+
 FF_GRID = {"theta_max": 1.5707963267948966, "phi_max": 2 * 3.141592653589793, "len_t": 20.0,
            "d_theta": 3.141592653589793 / 36, "d_phi": 2 * 3.141592653589793 / 12, "d_t": 2.0}
 
@@ -221,20 +253,20 @@ def farfield_main():
     print("wrote", path, len(recs), "records")
 
 
-def run_flavour(flavour, scene_name, fmt=None):
+def run_flavour(flavour, scene_name, fmt=None, source="golden_scenes"):
     """Run one scene in a fresh interpreter (each reference flavour is a module
     named luminis_mc) and return {sensor index: tally, 'hits': [...]}."""
     code = f"""
 import sys, json, glob, ctypes, numpy as np
 sys.path.insert(0, {REPO!r}); sys.path.insert(0, {os.path.join(REPO, 'luminis-mc_b200')!r})
-from tests.golden.make_golden import golden_scenes
+from tests.golden.make_golden import golden_scenes, estimator_scenes
 from luminis_mc_b200 import workloads as W
 from oracle import pyoracle as O
 lm = O.reference_module({flavour!r}); lm.set_log_level(lm.LogLevel.off)
 if {fmt is not None!r}:
     so = ctypes.CDLL(glob.glob({os.path.join(REPO, 'oracle', '_ref', flavour, 'luminis_mc', '_core*.so')!r})[0])
     so.lmc_replay_set_format({fmt if fmt is not None else 0})
-spec = [s for s in golden_scenes() if s["name"] == {scene_name!r}][0]
+spec = [s for s in {source}() if s["name"] == {scene_name!r}][0]
 cfg, hs, keep = W.build(lm, spec, n_threads=1)
 lm.run_simulation_parallel(cfg)
 out = {{}}
@@ -273,5 +305,7 @@ if __name__ == "__main__":
         stat_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "farfield":
         farfield_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "estimator":
+        estimator_main()
     else:
         main()

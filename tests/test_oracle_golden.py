@@ -135,3 +135,18 @@ def test_farfield_fluence_pinned_by_reference_records():
                                "ref_farfield_fluence_small.npz"))["sensor0"]
     got = O.Oracle(spec).run(spec["n_photons"], spec["seed"], rng="philox_u53").tallies[0]
     np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("name", ["estimator_mie", "estimator_bilayer"])
+def test_oracle_estimator_reproduces_reference(name):
+    """Estimator-mode FarFieldCBS (the last-flight CBS estimate at every vertex): the
+    oracle's tallies and hit counts equal the reference's on the Philox stream
+    (tests/golden/ref_philox_estimator_*.npz, made by the replay build)."""
+    from tests.golden.make_golden import estimator_scenes
+    spec = [s for s in estimator_scenes() if s["name"] == name][0]
+    g = np.load(os.path.join(GOLDEN, f"ref_philox_{name}.npz"))
+    res = O.Oracle(spec).run(spec["n_photons"], spec["seed"], rng="philox_u53")
+    for i, t in enumerate(res.tallies):
+        ref = g[f"sensor{i}"]
+        np.testing.assert_allclose(t, ref, rtol=1e-13, atol=1e-13 * np.abs(ref).max())
+        assert res.hits[i] == g["hits"][i]
