@@ -124,6 +124,8 @@ typedef struct lmc_sensor_desc {
   int f_events; int events_min, events_max;
   double len_x, len_y, len_t, dx, dy, dt;              /* planar sensors            */
   double theta_max_grid, phi_max_grid, dtheta, dphi;   /* far-field sensors         */
+  double theta_pp_max;          /* estimator-mode FarFieldCBS: theta cap of the estimated
+                                   grid, <= 0 none (FarFieldCBSSensor::theta_pp_max)   */
 } lmc_sensor_desc;
 
 /* The scene: Sample + Laser + SensorsGroup of a SimConfig

@@ -24,6 +24,7 @@ struct Medium {
   const float4 *amp_f;
   double mu_s;                           // scattering coefficient (likelihood-ratio scores)
   float mu_s_f, pad_s;
+  double I_norm;                         // int (|S1|^2 + |S2|^2) sin(theta), the estimator's p(Omega)
 };
 
 struct Layer {
@@ -36,9 +37,11 @@ struct Sensor {
   int f_theta, f_phi, f_pos, f_dir, f_events, direction, events_min, events_max;
   double cos_min, cos_max, phi_min, phi_max, x_min, x_max, y_min, y_max;
   double len_x, len_y, len_t, dx, dy, dt, dtheta, dphi;
-  int N_t, N_x, N_y, N_theta, N_phi, pad;
+  int N_t, N_x, N_y, N_theta, N_phi;
+  int est_n;                             // estimator-mode FarFieldCBS: bins estimated
   unsigned long long tally_off;          // offset in doubles into the tally buffer
   unsigned long long plane_stride;       // doubles between Stokes planes
+  const double4 *est_bins;               // per estimated bin: s_out (x, y, z), dOmega dphi
 };
 
 struct Laser {

@@ -951,6 +951,305 @@ __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData
   }
 }
 
+// ------------------------------------------------ last-flight CBS estimator
+// FarFieldCBSSensor::process_estimation (src/detector.cpp:1315-1566).  At every
+// scattering vertex, before the scatter is sampled, the photon is forced toward the
+// centre of every angular bin of an estimator-mode FarFieldCBS grid.  The bin gets the
+// weight w mu_s / mu_t x transmittance to the plane x p(Omega) dOmega, with
+// p = F / (pi I_norm), and the forward field.  From the second vertex on it also gets
+// the reverse (CBS) field with its geometric phase.  Computed in binary64 whatever the
+// transport precision.  One thread runs all bins of its own vertex, starting at a
+// lane-dependent bin so that the lanes of a warp update different tally cells at
+// each step.
+struct EstVertex {
+  double pos[3], P[9], P1[9], r1[3];
+  Cx<double> Em, En, T[4];      // Jones vector; interior product including the newest event
+  double w, opath;
+  unsigned long long index;
+  int events, med, first_med, pad;
+};
+
+__device__ __forceinline__ V3<double> drow(const double *P, int r)
+{
+  return v3<double>(P[3 * r], P[3 * r + 1], P[3 * r + 2]);
+}
+
+// Stages A + B of the reverse path with P_{n-1} = the current frame
+// (src/detector.cpp:1079-1118).
+__device__ __forceinline__ void est_prefix(const Scene &sc, const double *Pnm1, const Cx<double> *T,
+                                           int med_n, Cx<double> &Om, Cx<double> &On)
+{
+  const Laser &L = sc.laser;
+  const V3<double> m0 = v3<double>(L.m[0], L.m[1], L.m[2]);
+  const V3<double> n0 = v3<double>(L.n[0], L.n[1], L.n[2]);
+  const V3<double> s0 = v3<double>(L.dir[0], L.dir[1], L.dir[2]);
+  const Cx<double> E0m = {L.E[0], L.E[1]}, E0n = {L.E[2], L.E[3]};
+  const V3<double> mnm1 = drow(Pnm1, 0), nnm1 = drow(Pnm1, 1), snm1 = drow(Pnm1, 2);
+  const V3<double> s_out_a = vscale(snm1, -1.0);
+  Cx<double> Sa2, Sa1;
+  amplitudes<double>(sc.media[med_n], unit_angle(s0, s_out_a), Sa2, Sa1);
+  const V3<double> np_ = safe_unit(vcross_unit(s0, s_out_a), n0);
+  const V3<double> mp_in = safe_unit(vcross_unit(np_, s0), m0);
+  const V3<double> mp_out = safe_unit(vcross_unit(np_, s_out_a), mnm1);
+  double r00 = vdot(mp_in, m0), r01 = vdot(mp_in, n0), r10 = vdot(np_, m0), r11 = vdot(np_, n0);
+  Cx<double> Em = cadd(cmul(cscale(Sa2, r00), E0m), cmul(cscale(Sa2, r01), E0n));
+  Cx<double> En = cadd(cmul(cscale(Sa1, r10), E0m), cmul(cscale(Sa1, r11), E0n));
+  const V3<double> nn1 = vscale(nnm1, -1.0);
+  r00 = vdot(mnm1, mp_out); r01 = vdot(mnm1, np_); r10 = vdot(nn1, mp_out); r11 = vdot(nn1, np_);
+  Cx<double> tm = cadd(cscale(Em, r00), cscale(En, r01));
+  Cx<double> tn = cadd(cscale(Em, r10), cscale(En, r11));
+  tn = {-tn.re, -tn.im};
+  Em = cadd(cmul(T[0], tm), cmul(T[2], tn));
+  En = cadd(cmul(T[1], tm), cmul(T[3], tn));
+  Om = Em;
+  On = {-En.re, -En.im};
+}
+
+// Stage C and the normalisation (src/detector.cpp:1122-1161).
+__device__ __forceinline__ void est_suffix(const Scene &sc, const double *P1, const double *Pn, int med_1,
+                                           Cx<double> Em, Cx<double> En, Cx<double> &Om, Cx<double> &On)
+{
+  const V3<double> m1 = drow(P1, 0), n1 = drow(P1, 1), s1 = drow(P1, 2);
+  const V3<double> mn = drow(Pn, 0), nn = drow(Pn, 1), sn = drow(Pn, 2);
+  const V3<double> s_in_c = vscale(s1, -1.0);
+  const V3<double> n1m = vscale(n1, -1.0);
+  Cx<double> Sc2, Sc1;
+  amplitudes<double>(sc.media[med_1], unit_angle(s_in_c, sn), Sc2, Sc1);
+  const V3<double> npp = safe_unit(vcross_unit(s_in_c, sn), n1m);
+  const V3<double> mpp_in = safe_unit(vcross_unit(npp, s_in_c), m1);
+  const V3<double> mpp_out = safe_unit(vcross_unit(npp, sn), mn);
+  double r00 = vdot(mpp_in, m1), r01 = vdot(mpp_in, n1m), r10 = vdot(npp, m1), r11 = vdot(npp, n1m);
+  const Cx<double> Fm = cadd(cmul(cscale(Sc2, r00), Em), cmul(cscale(Sc2, r01), En));
+  const Cx<double> Fn = cadd(cmul(cscale(Sc1, r10), Em), cmul(cscale(Sc1, r11), En));
+  r00 = vdot(mn, mpp_out); r01 = vdot(mn, npp); r10 = vdot(nn, mpp_out); r11 = vdot(nn, npp);
+  Cx<double> gm = cadd(cscale(Fm, r00), cscale(Fn, r01));
+  Cx<double> gn = cadd(cscale(Fm, r10), cscale(Fn, r11));
+  const double nrm = sqrt(cnorm(gm) + cnorm(gn));
+  if (nrm > 1e-300) {
+    gm = {gm.re / nrm, gm.im / nrm};
+    gn = {gn.re / nrm, gn.im / nrm};
+  } else {
+    gm = {0.0, 0.0};
+    gn = {0.0, 0.0};
+  }
+  Om = gm;
+  On = gn;
+}
+
+// Optical depth of a straight ray to the detector plane, layer by layer
+// (src/detector.cpp:52-102).
+__device__ __forceinline__ double est_optical_depth(const Scene &sc, const double *start, V3<double> dir,
+                                                    double L_total)
+{
+  double tau = 0.0, traveled = 0.0;
+  double px = start[0], py = start[1], pz = start[2];
+  int layer = layer_index_at<double>(sc, pz);
+  if (layer >= sc.n_layers)
+    return 0.0;
+  if (sc.n_layers == 1)
+    return sc.media[sc.layers[layer].medium].mu_t * L_total;
+  const double dz = dir.z;
+  for (int guard = 0; guard <= 2 * LMC_MAX_LAYERS && traveled < L_total - 1e-15; ++guard) {
+    const double remaining = L_total - traveled;
+    const double mu = sc.media[sc.layers[layer].medium].mu_t;
+    double seg = remaining;
+    if (fabs(dz) > 1e-15) {
+      double zi;
+      if (find_next_interface<double>(sc, pz, pz + dz * remaining, zi)) {
+        const double sd = (zi - pz) / dz;
+        if (sd > 1e-15 && sd < remaining)
+          seg = sd;
+      }
+    }
+    tau += mu * seg;
+    px += dir.x * seg;
+    py += dir.y * seg;
+    pz += dir.z * seg;
+    traveled += seg;
+    if (seg >= remaining - 1e-15)
+      break;
+    const int next = layer_index_at<double>(sc, pz + ((dz > 0) ? 1e-12 : -1e-12));
+    if (next >= sc.n_layers)
+      break;
+    layer = next;
+  }
+  return tau;
+}
+
+template <typename R>
+__device__ __noinline__ void estimate_vertex(const Scene &sc, const RunParams &rp, const EstVertex v,
+                                             unsigned long long *s_hits)
+{
+  const Laser &L = sc.laser;
+  const V3<double> s_in = v3<double>(L.dir[0], L.dir[1], L.dir[2]);
+  const V3<double> m_cur = drow(v.P, 0), n_cur = drow(v.P, 1), s_cur = drow(v.P, 2);
+  const Medium &med = sc.media[v.med];
+  const unsigned lane = threadIdx.x & 31u;
+  for (int si = 0; si < sc.n_sensors; ++si) {
+    const Sensor &s = sc.sensors[si];
+    if (s.kind != LMC_SENSOR_FARFIELD_CBS || !s.estimator)
+      continue;
+    if (s.f_events && (v.events < s.events_min || v.events > s.events_max))
+      continue;
+    if (med.I_norm < 1e-300)
+      continue;
+    const double w_scatter = v.w * (med.mu_s / med.mu_t);
+    if (w_scatter < 1e-300)
+      continue;
+    const bool multi = v.events >= 1;
+    Cx<double> pre_m = {0.0, 0.0}, pre_n = {0.0, 0.0};
+    if (multi)
+      est_prefix(sc, v.P, v.T, v.med, pre_m, pre_n);
+    const double t_launch = (s.dt > 0) ? emission_time<R>(L, rp, v.index) : 0.0;
+    double *base = rp.tallies + s.tally_off;
+    const unsigned long long P = s.plane_stride;
+    const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
+    const int nb = s.est_n;
+    for (int k = 0; k < nb; ++k) {
+      int b = k + (int)lane;
+      if (b >= nb)
+        b -= nb * (b / nb);
+      const double4 bin = s.est_bins[b];
+      const V3<double> s_out = v3<double>(bin.x, bin.y, bin.z);
+      const double denom = s_out.z;                        // plane z = 0, normal +z
+      if (fabs(denom) < 1e-14)
+        continue;
+      const double Lp = (-v.pos[2]) / denom;
+      if (Lp <= 0.0)
+        continue;
+      const double Tr = exp(-est_optical_depth(sc, v.pos, s_out, Lp));
+      if (Tr < 1e-20)
+        continue;
+      const V3<double> pv = vcross_unit(s_cur, s_out);
+      const double pn = sqrt(vdot(pv, pv));
+      if (pn < 1e-12)
+        continue;
+      const V3<double> p_hat = vscale(pv, 1.0 / pn);
+      const double sin_phi = -vdot(m_cur, p_hat);
+      const double cos_phi = vdot(n_cur, p_hat);
+      double cdot = vdot(s_cur, s_out);
+      cdot = cdot > 1.0 ? 1.0 : (cdot < -1.0 ? -1.0 : cdot);
+      const double th_scat = acos(cdot);
+      Cx<double> S2, S1;
+      amplitudes<double>(med, th_scat, S2, S1);
+      const double s22 = cnorm(S2), s11 = cnorm(S1);
+      const double Emm = cnorm(v.Em), Enn = cnorm(v.En);
+      const double c2 = cos_phi * cos_phi, sn2 = sin_phi * sin_phi;
+      const double e12 = v.Em.re * v.En.re + v.Em.im * v.En.im;
+      const double F = Emm * (s22 * c2 + s11 * sn2) + Enn * (s22 * sn2 + s11 * c2) +
+                       2.0 * e12 * (s22 - s11) * sin_phi * cos_phi;
+      if (F < 1e-300)
+        continue;
+      const double prob_bin = (F / (3.141592653589793 * med.I_norm)) * bin.w;
+      const double w_bin = w_scatter * Tr * prob_bin;
+      if (w_bin < 1e-300)
+        continue;
+      const int t_idx = time_bin(s, t_launch + (v.opath + Lp));
+      if (t_idx < 0)
+        continue;
+      double sa, ca;
+      sincos(L.k * Lp, &sa, &ca);
+      const double sw = sqrt(w_bin);
+      const Cx<double> amp = {sw * ca, sw * sa};
+      // exit frame A(theta, phi) P (src/detector.cpp:1027-1045)
+      double st, ct;
+      sincos(th_scat, &st, &ct);
+      double Pe[9];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double mj = v.P[j], nj = v.P[3 + j], sj = v.P[6 + j];
+        Pe[j] = ct * cos_phi * mj + ct * sin_phi * nj + (-st) * sj;
+        Pe[3 + j] = -sin_phi * mj + cos_phi * nj + 0.0 * sj;
+        Pe[6 + j] = st * cos_phi * mj + st * sin_phi * nj + ct * sj;
+      }
+      // forward field (S R(phi)) E / sqrt(F) (src/detector.cpp:121-160)
+      const double inv = 1.0 / sqrt(F);
+      const Cx<double> T00 = cscale(S2, cos_phi), T01 = cscale(S2, sin_phi);
+      const Cx<double> T10 = cscale(S1, -sin_phi), T11 = cscale(S1, cos_phi);
+      const Cx<double> Efm = cmul(cscale(cadd(cmul(T00, v.Em), cmul(T01, v.En)), inv), amp);
+      const Cx<double> Efn = cmul(cscale(cadd(cmul(T10, v.Em), cmul(T11, v.En)), inv), amp);
+      const Cx<double> Efx = cadd(cscale(Efm, Pe[0]), cscale(Efn, Pe[3]));
+      const Cx<double> Efy = cadd(cscale(Efm, Pe[1]), cscale(Efn, Pe[4]));
+      Cx<double> Erx = {0.0, 0.0}, Ery = {0.0, 0.0};
+      if (multi) {
+        Cx<double> Rm, Rn;
+        est_suffix(sc, v.P1, Pe, v.first_med, pre_m, pre_n, Rm, Rn);
+        const double qx = (s_out.x + s_in.x) * L.k, qy = (s_out.y + s_in.y) * L.k,
+                     qz = (s_out.z + s_in.z) * L.k;
+        const double arg = qx * (v.pos[0] - v.r1[0]) + qy * (v.pos[1] - v.r1[1]) + qz * (v.pos[2] - v.r1[2]);
+        double sp_, cp_;
+        sincos(arg, &sp_, &cp_);
+        const Cx<double> pp = {cp_, sp_};
+        const Cx<double> Rm2 = cmul(cmul(Rm, amp), pp), Rn2 = cmul(cmul(Rn, amp), pp);
+        Erx = cadd(cscale(Rm2, Pe[0]), cscale(Rn2, Pe[3]));
+        Ery = cadd(cscale(Rm2, Pe[1]), cscale(Rn2, Pe[4]));
+      }
+      // accumulate_stokes (src/detector.cpp:1194-1226)
+      const Cx<double> Ex = cadd(Efx, Erx), Ey = cadd(Efy, Ery);
+      const Cx<double> c_xy = cmul(Ex, Cx<double>{Ey.re, -Ey.im});
+      const Cx<double> f_xy = cmul(Efx, Cx<double>{Efy.re, -Efy.im});
+      const Cx<double> r_xy = cmul(Erx, Cx<double>{Ery.re, -Ery.im});
+      const double c0 = cnorm(Ex) + cnorm(Ey), c1 = cnorm(Ex) - cnorm(Ey);
+      const double c2s = 2.0 * c_xy.re, c3 = 2.0 * c_xy.im;
+      const double i0 = cnorm(Efx) + cnorm(Efy) + cnorm(Erx) + cnorm(Ery);
+      const double i1 = cnorm(Efx) - cnorm(Efy) + cnorm(Erx) - cnorm(Ery);
+      const double i2 = 2.0 * (f_xy.re + r_xy.re), i3 = 2.0 * (f_xy.im + r_xy.im);
+      const unsigned long long cell = (unsigned long long)(b / s.N_phi) * s.N_phi + (b % s.N_phi);
+      add4(base, P, cell, c0, c1, c2s, c3);
+      add4(base + 4 * P, P, cell, i0, i1, i2, i3);
+      if (t_idx >= 1) {
+        add4(base, P, t_idx * tstride + cell, c0, c1, c2s, c3);
+        add4(base + 4 * P, P, t_idx * tstride + cell, i0, i1, i2, i3);
+      }
+    }
+    atomicAdd(s_hits + si, 1ull);
+  }
+}
+
+// The vertex a photon is at, as the estimator reads it.
+template <typename R>
+__device__ __forceinline__ void estimate_at_vertex(const Scene &sc, const RunParams &rp, const Photon<R> &ph,
+                                                   const Side<R> &side, int med_idx, unsigned long long *s_hits)
+{
+  const int tid = threadIdx.x;
+  EstVertex v;
+  v.pos[0] = ph.px; v.pos[1] = ph.py; v.pos[2] = ph.pz;
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    v.P[j] = ph.P[j];
+    v.P1[j] = side.first[3 + j][tid];
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    v.r1[j] = side.first[j][tid];
+  v.Em = {ph.Em.re, ph.Em.im};
+  v.En = {ph.En.re, ph.En.im};
+  v.w = ph.w;
+  v.opath = ph.opath;
+  v.index = ph.index();
+  v.events = (int)ph.events;
+  v.med = med_idx;
+  v.first_med = side.first_med[tid];
+  // interior product for the estimated path (src/detector.cpp:1462-1469): the
+  // newest event's raw factor folded into the committed product (from 2 events on)
+  const Cx<double> T0 = {side.T[0][tid], side.T[1][tid]}, T1 = {side.T[2][tid], side.T[3][tid]};
+  const Cx<double> T2 = {side.T[4][tid], side.T[5][tid]}, T3 = {side.T[6][tid], side.T[7][tid]};
+  if (ph.events >= 2) {
+    const Cx<double> pS2 = {side.last[0][tid], side.last[1][tid]};
+    const Cx<double> pS1 = {side.last[2][tid], side.last[3][tid]};
+    const double pc = side.last[4][tid], ps = side.last[5][tid];
+    const Cx<double> B00 = cscale(pS2, pc), B01 = cscale(pS2, ps), B10 = cscale(pS1, -ps), B11 = cscale(pS1, pc);
+    v.T[0] = cadd(cmul(B00, T0), cmul(B01, T2));
+    v.T[1] = cadd(cmul(B00, T1), cmul(B01, T3));
+    v.T[2] = cadd(cmul(B10, T0), cmul(B11, T2));
+    v.T[3] = cadd(cmul(B10, T1), cmul(B11, T3));
+  } else {
+    v.T[0] = T0; v.T[1] = T1; v.T[2] = T2; v.T[3] = T3;
+  }
+  v.pad = 0;
+  estimate_vertex<R>(sc, rp, v, s_hits);
+}
+
 // Sensor::check_conditions (src/detector.cpp:374-417)
 template <typename R>
 __device__ __forceinline__ bool check_conditions(const Sensor &s, double hx, double hy, const Photon<R> &ph,
@@ -1170,7 +1469,7 @@ constexpr int kMaxRejectionTrials = 1 << 16;
 
 // One loop iteration of run_photon (src/simulation.cpp:297-614).  Returns the
 // photon's fate (kAlive if it continues).
-template <typename R, bool kQueue, bool kAdj>
+template <typename R, bool kQueue, bool kAdj, bool kEst = false>
 __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, Photon<R> &ph,
                                           Side<R> &side, Flight<R> &fl, Counters &cnt,
                                           unsigned long long *s_hits)
@@ -1245,6 +1544,8 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   const Medium &m = sc.media[med_idx];
   if (kAdj)
     flight_scatter<R>(sc, fl, fl.seg_med, fl.seg_len);
+  if (kEst)                                                   // :419-426 run_estimators
+    estimate_at_vertex<R>(sc, rp, ph, side, med_idx, s_hits);
 
   const R theta = sample_theta<R>(m, uniform<R>(ph.rng, rp));  // :429
   Cx<R> S2, S1;
@@ -1444,10 +1745,11 @@ __device__ __forceinline__ int sweep_scene(const RunParams &rp, unsigned long lo
   return lo;
 }
 
-// kAdj: likelihood-ratio run (queued mode only).  kSweep: g_scene is an array of
+// kEst: the scene has an estimator-mode FarFieldCBS sensor (estimate_vertex at every
+// vertex).  kAdj: likelihood-ratio run (queued mode only).  kSweep: g_scene is an array of
 // rp.n_scenes scenes read from global memory (L1-cached), photon g belongs to scene
 // sweep_scene(g), and each lane follows its own photon's scene.
-template <typename R, bool kQueue, int kMinBlocks, bool kAdj = false, bool kSweep = false>
+template <typename R, bool kQueue, int kMinBlocks, bool kAdj = false, bool kSweep = false, bool kEst = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
   __shared__ __align__(16) unsigned char s_raw[kSweep ? 16 : sizeof(Scene)];
@@ -1500,7 +1802,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
     if (__all_sync(kFull, done))
       break;
     if (alive) {
-      const int fate = event_step<R, kQueue, kAdj>(*scp, rp, ph, side, fl, cnt, s_hits);
+      const int fate = event_step<R, kQueue, kAdj, kEst>(*scp, rp, ph, side, fl, cnt, s_hits);
       if (fate != kAlive) {
         alive = false;
         cnt.draws += ph.rng.draw;

@@ -65,6 +65,7 @@ struct lmc_handle {
   unsigned cbs_mask = 0;                 // sensors that need the CBS fields of a hit
   bool queued = false;                   // every sensor plane at z <= 0: queued kernel pair
   int max_planes = 0;                    // most sensor planes of any scene
+  bool has_est = false;                  // an estimator-mode FarFieldCBS sensor
   // sweep handles (lmc_create_sweep): n_scenes scenes in one device array
   bool sweep = false;
   int n_scenes = 1;
@@ -162,9 +163,6 @@ lmc_status validate(const lmc_scene *s)
     const lmc_sensor_desc &S = s->sensors[i];
     if (S.kind < 0 || S.kind > 3)
       return fail(LMC_ERR_INVALID, "unknown sensor kind");
-    if (S.kind == LMC_SENSOR_FARFIELD_CBS && S.estimator)
-      return fail(LMC_ERR_UNSUPPORTED,
-                  "estimator-mode FarFieldCBSSensor (process_estimation) is not implemented");
     if (S.kind == LMC_SENSOR_FARFIELD_CBS || S.kind == LMC_SENSOR_FARFIELD_FLUENCE) {
       if (!(S.dtheta > 0) || !(S.dphi > 0) || !(S.theta_max_grid > 0) || !(S.phi_max_grid > 0))
         return fail(LMC_ERR_INVALID, "far-field sensor bin widths and extents must be positive");
@@ -242,8 +240,40 @@ struct SceneBuild {
   int sensor_dims[LMC_MAX_SENSORS][4] = {};
   unsigned cbs_mask = 0;
   bool queued = false;
+  bool has_est = false;                  // an estimator-mode FarFieldCBS sensor
+  size_t est_off[LMC_MAX_SENSORS] = {};  // its bin table in the arena
   MedOff mo[LMC_MAX_MEDIA] = {};
 };
+
+// int_0^pi (|S1|^2 + |S2|^2) sin(theta) dtheta over the medium's amplitude table,
+// midpoint rule with 2048 points (src/detector.cpp:106-118); the table lookup is
+// DataTable's clamped lerp (src/table.cpp:100-118).
+double medium_I_norm(const lmc_medium_desc &M)
+{
+  const int n = 2048;
+  const double inv_dx = 1.0 / M.amp_dtheta;
+  const int last = M.amp_n - 1;
+  double acc = 0.0;
+  const double dth = M_PI / n;
+  for (int i = 0; i < n; i++) {
+    const double th = (i + 0.5) * dth;
+    const double pos = th * inv_dx;
+    double v[4];                                // s1.re, s1.im, s2.re, s2.im
+    if (pos <= 0.0 || pos >= (double)last) {
+      const int k = pos <= 0.0 ? 0 : last;
+      v[0] = M.amp_s1[2 * k]; v[1] = M.amp_s1[2 * k + 1];
+      v[2] = M.amp_s2[2 * k]; v[3] = M.amp_s2[2 * k + 1];
+    } else {
+      const int k = (int)pos;
+      const double t = pos - (double)k;
+      const double *a1 = M.amp_s1 + 2 * k, *a2 = M.amp_s2 + 2 * k;
+      v[0] = a1[0] + t * (a1[2] - a1[0]); v[1] = a1[1] + t * (a1[3] - a1[1]);
+      v[2] = a2[0] + t * (a2[2] - a2[0]); v[3] = a2[1] + t * (a2[3] - a2[1]);
+    }
+    acc += ((v[0] * v[0] + v[1] * v[1]) + (v[2] * v[2] + v[3] * v[3])) * std::sin(th);
+  }
+  return acc * dth;
+}
 
 // tally_base: offset (doubles) of this scene's first sensor in the tally buffer.
 void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned char> &arena, SceneBuild &b)
@@ -385,6 +415,37 @@ void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned cha
     }
     o.ad = put(ad.data(), ad.size() * sizeof(double4));
     o.af = put(af.data(), af.size() * sizeof(float4));
+    d.I_norm = medium_I_norm(M);
+  }
+  // Estimator-mode FarFieldCBS: the bin directions of the estimated grid around the
+  // backscatter axis -s_in of the launch frame, with their solid angles
+  // (src/detector.cpp:886-904, :1476-1498), evaluated once here.
+  for (int i = 0; i < s->n_sensors; ++i) {
+    const lmc_sensor_desc &S = s->sensors[i];
+    dev::Sensor &d = sc.sensors[i];
+    if (S.kind != LMC_SENSOR_FARFIELD_CBS || !d.estimator)
+      continue;
+    const double th_cap = (S.theta_pp_max > 0.0) ? std::min(S.theta_pp_max, S.theta_max_grid)
+                                                 : S.theta_max_grid;
+    const int i_max = std::min(d.N_theta, (int)(th_cap / S.dtheta));
+    const double *e1 = L.local_m, *e2 = L.local_n, *s_in = L.direction;
+    std::vector<double4> bins;
+    for (int it = 0; it < i_max; ++it) {
+      const double th_det = (it + 0.5) * S.dtheta;
+      const double c_th = std::cos(th_det), s_th = std::sin(th_det);
+      const double dOmega_band = std::cos(it * S.dtheta) - std::cos((it + 1) * S.dtheta);
+      for (int jp = 0; jp < d.N_phi; ++jp) {
+        const double ph_det = (jp + 0.5) * S.dphi;
+        const double c_ph = std::cos(ph_det), s_ph = std::sin(ph_det);
+        double so[3];
+        for (int k = 0; k < 3; ++k)
+          so[k] = (e1[k] * (s_th * c_ph) + e2[k] * (s_th * s_ph)) + (s_in[k] * -1.0) * c_th;
+        bins.push_back(make_double4(so[0], so[1], so[2], dOmega_band * S.dphi));
+      }
+    }
+    d.est_n = (int)bins.size();
+    b.est_off[i] = bins.empty() ? 0 : put(bins.data(), bins.size() * sizeof(double4));
+    b.has_est = true;
   }
 }
 
@@ -403,6 +464,9 @@ void patch_tables(SceneBuild &b, unsigned char *base)
     d.amp_d = reinterpret_cast<const double4 *>(base + o.ad);
     d.amp_f = reinterpret_cast<const float4 *>(base + o.af);
   }
+  for (int i = 0; i < b.sc.n_sensors; ++i)
+    if (b.sc.sensors[i].est_n > 0)
+      b.sc.sensors[i].est_bins = reinterpret_cast<const double4 *>(base + b.est_off[i]);
 }
 
 // Device allocations shared by lmc_create and lmc_create_sweep: arena, scenes,
@@ -464,6 +528,7 @@ lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
   h->queued = b.queued;
   h->cbs_mask = b.cbs_mask;
   h->max_planes = b.sc.n_planes;
+  h->has_est = b.has_est;
   for (int i = 0; i < LMC_MAX_SENSORS; ++i) {
     h->sensor_off[i] = b.sensor_off[i];
     h->sensor_count[i] = b.sensor_count[i];
@@ -579,8 +644,12 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   if (opts->max_events < 0)
     return fail(LMC_ERR_INVALID, "max_events must be non-negative");
   const bool sw = h->sweep;
+  const bool est = h->has_est;
   if (sw && adj)
     return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs are not available for sweeps");
+  if (est && (adj || !h->queued))
+    return fail(LMC_ERR_UNSUPPORTED, "estimator-mode FarFieldCBS runs need every sensor plane at "
+                                     "z <= 0 and no likelihood-ratio outputs");
   for (int k = 0; k < h->n_scenes; ++k) {
     const dev::Scene &scn = sw ? h->scenes[k] : h->scene;
     for (int i = 0; i < scn.n_sensors; ++i)
@@ -640,7 +709,9 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   // 2-block (<=128 registers) variant; blocks_per_sm == 1 or 2 selects the latter
   const bool three = fp32 && h->queued && !adj && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
   const void *tk =
-      sw ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, false, true>
+      est ? (fp32 ? (const void *)dev::transport_kernel<float, true, 2, false, false, true>
+                  : (const void *)dev::transport_kernel<double, true, 1, false, false, true>)
+      : sw ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, false, true>
                  : (const void *)dev::transport_kernel<double, true, 2, false, true>)
       : adj ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, true>
                   : (const void *)dev::transport_kernel<double, true, 1, true>)
@@ -710,7 +781,12 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     const size_t pair = 2 * (size_t)(done / batch);
     if (stats)
       LMC_CUDA(cudaEventRecord(h->kev[pair], stream));
-    if (sw) {
+    if (est) {
+      if (fp32)
+        dev::transport_kernel<float, true, 2, false, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
+      else
+        dev::transport_kernel<double, true, 1, false, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
+    } else if (sw) {
       if (fp32)
         dev::transport_kernel<float, true, 3, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
       else
@@ -823,10 +899,11 @@ lmc_status lmc_create_sweep(const lmc_scene *scenes, int n_scenes, lmc_handle **
   h->queued = true;
   for (int k = 0; k < n_scenes; ++k) {
     build_scene(scenes + k, tally, arena, builds[k]);
-    if (!builds[k].queued) {
+    if (!builds[k].queued || builds[k].has_est) {
       delete h;
       return fail(LMC_ERR_UNSUPPORTED, "scene " + std::to_string(k) +
-                                           ": a sweep needs every sensor plane at z <= 0");
+                                           ": a sweep needs every sensor plane at z <= 0 and "
+                                           "no estimator-mode sensor");
     }
     lmc_handle::SceneLayout &L = h->layouts[k];
     L.tally_base = tally;
@@ -1099,6 +1176,9 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
   const lmc_status v = validate(s);
   if (v != LMC_OK)
     return v;
+  for (int i = 0; i < s->n_sensors; ++i)
+    if (s->sensors[i].kind == LMC_SENSOR_FARFIELD_CBS && s->sensors[i].estimator && s->sensors[i].z == 0.0)
+      return fail(LMC_ERR_UNSUPPORTED, "lmc_run_noalloc: estimator-mode FarFieldCBS is not available here");
   if (opts->precision != LMC_PRECISION_FP32 && opts->precision != LMC_PRECISION_FP64)
     return fail(LMC_ERR_INVALID, "unknown precision");
   if (opts->max_events < 0)

@@ -53,7 +53,7 @@ class SensorDesc(C.Structure):
                 ("len_x", C.c_double), ("len_y", C.c_double), ("len_t", C.c_double),
                 ("dx", C.c_double), ("dy", C.c_double), ("dt", C.c_double),
                 ("theta_max_grid", C.c_double), ("phi_max_grid", C.c_double),
-                ("dtheta", C.c_double), ("dphi", C.c_double)]
+                ("dtheta", C.c_double), ("dphi", C.c_double), ("theta_pp_max", C.c_double)]
 
 
 class SceneDesc(C.Structure):

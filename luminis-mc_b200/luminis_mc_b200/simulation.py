@@ -110,7 +110,12 @@ def _sensor_desc(d: N.SensorDesc, s) -> None:
         d.dtheta, d.dphi = s.dtheta, s.dphi
         d.len_t, d.dt = s.t_max, s.dt
         if isinstance(s, FarFieldCBSSensor) and s.phi_explicit:
+            if s.estimator_enabled:
+                raise NotImplementedError("estimator-mode FarFieldCBSSensor with explicit phi "
+                                          "slices is not supported by the GPU transport")
             d.phi_max_grid = s.N_phi * s.dphi       # the explicit slices set the column count
+        if isinstance(s, FarFieldCBSSensor):
+            d.theta_pp_max = s.theta_pp_max
     elif isinstance(s, PlanarFluenceSensor):
         d.len_x, d.len_y, d.len_t = s.len_x, s.len_y, s.len_t
         d.dx, d.dy, d.dt = s.dx, s.dy, s.dt
