@@ -469,6 +469,33 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
         "sequential_launches": total * world / (seq_ms * 1e-3),
         "workload": "256 single-layer Mie media, FarFieldCBS 100x1 each, seeded draws "
                     "(numpy default_rng(2026))"}
+
+    # estimator-mode FarFieldCBS (the reference's last-flight CBS estimate at every
+    # vertex), mie_cbs_small geometry with its 100-bin grid, against the reference's own
+    # estimator on this host's cores
+    espec = W.mie_cbs_small(200_000, 4242)
+    espec["sensors"] = [dict(espec["sensors"][0], estimator=True)]
+    ecfg, _, ekeep = W.build(lm, espec)
+    PE = int(espec["n_photons"])
+    for prec in ("fp64", "fp32"):
+        run = DeviceRun(ecfg, device=f"cuda:{local}")
+        run.run(20_000, 4242, precision=prec, stream=stream.cuda_stream)
+        flush.zero_()
+        st, _ = run.run(PE, 4242, begin=(1 + rank) * PE, precision=prec, stream=stream.cuda_stream)
+        run.close()
+        ms = max_ms(st["kernel_ms"])
+        out[f"estimator_{prec}"] = {"value": PE * world / (ms * 1e-3), "unit": "photons/s",
+                                    "workload": "mie_cbs_small, FarFieldCBS 100x1 in estimator mode",
+                                    "photons": PE}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rate, n, dt = reference_sample(espec, 6.0, os.cpu_count() or 1)
+            out["estimator_fp64"]["cpu_reference"] = {
+                "value": rate, "unit": "photons/s", "cores": os.cpu_count(),
+                "sample": f"{n} photons in {dt:.1f} s, reference run_simulation_parallel "
+                          f"(oracle/_ref/perf), estimator mode"}
+        except Exception as exc:
+            out["estimator_fp64"]["cpu_reference"] = {"value": None, "sample": f"unavailable: {exc}"}
     return out
 
 
