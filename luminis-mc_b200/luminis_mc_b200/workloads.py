@@ -18,6 +18,8 @@ Workloads (synthetic media; no dataset is involved):
   * ``mie_long_paths``     Mie r=1.0 um, mu_s=100/mm, mu_a=1e-4/mm, MAX_EVENTS
                            raised to 1e6, FarFieldCBS 400 bins to 0.02 rad and a
                            256 x 256 PlanarFieldSensor.
+  * ``mixture_bilayer``    a three-species MixtureLayer slab over the Mie medium.
+  * ``mixture_cbs_small``  a semi-infinite two-species MixtureLayer.
   * ``mie_sweep(i)``       one of 256 single-layer Mie media with seeded random
                            radius / mu_s / mu_a / photon count.
 """
@@ -137,8 +139,43 @@ def mie_sweep(i, seed=12345, count=256):
     return spec
 
 
+def mixture_bilayer(n_photons=10_000_000, seed=12345):
+    """A MixtureLayer of three co-located species -- polystyrene spheres r = 0.5 um
+    (n = 3e6 /mm^3, mu_s_i ~ 6.1/mm) and r = 0.25 um (1.5e7 /mm^3, ~2.3/mm) and RGD
+    spheres r = 0.1 um (2e9 /mm^3, ~4.6/mm), each with its own albedo -- in 0 <= z < 0.5
+    mm over the semi-infinite Mie medium.  Circular polarisation; FarFieldCBS 200 x 8,
+    PlanarFluence 100 x 100 x 32 time bins over 10 x 10 mm."""
+    spec = bilayer_rgd_mie(n_photons, seed)
+    spec["name"] = "mixture_bilayer"
+    spec["phases"].append(_mie_phase(0.25e-3))
+    spec["media"].append(_medium("mie", 2, 0.25e-3, 5.0, 0.2))
+    spec["layers"] = [{"species": [1, 0, 2], "densities": [3.0e6, 2.0e9, 1.5e7],
+                       "z_min": 0.0, "z_max": 0.5},
+                      {"medium": 1, "z_min": 0.5, "z_max": math.inf}]
+    spec["sensors"][1].update(dx=0.1, dy=0.1, len_t=31.0, d_t=1.0)
+    spec["sensors"].pop(2)
+    return spec
+
+
+def mixture_cbs_small(n_photons=1_000_000, seed=12345):
+    """A semi-infinite MixtureLayer of the r = 0.5 um Mie and r = 0.1 um RGD species
+    (3e6 and 2e9 /mm^3), linear pencil beam, FarFieldCBS 100 x 1 and PlanarFluence."""
+    spec = mie_cbs_small(n_photons, seed)
+    spec["name"] = "mixture_cbs_small"
+    spec["phases"].append({"kind": "rdemc", "wavelength": LAMBDA, "radius": 0.1e-3,
+                           "n_particle": N_SPHERE, "n_medium": N_WATER, "nDiv": 1000,
+                           "min": 0.0, "max": PI})
+    spec["media"].append(_medium("rgd", 1, 0.1e-3, 20.0, 0.05, 0.05))
+    spec["layers"] = [{"species": [0, 1], "densities": [3.0e6, 2.0e9],
+                       "z_min": 0.0, "z_max": math.inf}]
+    spec["sensors"].append({"kind": "planar_fluence", "z": 0.0, "len_x": 4.0, "len_y": 4.0,
+                            "len_t": 0.0, "dx": 0.25, "dy": 0.25, "d_t": 0.0, "absorb": True})
+    return spec
+
+
 WORKLOADS = {"mie_cbs_small": mie_cbs_small, "bilayer_rgd_mie": bilayer_rgd_mie,
-             "bilayer_hg": bilayer_hg, "mie_long_paths": mie_long_paths}
+             "bilayer_hg": bilayer_hg, "mie_long_paths": mie_long_paths,
+             "mixture_bilayer": mixture_bilayer, "mixture_cbs_small": mixture_cbs_small}
 
 
 # --------------------------------------------------------------------------- builder
@@ -175,7 +212,11 @@ def build(lm, spec, n_photons=None, seed=None, n_threads=None):
     keep += media
     sample = lm.Sample(spec.get("n_host", 1.0))
     for l in spec["layers"]:
-        sample.add_layer(media[l["medium"]], l["z_min"], l["z_max"])
+        if "species" in l:
+            sample.add_mixture_layer([media[i] for i in l["species"]],
+                                     [float(n) for n in l["densities"]], l["z_min"], l["z_max"])
+        else:
+            sample.add_layer(media[l["medium"]], l["z_min"], l["z_max"])
     L = spec["laser"]
     source = {"point": lm.LaserSource.Point, "uniform": lm.LaserSource.Uniform,
               "gaussian": lm.LaserSource.Gaussian}[L.get("source", "point")]

@@ -482,11 +482,22 @@ typedef struct {
   size_t n_doubles;
 } osensor;
 
+/* A layer's transport coefficients (Layer::mu_attenuation/mu_scattering/mu_absorption,
+ * sample_free_path): the wrapped medium's for a HomogeneousLayer, the aggregates of
+ * MixtureLayer's constructor (src/sample.cpp:41-88) for a mixture. */
+typedef struct {
+  double mu_s, mu_a, mu_t, mfp;
+  int n_species;                  /* 0: HomogeneousLayer (no species draw) */
+  int species[LMC_O_MAX_SPECIES];
+  double mu_s_i[LMC_O_MAX_SPECIES], cdf[LMC_O_MAX_SPECIES];
+} olayer;
+
 struct lmc_o_handle {
   lmc_o_scene scene;
   double light_speed;             /* 1 / n_host (src/sample.cpp:110-111) */
   ophase phase[LMC_O_MAX_PHASE];
   omedium media[LMC_O_MAX_MEDIA];
+  olayer layer[LMC_O_MAX_LAYERS];
   double interfaces[LMC_O_MAX_LAYERS];
   int n_interfaces;
   osensor sensors[LMC_O_MAX_SENSORS];
@@ -610,9 +621,83 @@ static int is_inside(const lmc_o_handle *h, v3 p)             /* :268-288 */
   return 1;
 }
 
-static const omedium *layer_medium(const lmc_o_handle *h, int layer)
+static const olayer *layer_at(const lmc_o_handle *h, int layer)
 {
-  return &h->media[h->scene.layers[layer].medium];
+  return &h->layer[layer];
+}
+
+/* MixtureLayer constructor (src/sample.cpp:41-88): mu_s_i = n_i sigma_s_i, the
+ * absorption that keeps each species' albedo, mu_t, mfp = 1 / mu_s_total and the
+ * selection CDF over mu_s_i (last entry exactly 1).  A HomogeneousLayer takes its
+ * medium's coefficients (include/luminis/core/sample.hpp:142-144). */
+static int olayer_init(const lmc_o_handle *h, const lmc_o_layer *p, olayer *L, char *err, int err_len)
+{
+  memset(L, 0, sizeof(*L));
+  if (p->n_species <= 0) {
+    const omedium *m = &h->media[p->medium];
+    L->mu_s = m->p.mu_s;
+    L->mu_a = m->p.mu_a;
+    L->mu_t = m->mu_t;
+    L->mfp = m->p.mfp;
+    return 0;
+  }
+  if (p->n_species > LMC_O_MAX_SPECIES) {
+    snprintf(err, (size_t)err_len, "MixtureLayer: too many species");
+    return -1;
+  }
+  L->n_species = p->n_species;
+  double mu_s_total = 0.0, mu_a_total = 0.0;
+  for (int i = 0; i < p->n_species; ++i) {
+    const int mi = p->species[i];
+    if (mi < 0 || mi >= h->scene.n_media) {
+      snprintf(err, (size_t)err_len, "MixtureLayer: species pointer must not be null.");
+      return -1;
+    }
+    const omedium *sp = &h->media[mi];
+    const ophase *ph = &h->phase[sp->phase];
+    if (ph->p.kind != LMC_O_PHASE_MIE && ph->p.kind != LMC_O_PHASE_RDEMC) {
+      /* PhaseFunction::scattering_cross_section exits for other phase functions */
+      snprintf(err, (size_t)err_len, "PhaseFunction::scattering_cross_section: Not implemented");
+      return -1;
+    }
+    const double mu_s = p->number_density[i] * ph->sigma_s;
+    L->species[i] = mi;
+    L->mu_s_i[i] = mu_s;
+    mu_s_total += mu_s;
+    if (sp->p.mu_s > 0.0)
+      mu_a_total += mu_s * (sp->p.mu_a / sp->p.mu_s);
+  }
+  if (mu_s_total <= 0.0) {
+    snprintf(err, (size_t)err_len, "MixtureLayer: total mu_s must be positive");
+    return -1;
+  }
+  L->mu_s = mu_s_total;
+  L->mu_a = mu_a_total;
+  L->mu_t = mu_s_total + mu_a_total;
+  L->mfp = 1.0 / mu_s_total;
+  double acc = 0.0;
+  for (int i = 0; i < p->n_species; ++i) {
+    acc += L->mu_s_i[i] / mu_s_total;
+    L->cdf[i] = acc;
+  }
+  L->cdf[p->n_species - 1] = 1.0;
+  return 0;
+}
+
+/* Layer::select_scatter_medium: the lone medium without a draw (HomogeneousLayer),
+ * or lower_bound of one uniform on the selection CDF (src/sample.cpp:96-104). */
+static int select_scatter_medium(const lmc_o_handle *h, int layer, orng *rng)
+{
+  const olayer *L = &h->layer[layer];
+  if (L->n_species == 0)
+    return h->scene.layers[layer].medium;
+  const double u = orng_uniform(rng);
+  int idx = 0;
+  while (idx < L->n_species && L->cdf[idx] < u)
+    idx++;
+  if (idx >= L->n_species)
+    idx = L->n_species - 1;
+  return L->species[idx];
 }
 
 /* Sensor::check_conditions, src/detector.cpp:374-417 */
@@ -1044,11 +1129,11 @@ static double optical_depth_to_detector(const lmc_o_handle *h, v3 start, v3 dir,
   if (layer >= h->scene.n_layers)
     return 0.0;
   if (h->scene.n_layers == 1)
-    return layer_medium(h, layer)->mu_t * L_total;
+    return layer_at(h, layer)->mu_t * L_total;
   const double dz = dir.z;
   while (traveled < L_total - 1e-15) {
     const double remaining = L_total - traveled;
-    const double mu = layer_medium(h, layer)->mu_t;
+    const double mu = layer_at(h, layer)->mu_t;
     double seg = remaining;
     if (fabs(dz) > 1e-15) {
       double zi;
@@ -1135,7 +1220,10 @@ static void estimate_farfield_cbs(const lmc_o_handle *h, const osensor *s, doubl
   const v3 e3 = v3scale(s_in, -1.0);
   const m3 *Pcur = &ph->P;
   const v3 m_cur = m3row(Pcur, 0), n_cur = m3row(Pcur, 1), s_cur = m3row(Pcur, 2);
-  const double w_scatter = ph->weight * (med->p.mu_s / med->mu_t);
+  /* first vertex: the layer's aggregate albedo (src/detector.cpp:1378); later
+   * vertices: the selected species' own (:1472).  Equal for a HomogeneousLayer. */
+  const olayer *SL = layer_at(h, ph->current_layer);
+  const double w_scatter = ph->weight * (ph->events == 0 ? SL->mu_s / SL->mu_t : med->p.mu_s / med->mu_t);
   if (w_scatter < 1e-300)
     return;
   const double th_cap = (p->theta_pp_max > 0.0) ? fmin(p->theta_pp_max, p->theta_max_grid) : p->theta_max_grid;
@@ -1338,8 +1426,8 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
     memset(t_adj->score, 0, sizeof(t_adj->score));
 
   while (ph->alive) {
-    const omedium *cur = layer_medium(h, ph->current_layer);
-    double step = -1 * cur->p.mfp * log(orng_uniform(rng));      /* medium.cpp:123-126 */
+    const olayer *cur = layer_at(h, ph->current_layer);
+    double step = -1 * cur->mfp * log(orng_uniform(rng));        /* medium.cpp:123-126, sample.cpp:90-94 */
     if (t_adj)
       oadj_flight_start(h, h->scene.layers[ph->current_layer].medium);
     st->steps++;
@@ -1355,7 +1443,7 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
       if (t < 0.0 || t > 1.0)
         break;
       const double step_to_iface = step * t;
-      const double remaining_optical = (step - step_to_iface) * layer_medium(h, ph->current_layer)->mu_t;
+      const double remaining_optical = (step - step_to_iface) * layer_at(h, ph->current_layer)->mu_t;
       ph->opticalpath += step_to_iface;
       ph->optical_path += n_step * step_to_iface;
       ph->prev_pos = ph->pos;
@@ -1381,7 +1469,7 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
         break;
       }
       ph->current_layer = new_layer;
-      const double new_mu_t = layer_medium(h, ph->current_layer)->mu_t;
+      const double new_mu_t = layer_at(h, ph->current_layer)->mu_t;
       if (new_mu_t > 0)
         step = remaining_optical / new_mu_t;
       else
@@ -1418,7 +1506,7 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
     }
     ph->current_layer = layer_index_at(h, ph->pos.z);
     const int scatter_layer = ph->current_layer;
-    const int med_idx = h->scene.layers[scatter_layer].medium;  /* :423-426 */
+    const int med_idx = select_scatter_medium(h, scatter_layer, rng);  /* :419-426 */
     const omedium *sm = &h->media[med_idx];
     ph->active_medium = med_idx;
     for (int si = 0; si < h->scene.n_sensors; ++si) {             /* :419-426 run_estimators */
@@ -1523,9 +1611,10 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
     }
     ph->events++;                                               /* :578-587 */
     st->events++;
-    const double layer_mu_t = sm->mu_t;
+    const olayer *SL = layer_at(h, scatter_layer);             /* the layer's aggregate albedo */
+    const double layer_mu_t = SL->mu_t;
     if (layer_mu_t > 0) {
-      const double scattering_prob = sm->p.mu_s / layer_mu_t;
+      const double scattering_prob = SL->mu_s / layer_mu_t;
       ph->weight *= scattering_prob;
     }
     if (ph->weight < 1e-4) {                                    /* :596-607 */
@@ -1572,6 +1661,18 @@ lmc_o_handle *lmc_oracle_create(const lmc_o_scene *scene, char *err, int err_len
       return NULL;
     }
     h->media[i].I_norm = compute_I_norm(&h->media[i]);
+  }
+  for (int l = 0; l < scene->n_layers; ++l) {
+    const lmc_o_layer *L = &scene->layers[l];
+    if (L->n_species <= 0 && (L->medium < 0 || L->medium >= scene->n_media)) {
+      snprintf(err, (size_t)err_len, "Sample::add_layer: medium pointer must not be null.");
+      lmc_oracle_destroy(h);
+      return NULL;
+    }
+    if (olayer_init(h, L, &h->layer[l], err, err_len) != 0) {
+      lmc_oracle_destroy(h);
+      return NULL;
+    }
   }
   for (int l = 1; l < scene->n_layers; ++l)                     /* sample.cpp:155-158 */
     h->interfaces[h->n_interfaces++] = scene->layers[l].z_min;
@@ -1734,6 +1835,9 @@ int lmc_oracle_run_adjoint(lmc_o_handle *h, uint64_t seed, uint64_t begin, uint6
                            const lmc_o_adjoint *a, double *out, lmc_o_stats *stats)
 {
   oadj A;
+  for (int l = 0; l < h->scene.n_layers; ++l)
+    if (h->layer[l].n_species > 0)
+      return -3;                  /* the likelihood-ratio scores model HomogeneousLayers only */
   if (oadj_layout(h, a, &A) != 0)
     return -3;
   A.out = out;

@@ -31,6 +31,7 @@ extern "C" {
 #define LMC_O_MAX_MEDIA 16
 #define LMC_O_MAX_LAYERS 16
 #define LMC_O_MAX_SENSORS 8
+#define LMC_O_MAX_SPECIES 8
 
 enum lmc_o_phase_kind {
   LMC_O_PHASE_UNIFORM = 0,    /* src/phase.cpp:78-83   */
@@ -76,9 +77,16 @@ typedef struct lmc_o_medium {
   double mu_a, mu_s, mfp;
 } lmc_o_medium;
 
+/* HomogeneousLayer of `medium` (n_species == 0), or a MixtureLayer
+ * (include/luminis/core/sample.hpp:150-205) of n_species co-located media at
+ * number densities n_i [1/mm^3]: mu_s_i = n_i sigma_s_i with sigma_s_i the
+ * species' phase-function scattering cross-section (Mie and RD-EMC only). */
 typedef struct lmc_o_layer {
   int medium;
   double z_min, z_max;
+  int n_species;
+  int species[LMC_O_MAX_SPECIES];
+  double number_density[LMC_O_MAX_SPECIES];
 } lmc_o_layer;
 
 typedef struct lmc_o_laser {

@@ -42,8 +42,13 @@ class Medium(C.Structure):
                 ("mu_a", C.c_double), ("mu_s", C.c_double), ("mfp", C.c_double)]
 
 
+MAX_SPECIES = 8
+
+
 class Layer(C.Structure):
-    _fields_ = [("medium", C.c_int), ("z_min", C.c_double), ("z_max", C.c_double)]
+    _fields_ = [("medium", C.c_int), ("z_min", C.c_double), ("z_max", C.c_double),
+                ("n_species", C.c_int), ("species", C.c_int * MAX_SPECIES),
+                ("number_density", C.c_double * MAX_SPECIES)]
 
 
 class Laser(C.Structure):
@@ -192,9 +197,16 @@ def scene_from_spec(spec: dict) -> Scene:
     layers = spec["layers"]
     sc.n_layers = len(layers)
     for i, l in enumerate(layers):
-        sc.layers[i].medium = int(l["medium"])
         sc.layers[i].z_min = float(l["z_min"])
         sc.layers[i].z_max = float(l["z_max"])
+        if "species" in l:                      # MixtureLayer
+            sc.layers[i].medium = -1
+            sc.layers[i].n_species = len(l["species"])
+            for k, (m, n) in enumerate(zip(l["species"], l["densities"])):
+                sc.layers[i].species[k] = int(m)
+                sc.layers[i].number_density[k] = float(n)
+        else:
+            sc.layers[i].medium = int(l["medium"])
     L = spec["laser"]
     _vec(sc.laser.position, L.get("position", (0.0, 0.0, 1e-9)))
     _vec(sc.laser.direction, L.get("direction", (0.0, 0.0, 1.0)))

@@ -18,6 +18,7 @@ tallies and hit counts:
     python tests/golden/make_golden.py stat   (the replica fixtures only)
     python tests/golden/make_golden.py farfield  (far-field fluence from reference records)
     python tests/golden/make_golden.py estimator (estimator-mode FarFieldCBS, Philox stream)
+    python tests/golden/make_golden.py mixture   (MixtureLayer scenes, both streams)
 
 The fixtures pin the oracle (tests/test_oracle_golden.py) and the GPU path
 (tests/test_gpu_golden.py) without the reference present at test time.
@@ -158,6 +159,35 @@ def estimator_main():
     print("wrote", meta)
 
 
+def mixture_scenes():
+    """MixtureLayer scenes (species drawn per vertex, aggregate free paths and albedo):
+    the three-species slab over the Mie medium (FarFieldCBS 200 x 8, PlanarFluence with
+    time bins), the semi-infinite two-species mixture, and estimator-mode FarFieldCBS
+    in that mixture (first-vertex layer albedo, later-vertex species albedo)."""
+    a = W.mixture_bilayer(1500, 41)
+    a["name"] = "mixture_bilayer_small"
+    a["sensors"][1].update(len_x=4.0, len_y=4.0, dx=0.25, dy=0.25, len_t=15.0, d_t=1.0)
+    b = W.mixture_cbs_small(2000, 42)
+    c = W.mixture_cbs_small(250, 43)
+    c["name"] = "estimator_mixture"
+    c["media"][1].update(mu_a=0.5)
+    c["sensors"] = [dict(c["sensors"][0], estimator=True, d_theta=2e-3, theta_max=0.1)]
+    return [a, b, c]
+
+
+def mixture_main():
+    meta = {}
+    for spec in mixture_scenes():
+        name = spec["name"]
+        np.savez_compressed(os.path.join(HERE, f"ref_philox_{name}.npz"),
+                            **run_flavour("replay", name, fmt=0, source="mixture_scenes"))
+        if not name.startswith("estimator"):
+            np.savez_compressed(os.path.join(HERE, f"ref_xoshiro_{name}.npz"),
+                                **run_flavour("pin", name, source="mixture_scenes"))
+        meta[name] = {"n_photons": spec["n_photons"], "seed": spec["seed"]}
+    print("wrote", meta)
+
+
 FF_GRID = {"theta_max": 1.5707963267948966, "phi_max": 2 * 3.141592653589793, "len_t": 20.0,
            "d_theta": 3.141592653589793 / 36, "d_phi": 2 * 3.141592653589793 / 12, "d_t": 2.0}
 
@@ -259,7 +289,7 @@ def run_flavour(flavour, scene_name, fmt=None, source="golden_scenes"):
     code = f"""
 import sys, json, glob, ctypes, numpy as np
 sys.path.insert(0, {REPO!r}); sys.path.insert(0, {os.path.join(REPO, 'luminis-mc_b200')!r})
-from tests.golden.make_golden import golden_scenes, estimator_scenes
+from tests.golden.make_golden import golden_scenes, estimator_scenes, mixture_scenes
 from luminis_mc_b200 import workloads as W
 from oracle import pyoracle as O
 lm = O.reference_module({flavour!r}); lm.set_log_level(lm.LogLevel.off)
@@ -307,5 +337,7 @@ if __name__ == "__main__":
         farfield_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "estimator":
         estimator_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "mixture":
+        mixture_main()
     else:
         main()
