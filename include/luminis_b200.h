@@ -48,6 +48,8 @@ extern "C" {
 #define LMC_MAX_LAYERS 16
 #define LMC_MAX_MEDIA 16
 #define LMC_MAX_SENSORS 8
+#define LMC_MAX_SPECIES 8         /* co-located species of one MixtureLayer              */
+#define LMC_MAX_MIX_ENTRIES 32    /* species over all MixtureLayers of one scene         */
 #define LMC_MAX_SWEEP_SCENES 4096
 
 typedef enum lmc_status {
@@ -83,12 +85,23 @@ typedef struct lmc_medium_desc {
   const double *amp_s2;         /* S2(theta_i), interleaved re, im                     */
   double mu_a, mu_s;            /* 1/mm; mu_t = mu_a + mu_s (src/medium.cpp:61-71)     */
   double mean_free_path;        /* mm; free paths are -mfp*ln(u) (src/medium.cpp:123)  */
+  double cross_section;         /* mm^2; single-particle scattering cross-section
+                                   Q_sca pi r^2 of the phase function
+                                   (include/luminis/core/medium.hpp:186-188); read for
+                                   MixtureLayer species only; <= 0: none              */
 } lmc_medium_desc;
 
-/* HomogeneousLayer z in [z_min, z_max) (include/luminis/core/sample.hpp:120-147). */
+/* One slab z in [z_min, z_max): a HomogeneousLayer of `medium`
+ * (include/luminis/core/sample.hpp:120-147), or a MixtureLayer (sample.hpp:150-205,
+ * src/sample.cpp:41-104) of n_species co-located media at number densities n_i:
+ * mu_s_i = n_i sigma_s_i, mu_a = sum mu_s_i (mu_a/mu_s)_i, free paths with the mean
+ * 1 / sum mu_s_i, and one uniform per vertex selects the species by mu_s_i. */
 typedef struct lmc_layer_desc {
   double z_min, z_max;          /* z_max may be +inf for the last layer                */
-  int medium;
+  int medium;                   /* HomogeneousLayer: index into media[]                */
+  int n_species;                /* 0: HomogeneousLayer; 1..LMC_MAX_SPECIES: MixtureLayer */
+  int species[LMC_MAX_SPECIES]; /* MixtureLayer: media[] indices of the species        */
+  double number_density[LMC_MAX_SPECIES];  /* MixtureLayer: n_i, 1/mm^3                */
 } lmc_layer_desc;
 
 /* Laser (include/luminis/core/laser.hpp:24-96). */

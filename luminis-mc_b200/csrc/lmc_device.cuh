@@ -15,8 +15,8 @@ struct Medium {
   int theta_kind, theta_n, amp_n, pad;
   double hg_g;
   double amp_inv_dx;
-  double mu_t, mfp, albedo;             // albedo = mu_s / mu_t (1 if mu_t == 0: no split)
-  float hg_g_f, amp_inv_dx_f, mu_t_f, mfp_f, albedo_f, pad_f;
+  double mu_t, mfp;                     // the medium's own (species albedo, scores)
+  float hg_g_f, amp_inv_dx_f, mu_t_f, mfp_f;
   const double *th_val_d, *th_cdf_d;
   const double2 *th_cs;                  // (cdf[i], slope into node i) for the fp32 path
   const int *guide_d;                    // kGuideBuckets + 1 entries
@@ -27,9 +27,17 @@ struct Medium {
   double I_norm;                         // int (|S1|^2 + |S2|^2) sin(theta), the estimator's p(Omega)
 };
 
+// A layer with its transport coefficients (Layer::mu_attenuation, mu_scattering,
+// sample_free_path): its medium's for a HomogeneousLayer, the MixtureLayer aggregates
+// otherwise (src/sample.cpp:41-94).  A mixture's species and selection CDF are the
+// entries [mix_begin, mix_begin + n_species) of Scene::mix_cdf / mix_species.
 struct Layer {
   double z_min, z_max;
-  int medium, pad;
+  int medium;                            // HomogeneousLayer: its medium
+  int n_species;                         // 0: HomogeneousLayer; else MixtureLayer species
+  int mix_begin, pad;
+  double mu_s, mu_t, mfp, albedo;        // albedo = mu_s / mu_t (1 if mu_t == 0: no split)
+  float mu_t_f, mfp_f;
 };
 
 struct Sensor {
@@ -67,6 +75,8 @@ struct __align__(16) Scene {
   float plane_z_f[LMC_MAX_SENSORS];
   float top_f, pad_f;
   Layer layers[LMC_MAX_LAYERS];
+  double mix_cdf[LMC_MAX_MIX_ENTRIES];   // MixtureLayer selection CDFs (last entry 1)
+  int mix_species[LMC_MAX_MIX_ENTRIES];  // MixtureLayer species (media indices)
   Medium media[LMC_MAX_MEDIA];
   Sensor sensors[LMC_MAX_SENSORS];
   Laser laser;

@@ -77,6 +77,12 @@ template <> __device__ __forceinline__ double med_mfp<double>(const Medium &m) {
 template <typename R> __device__ __forceinline__ R med_mut(const Medium &m);
 template <> __device__ __forceinline__ float med_mut<float>(const Medium &m) { return m.mu_t_f; }
 template <> __device__ __forceinline__ double med_mut<double>(const Medium &m) { return m.mu_t; }
+template <typename R> __device__ __forceinline__ R lay_mfp(const Layer &l);
+template <> __device__ __forceinline__ float lay_mfp<float>(const Layer &l) { return l.mfp_f; }
+template <> __device__ __forceinline__ double lay_mfp<double>(const Layer &l) { return l.mfp; }
+template <typename R> __device__ __forceinline__ R lay_mut(const Layer &l);
+template <> __device__ __forceinline__ float lay_mut<float>(const Layer &l) { return l.mu_t_f; }
+template <> __device__ __forceinline__ double lay_mut<double>(const Layer &l) { return l.mu_t; }
 template <typename R> __device__ __forceinline__ R sc_iface(const Scene &s, int i);
 template <> __device__ __forceinline__ float sc_iface<float>(const Scene &s, int i) { return s.interfaces_f[i]; }
 template <> __device__ __forceinline__ double sc_iface<double>(const Scene &s, int i) { return s.interfaces[i]; }
@@ -966,7 +972,7 @@ struct EstVertex {
   Cx<double> Em, En, T[4];      // Jones vector; interior product including the newest event
   double w, opath;
   unsigned long long index;
-  int events, med, first_med, pad;
+  int events, med, first_med, layer;
 };
 
 __device__ __forceinline__ V3<double> drow(const double *P, int r)
@@ -1047,11 +1053,11 @@ __device__ __forceinline__ double est_optical_depth(const Scene &sc, const doubl
   if (layer >= sc.n_layers)
     return 0.0;
   if (sc.n_layers == 1)
-    return sc.media[sc.layers[layer].medium].mu_t * L_total;
+    return sc.layers[layer].mu_t * L_total;
   const double dz = dir.z;
   for (int guard = 0; guard <= 2 * LMC_MAX_LAYERS && traveled < L_total - 1e-15; ++guard) {
     const double remaining = L_total - traveled;
-    const double mu = sc.media[sc.layers[layer].medium].mu_t;
+    const double mu = sc.layers[layer].mu_t;
     double seg = remaining;
     if (fabs(dz) > 1e-15) {
       double zi;
@@ -1093,7 +1099,10 @@ __device__ __noinline__ void estimate_vertex(const Scene &sc, const RunParams &r
       continue;
     if (med.I_norm < 1e-300)
       continue;
-    const double w_scatter = v.w * (med.mu_s / med.mu_t);
+    // the layer's aggregate albedo at the first vertex (src/detector.cpp:1378), the
+    // selected species' own later (:1472); the same for a HomogeneousLayer
+    const Layer &VL = sc.layers[v.layer];
+    const double w_scatter = v.w * (v.events == 0 ? VL.mu_s / VL.mu_t : med.mu_s / med.mu_t);
     if (w_scatter < 1e-300)
       continue;
     const bool multi = v.events >= 1;
@@ -1229,6 +1238,7 @@ __device__ __forceinline__ void estimate_at_vertex(const Scene &sc, const RunPar
   v.index = ph.index();
   v.events = (int)ph.events;
   v.med = med_idx;
+  v.layer = ph.layer;
   v.first_med = side.first_med[tid];
   // interior product for the estimated path (src/detector.cpp:1462-1469): the
   // newest event's raw factor folded into the committed product (from 2 events on)
@@ -1246,7 +1256,6 @@ __device__ __forceinline__ void estimate_at_vertex(const Scene &sc, const RunPar
   } else {
     v.T[0] = T0; v.T[1] = T1; v.T[2] = T2; v.T[3] = T3;
   }
-  v.pad = 0;
   estimate_vertex<R>(sc, rp, v, s_hits);
 }
 
@@ -1476,9 +1485,9 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
 {
   rng_prefetch<R>(ph.rng, rp);
   {
-    // free path (src/medium.cpp:123-126)
-    const Medium &cm = sc.media[sc.layers[ph.layer].medium];
-    R step = -med_mfp<R>(cm) * m_log(uniform<R>(ph.rng, rp));
+    // free path with the layer's mean free path (src/medium.cpp:123-126,
+    // src/sample.cpp:90-94)
+    R step = -lay_mfp<R>(sc.layers[ph.layer]) * m_log(uniform<R>(ph.rng, rp));
     cnt.steps++;
     if (kAdj)
       flight_start<R>(sc, fl, sc.layers[ph.layer].medium);
@@ -1500,8 +1509,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
       }
       if (at_iface && crossing >= sc.n_interfaces)   // each crossing passes a distinct interface
         return kError;
-      const R rem = at_iface ? (step - s_move) * med_mut<R>(sc.media[sc.layers[ph.layer].medium])
-                             : R(0);
+      const R rem = at_iface ? (step - s_move) * lay_mut<R>(sc.layers[ph.layer]) : R(0);
       ph.opath += (double)s_move;
       const R x0 = ph.px, y0 = ph.py, z0 = ph.pz;
       ph.px += dx * s_move;
@@ -1531,7 +1539,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
       if (nl >= sc.n_layers)
         return kStack;
       ph.layer = nl;
-      const R nmt = med_mut<R>(sc.media[sc.layers[nl].medium]);
+      const R nmt = lay_mut<R>(sc.layers[nl]);
       step = (nmt > R(0)) ? rem / nmt : rem;
     }
     // Sample::is_inside (src/sample.cpp:268-288)
@@ -1540,7 +1548,18 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
       return kEscaped;
   }
   ph.layer = layer_index_at<R>(sc, ph.pz);
-  const int med_idx = sc.layers[ph.layer].medium;
+  // Layer::select_scatter_medium (src/simulation.cpp:419-425): a HomogeneousLayer's
+  // medium without a draw, or a MixtureLayer species by one uniform and lower_bound
+  // on its selection CDF (src/sample.cpp:96-104), compared in binary64
+  const Layer &SL = sc.layers[ph.layer];
+  int med_idx = SL.medium;
+  if (SL.n_species > 0) {
+    const double u = (double)uniform<R>(ph.rng, rp);
+    int i = 0;
+    while (i < SL.n_species - 1 && sc.mix_cdf[SL.mix_begin + i] < u)
+      ++i;
+    med_idx = sc.mix_species[SL.mix_begin + i];
+  }
   const Medium &m = sc.media[med_idx];
   if (kAdj)
     flight_scatter<R>(sc, fl, fl.seg_med, fl.seg_len);
@@ -1675,7 +1694,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   }
   ph.events++;                                                // :578-587
   cnt.events++;
-  ph.w *= m.albedo;
+  ph.w *= SL.albedo;                                          // the layer's aggregate albedo
   if (ph.w < 1e-4) {                                          // :596-607
     if (uniform<R>(ph.rng, rp) < R(0.1))
       ph.w /= 0.1;

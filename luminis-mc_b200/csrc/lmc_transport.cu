@@ -113,10 +113,36 @@ lmc_status validate(const lmc_scene *s)
     return fail(LMC_ERR_INVALID, "at most " + std::to_string(LMC_MAX_SENSORS) + " sensors");
   if (!(s->n_host > 0.0) || !finite(s->n_host))
     return fail(LMC_ERR_INVALID, "host refractive index must be positive and finite");
+  int mix_entries = 0;
   for (int l = 0; l < s->n_layers; ++l) {                  // src/sample.cpp:120-140
     const lmc_layer_desc &L = s->layers[l];
-    if (L.medium < 0 || L.medium >= s->n_media)
+    if (L.n_species < 0 || L.n_species > LMC_MAX_SPECIES)
+      return fail(LMC_ERR_INVALID, "a MixtureLayer holds 1.." + std::to_string(LMC_MAX_SPECIES) + " species");
+    if (L.n_species == 0 && (L.medium < 0 || L.medium >= s->n_media))
       return fail(LMC_ERR_INVALID, "layer medium index out of range");
+    if (L.n_species > 0) {                                 // src/sample.cpp:41-82
+      mix_entries += L.n_species;
+      if (mix_entries > LMC_MAX_MIX_ENTRIES)
+        return fail(LMC_ERR_UNSUPPORTED, "at most " + std::to_string(LMC_MAX_MIX_ENTRIES) +
+                                             " species over all MixtureLayers of a scene");
+      double mu_s_total = 0.0;
+      for (int i = 0; i < L.n_species; ++i) {
+        const int m = L.species[i];
+        if (m < 0 || m >= s->n_media)
+          return fail(LMC_ERR_INVALID, "MixtureLayer: species pointer must not be null.");
+        const double sig = s->media[m].cross_section;
+        if (!(sig > 0.0) || !finite(sig))
+          return fail(LMC_ERR_INVALID, "PhaseFunction::scattering_cross_section: Not implemented "
+                                       "for this phase function.");
+        if (!finite(L.number_density[i]))
+          return fail(LMC_ERR_INVALID, "MixtureLayer: number densities must be finite");
+        mu_s_total += L.number_density[i] * sig;
+      }
+      if (!(mu_s_total > 0.0) || !finite(mu_s_total))
+        return fail(LMC_ERR_INVALID, "MixtureLayer: total mu_s must be positive (check number "
+                                     "densities and that the species' phase functions expose a "
+                                     "scattering cross-section).");
+    }
     if (!(L.z_max > L.z_min))
       return fail(LMC_ERR_INVALID, "Sample::add_layer: z_max must be greater than z_min.");
     if (l == 0 && L.z_min != 0.0)
@@ -275,6 +301,61 @@ double medium_I_norm(const lmc_medium_desc &M)
   return acc * dth;
 }
 
+// Layers, interfaces and MixtureLayer tables of the device scene.  A HomogeneousLayer
+// takes its medium's coefficients (include/luminis/core/sample.hpp:142-144); a
+// MixtureLayer the aggregates of its constructor (src/sample.cpp:55-88): mu_s_i =
+// n_i sigma_i, absorption keeping each species' albedo, mu_t, mfp = 1 / mu_s and the
+// normalised CDF over mu_s_i whose last entry is exactly 1.
+void fill_layers(const lmc_scene *s, dev::Scene &sc)
+{
+  int mix = 0;
+  for (int l = 0; l < s->n_layers; ++l) {
+    const lmc_layer_desc &in = s->layers[l];
+    dev::Layer &d = sc.layers[l];
+    d.z_min = in.z_min;
+    d.z_max = in.z_max;
+    if (in.n_species == 0) {
+      const lmc_medium_desc &M = s->media[in.medium];
+      d.medium = in.medium;
+      d.mu_s = M.mu_s;
+      d.mu_t = M.mu_a + M.mu_s;                             // src/medium.cpp:61-71
+      d.mfp = M.mean_free_path;
+    } else {
+      double mu_s_i[LMC_MAX_SPECIES];
+      double mu_s_total = 0.0, mu_a_total = 0.0;
+      for (int i = 0; i < in.n_species; ++i) {
+        const lmc_medium_desc &M = s->media[in.species[i]];
+        mu_s_i[i] = in.number_density[i] * M.cross_section;
+        mu_s_total += mu_s_i[i];
+        if (M.mu_s > 0.0)
+          mu_a_total += mu_s_i[i] * (M.mu_a / M.mu_s);
+      }
+      d.medium = in.species[0];
+      d.n_species = in.n_species;
+      d.mix_begin = mix;
+      d.mu_s = mu_s_total;
+      d.mu_t = mu_s_total + mu_a_total;
+      d.mfp = 1.0 / mu_s_total;
+      double acc = 0.0;
+      for (int i = 0; i < in.n_species; ++i) {
+        acc += mu_s_i[i] / mu_s_total;
+        sc.mix_cdf[mix + i] = acc;
+        sc.mix_species[mix + i] = in.species[i];
+      }
+      sc.mix_cdf[mix + in.n_species - 1] = 1.0;
+      mix += in.n_species;
+    }
+    d.albedo = d.mu_t > 0 ? d.mu_s / d.mu_t : 1.0;          // src/simulation.cpp:578-587
+    d.mu_t_f = (float)d.mu_t;
+    d.mfp_f = (float)d.mfp;
+    if (l > 0) {
+      sc.interfaces[sc.n_interfaces] = in.z_min;
+      sc.interfaces_f[sc.n_interfaces] = (float)in.z_min;
+      sc.n_interfaces++;
+    }
+  }
+}
+
 // tally_base: offset (doubles) of this scene's first sensor in the tally buffer.
 void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned char> &arena, SceneBuild &b)
 {
@@ -287,16 +368,7 @@ void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned cha
   sc.top_is_inf = std::isinf(sc.top) ? 1 : 0;
   sc.top_f = (float)sc.top;
   sc.n_step = 1.0 / (1.0 / s->n_host);                      // src/simulation.cpp:343,390
-  for (int l = 0; l < s->n_layers; ++l) {
-    sc.layers[l].z_min = s->layers[l].z_min;
-    sc.layers[l].z_max = s->layers[l].z_max;
-    sc.layers[l].medium = s->layers[l].medium;
-    if (l > 0) {
-      sc.interfaces[sc.n_interfaces] = s->layers[l].z_min;
-      sc.interfaces_f[sc.n_interfaces] = (float)s->layers[l].z_min;
-      sc.n_interfaces++;
-    }
-  }
+  fill_layers(s, sc);
   const lmc_laser_desc &L = s->laser;
   for (int j = 0; j < 3; ++j) {
     sc.laser.pos[j] = L.position[j];
@@ -379,10 +451,8 @@ void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned cha
     d.hg_g_f = (float)M.hg_g;
     d.mu_t = M.mu_a + M.mu_s;                               // src/medium.cpp:61-71
     d.mfp = M.mean_free_path;
-    d.albedo = d.mu_t > 0 ? M.mu_s / d.mu_t : 1.0;          // src/simulation.cpp:580-587
     d.mu_t_f = (float)d.mu_t;
     d.mfp_f = (float)d.mfp;
-    d.albedo_f = (float)d.albedo;
     d.amp_n = M.amp_n;
     d.amp_inv_dx = 1.0 / M.amp_dtheta;
     d.amp_inv_dx_f = (float)d.amp_inv_dx;
@@ -600,6 +670,9 @@ static lmc_status adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a,
     return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs need every sensor plane at z <= 0");
   if (h->scene.n_media > dev::kAdjMaxMedia)
     return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs support at most 4 media");
+  for (int l = 0; l < h->scene.n_layers; ++l)
+    if (h->scene.layers[l].n_species > 0)
+      return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs model HomogeneousLayers only");
   for (int i = 0; i < h->scene.n_media; ++i) {
     const dev::Medium &m = h->scene.media[i];
     if (!(m.mu_t > 0) || !(m.mu_s > 0))
@@ -1206,16 +1279,7 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
   sc.top_is_inf = std::isinf(sc.top) ? 1 : 0;
   sc.top_f = (float)sc.top;
   sc.n_step = 1.0 / (1.0 / s->n_host);
-  for (int l = 0; l < s->n_layers; ++l) {
-    sc.layers[l].z_min = s->layers[l].z_min;
-    sc.layers[l].z_max = s->layers[l].z_max;
-    sc.layers[l].medium = s->layers[l].medium;
-    if (l > 0) {
-      sc.interfaces[sc.n_interfaces] = s->layers[l].z_min;
-      sc.interfaces_f[sc.n_interfaces] = (float)s->layers[l].z_min;
-      sc.n_interfaces++;
-    }
-  }
+  fill_layers(s, sc);
   const lmc_laser_desc &L = s->laser;
   for (int j = 0; j < 3; ++j) {
     sc.laser.pos[j] = L.position[j];
@@ -1309,10 +1373,8 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     d.hg_g_f = (float)M.hg_g;
     d.mu_t = M.mu_a + M.mu_s;
     d.mfp = M.mean_free_path;
-    d.albedo = d.mu_t > 0 ? M.mu_s / d.mu_t : 1.0;
     d.mu_t_f = (float)d.mu_t;
     d.mfp_f = (float)d.mfp;
-    d.albedo_f = (float)d.albedo;
     d.amp_n = M.amp_n;
     d.amp_inv_dx = 1.0 / M.amp_dtheta;
     d.amp_inv_dx_f = (float)d.amp_inv_dx;

@@ -8,7 +8,7 @@ the reference does.
 """
 from .core import (Absorption, CMatrix, CrossingDirection, CVec2, DrainePhaseFunction,  # noqa: F401
                    FarFieldCBSSensor, FarFieldFluenceSensor, HenyeyGreensteinPhaseFunction, Laser,
-                   LaserSource, Layer, LogLevel, Matrix, MiePhaseFunction, MieMedium,
+                   LaserSource, Layer, LogLevel, Matrix, MiePhaseFunction, MieMedium, MixtureLayer,
                    PhaseFunction, PhotonRecordSensor, PlanarFieldSensor, PlanarFluenceSensor,
                    RayleighDebyeEMCPhaseFunction, RayleighDebyePhaseFunction,
                    RayleighPhaseFunction, RGDMedium, Rng, Sample, SampleLayer, ScatteringMedium,

@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libluminis_b200.so")
 
 MAX_LAYERS, MAX_MEDIA, MAX_SENSORS = 16, 16, 8
+MAX_SPECIES, MAX_MIX_ENTRIES = 8, 32
 
 LMC_OK, LMC_ERR_INVALID, LMC_ERR_CUDA, LMC_ERR_NOMEM, LMC_ERR_KERNEL, LMC_ERR_UNSUPPORTED = range(6)
 THETA_TABLE, THETA_TABLE_COS, THETA_HG, THETA_UNIFORM = range(4)
@@ -27,11 +28,14 @@ class MediumDesc(C.Structure):
     _fields_ = [("theta_kind", C.c_int), ("hg_g", C.c_double), ("theta_n", C.c_int),
                 ("theta_values", dptr), ("theta_cdf", dptr), ("amp_n", C.c_int),
                 ("amp_dtheta", C.c_double), ("amp_s1", dptr), ("amp_s2", dptr),
-                ("mu_a", C.c_double), ("mu_s", C.c_double), ("mean_free_path", C.c_double)]
+                ("mu_a", C.c_double), ("mu_s", C.c_double), ("mean_free_path", C.c_double),
+                ("cross_section", C.c_double)]
 
 
 class LayerDesc(C.Structure):
-    _fields_ = [("z_min", C.c_double), ("z_max", C.c_double), ("medium", C.c_int)]
+    _fields_ = [("z_min", C.c_double), ("z_max", C.c_double), ("medium", C.c_int),
+                ("n_species", C.c_int), ("species", C.c_int * MAX_SPECIES),
+                ("number_density", C.c_double * MAX_SPECIES)]
 
 
 class LaserDesc(C.Structure):

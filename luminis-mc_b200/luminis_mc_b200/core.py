@@ -571,6 +571,59 @@ class SampleLayer(Layer):
         return self.medium.mu_a
 
 
+class MixtureLayer(Layer):
+    """Several co-located species in one slab (include/luminis/core/sample.hpp:150-205,
+    src/sample.cpp:41-104).  mu_s_i = n_i sigma_s_i from each species' phase-function
+    scattering cross-section; the absorption keeps each species' albedo; free paths
+    use mfp_total = 1 / mu_s_total; every vertex draws one uniform that selects a
+    species on the normalised CDF of mu_s_i (last entry exactly 1)."""
+
+    def __init__(self, species, number_densities, z_min, z_max):
+        super().__init__(z_min, z_max)
+        species = list(species)
+        number_densities = [float(n) for n in number_densities]
+        if not species:
+            raise ValueError("MixtureLayer: species list must not be empty.")
+        if len(species) != len(number_densities):
+            raise ValueError("MixtureLayer: species and number_densities sizes differ.")
+        self.species = species
+        self.number_densities = number_densities
+        self.mu_s_i = []
+        mu_s_total = 0.0
+        mu_a_total = 0.0
+        for sp, n in zip(species, number_densities):
+            if sp is None:
+                raise ValueError("MixtureLayer: species pointer must not be null.")
+            mu_s = n * sp.scattering_cross_section()
+            self.mu_s_i.append(mu_s)
+            mu_s_total += mu_s
+            if sp.mu_s > 0.0:
+                mu_a_total += mu_s * (sp.mu_a / sp.mu_s)
+        if not mu_s_total > 0.0:
+            raise ValueError("MixtureLayer: total mu_s must be positive (check number densities "
+                             "and that the species' phase functions expose a scattering "
+                             "cross-section).")
+        self.mu_s_total = mu_s_total
+        self.mu_a_total = mu_a_total
+        self.mu_t_total = mu_s_total + mu_a_total
+        self.mfp_total = 1.0 / mu_s_total
+        self.selection_cdf = []
+        acc = 0.0
+        for mu_s in self.mu_s_i:
+            acc += mu_s / mu_s_total
+            self.selection_cdf.append(acc)
+        self.selection_cdf[-1] = 1.0
+
+    def mu_attenuation(self):
+        return self.mu_t_total
+
+    def mu_scattering(self):
+        return self.mu_s_total
+
+    def mu_absorption(self):
+        return self.mu_a_total
+
+
 class Sample:
     """Contiguous z-slabs from z = 0 sharing one host refractive index
     (include/luminis/core/sample.hpp:210-364, src/sample.cpp)."""
@@ -605,7 +658,11 @@ class Sample:
             self.interfaces.append(z_min)
 
     def add_mixture_layer(self, species, number_densities, z_min, z_max):
-        raise NotImplementedError("MixtureLayer is not supported by the GPU transport")
+        z_min, z_max = float(z_min), float(z_max)
+        self._validate(z_min, z_max)
+        self.layers.append(MixtureLayer(species, number_densities, z_min, z_max))
+        if len(self.layers) > 1:
+            self.interfaces.append(z_min)
 
     def size(self):
         return len(self.layers)

@@ -17,8 +17,8 @@ import numpy as np
 
 from . import _native as N
 from .core import (FarFieldCBSSensor, FarFieldFluenceSensor, HenyeyGreensteinPhaseFunction,
-                   Matrix, PlanarFieldSensor, PlanarFluenceSensor, UniformPhaseFunction,
-                   _TablePhase, solid_angle_bin)  # noqa: F401
+                   Matrix, MixtureLayer, PlanarFieldSensor, PlanarFluenceSensor,
+                   UniformPhaseFunction, _TablePhase, solid_angle_bin)  # noqa: F401
 
 
 class SimConfig:
@@ -87,6 +87,10 @@ def _medium_desc(d: N.MediumDesc, medium, keep: list) -> None:
     d.mu_a = medium.mu_a
     d.mu_s = medium.mu_s
     d.mean_free_path = medium.mean_free_path
+    try:
+        d.cross_section = float(ph.scattering_cross_section())
+    except NotImplementedError:
+        d.cross_section = 0.0
 
 
 def _sensor_desc(d: N.SensorDesc, s) -> None:
@@ -136,8 +140,7 @@ def scene_desc(config: SimConfig):
     media: list = []
     if len(sample.layers) > N.MAX_LAYERS:
         raise ValueError(f"at most {N.MAX_LAYERS} layers")
-    for i, layer in enumerate(sample.layers):
-        m = layer.medium
+    def medium_index(m):
         idx = next((k for k, x in enumerate(media) if x is m), None)
         if idx is None:
             if len(media) == N.MAX_MEDIA:
@@ -145,9 +148,21 @@ def scene_desc(config: SimConfig):
             idx = len(media)
             media.append(m)
             _medium_desc(sc.media[idx], m, keep)
+        return idx
+
+    for i, layer in enumerate(sample.layers):
         sc.layers[i].z_min = layer.z_min
         sc.layers[i].z_max = layer.z_max
-        sc.layers[i].medium = idx
+        if isinstance(layer, MixtureLayer):
+            if len(layer.species) > N.MAX_SPECIES:
+                raise NotImplementedError(f"a MixtureLayer of at most {N.MAX_SPECIES} species")
+            sc.layers[i].medium = -1
+            sc.layers[i].n_species = len(layer.species)
+            for k, (sp, n) in enumerate(zip(layer.species, layer.number_densities)):
+                sc.layers[i].species[k] = medium_index(sp)
+                sc.layers[i].number_density[k] = n
+        else:
+            sc.layers[i].medium = medium_index(layer.medium)
     sc.n_layers = len(sample.layers)
     sc.n_media = len(media)
     L = sc.laser

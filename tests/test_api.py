@@ -47,7 +47,7 @@ def test_sample_validation_messages():
     assert s.is_inside(lm.Vec3(0, 0, 5.0)) and not s.is_inside(lm.Vec3(0, 0, -1e-9))
 
 
-@pytest.mark.parametrize("extra", ["photon_record", "statistics", "absorption", "mixture"])
+@pytest.mark.parametrize("extra", ["photon_record", "statistics", "absorption"])
 def test_unsupported_parts_raise_before_any_launch(extra):
     cfg, _, keep = W.build(lm, W.mie_cbs_small(10, 1))
     if extra == "photon_record":
@@ -56,12 +56,54 @@ def test_unsupported_parts_raise_before_any_launch(extra):
         cfg.detector.add_detector(lm.StatisticsSensor(0.0))
     elif extra == "absorption":
         cfg.absorption = lm.Absorption(1.0, 1.0, 0.1, 0.1)
-    else:
-        with pytest.raises(NotImplementedError):
-            cfg.sample.add_mixture_layer([], [], 0.0, 1.0)
-        return
     with pytest.raises(NotImplementedError):
         scene_desc(cfg)
+
+
+def test_mixture_layer_aggregates_and_packing():
+    """MixtureLayer (src/sample.cpp:41-88): mu_s_i = n_i sigma_i, albedo-preserving
+    absorption, mfp_total, the selection CDF; packed as species + densities with each
+    species' cross-section in its medium description."""
+    spec = W.mixture_bilayer(10, 1)
+    cfg, _, keep = W.build(lm, spec)
+    layer = cfg.sample.get_layer(0)
+    assert isinstance(layer, lm.MixtureLayer)
+    sig = [sp.scattering_cross_section() for sp in layer.species]
+    mu_s_i = [n * s for n, s in zip(layer.number_densities, sig)]
+    assert layer.mu_s_i == mu_s_i
+    assert layer.mu_s_total == sum(mu_s_i)
+    mu_a = sum(m * (sp.mu_a / sp.mu_s) for m, sp in zip(mu_s_i, layer.species))
+    assert layer.mu_a_total == pytest.approx(mu_a, rel=1e-15)
+    assert layer.mu_t_total == layer.mu_s_total + layer.mu_a_total
+    assert layer.mfp_total == 1.0 / layer.mu_s_total
+    assert layer.selection_cdf[-1] == 1.0
+    assert all(a < b for a, b in zip(layer.selection_cdf, layer.selection_cdf[1:]))
+    assert layer.mu_attenuation() == layer.mu_t_total
+    sc, _, _ = scene_desc(cfg)
+    L0 = sc.layers[0]
+    assert L0.n_species == 3 and L0.medium == -1
+    for k in range(3):
+        m = sc.media[L0.species[k]]
+        assert m.cross_section == sig[k]
+        assert L0.number_density[k] == layer.number_densities[k]
+    assert sc.layers[1].n_species == 0 and sc.media[sc.layers[1].medium].cross_section > 0
+
+
+def test_mixture_layer_validation_messages():
+    hg = lm.MieMedium(lm.HenyeyGreensteinPhaseFunction(0.9), 0.5e-3, 1.59, 1.33, 0.633e-3)
+    s = lm.Sample(1.33)
+    with pytest.raises(ValueError, match="must not be empty"):
+        s.add_mixture_layer([], [], 0.0, 1.0)
+    with pytest.raises(ValueError, match="sizes differ"):
+        s.add_mixture_layer([hg], [1.0, 2.0], 0.0, 1.0)
+    with pytest.raises(NotImplementedError, match="scattering_cross_section"):
+        s.add_mixture_layer([hg], [1.0], 0.0, 1.0)
+    spec = W.mixture_cbs_small(10, 1)
+    cfg, _, keep = W.build(lm, spec)
+    with pytest.raises(ValueError, match="total mu_s must be positive"):
+        lm.Sample(1.33).add_mixture_layer(cfg.sample.get_layer(0).species, [0.0, 0.0], 0.0, 1.0)
+    with pytest.raises(ValueError, match="first layer must start at z = 0"):
+        lm.Sample(1.33).add_mixture_layer(cfg.sample.get_layer(0).species, [1.0, 1.0], 0.5, 1.0)
 
 
 @pytest.mark.parametrize("mutate,match", [

@@ -54,8 +54,8 @@ def _same(got, want, gst, wst):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("make", [W.mie_cbs_small, W.bilayer_rgd_mie],
-                         ids=["mie_cbs_small", "bilayer_rgd_mie"])
+@pytest.mark.parametrize("make", [W.mie_cbs_small, W.bilayer_rgd_mie, W.mixture_bilayer],
+                         ids=["mie_cbs_small", "bilayer_rgd_mie", "mixture_bilayer"])
 def test_noalloc_matches_lmc_run_twice(make, precision, cuda):
     spec = make(3000, 2024)
     cfg, _, keep = W.build(lm, spec)
