@@ -141,6 +141,23 @@ typedef struct lmc_sensor_desc {
                                    grid, <= 0 none (FarFieldCBSSensor::theta_pp_max)   */
 } lmc_sensor_desc;
 
+/* Absorption recorder (include/luminis/core/absortion.hpp:34-80,
+ * src/absortion.cpp:13-91): every scattering event deposits w mu_a/mu_t of the
+ * layer (1 where the layer has mu_t = 0) at the photon's position, binned on a
+ * cylindrical grid of n_r = floor(radius/d_r)+1 by n_z = floor(depth/d_z)+1 cells
+ * (r = sqrt(x^2+y^2) <= radius, 0 <= z <= depth).  d_t > 0 adds time slices:
+ * n_t = ceil(t_max/d_t)+1, slice 0 time-integrated and slice floor(t/d_t)+1 the
+ * window of arrival time t = launch time + path length. */
+typedef struct lmc_absorption_desc {
+  int enabled;
+  double radius, depth, d_r, d_z;
+  double d_t, t_max;            /* d_t = 0: time-integrated only                     */
+} lmc_absorption_desc;
+
+/* Tally-layout slot of the Absorption grid: [n_t][n_r][n_z], dims {n_t, n_r, n_z, 1},
+ * stored after the sensors. */
+#define LMC_TALLY_ABSORPTION (-2)
+
 /* The scene: Sample + Laser + SensorsGroup of a SimConfig
  * (include/luminis/core/simulation.hpp:67-90). */
 typedef struct lmc_scene {
@@ -152,6 +169,7 @@ typedef struct lmc_scene {
   lmc_laser_desc laser;
   int n_sensors;
   lmc_sensor_desc sensors[LMC_MAX_SENSORS];
+  lmc_absorption_desc absorption;   /* SimConfig::absorption (NULL: enabled = 0)     */
 } lmc_scene;
 
 typedef enum lmc_precision {
@@ -209,7 +227,8 @@ LMC_API lmc_status lmc_create(const lmc_scene *scene, lmc_handle **out);
 LMC_API void lmc_destroy(lmc_handle *h);
 
 /* Tally layout of sensor `sensor` inside the handle's tally buffer (doubles).
- * sensor = -1 returns the total size in *count.  dims as in the oracle:
+ * sensor = -1 returns the total size in *count; LMC_TALLY_ABSORPTION the Absorption
+ * grid (count 0 without one).  dims as in the oracle:
  *  FARFIELD_CBS [8][N_t][N_theta][N_phi], PLANAR_FLUENCE [4][N_t][N_x][N_y],
  *  PLANAR_FIELD [2][N_x][N_y][2], FARFIELD_FLUENCE [4][N_t][N_theta][N_phi]. */
 LMC_API lmc_status lmc_tally_layout(const lmc_handle *h, int sensor, size_t *offset, size_t *count,
@@ -265,7 +284,8 @@ LMC_API lmc_status lmc_run_noalloc(const lmc_scene *scene, uint64_t seed, uint64
 LMC_API lmc_status lmc_create_sweep(const lmc_scene *scenes, int n_scenes, lmc_handle **out);
 
 /* Sensor `sensor` of scene `scene` in the sweep's tally buffer (scene = -1: total size in
- * *count); dims as lmc_tally_layout. */
+ * *count; sensor = LMC_TALLY_ABSORPTION: the scene's Absorption grid); dims as
+ * lmc_tally_layout. */
 LMC_API lmc_status lmc_sweep_layout(const lmc_handle *h, int scene, int sensor, size_t *offset,
                                     size_t *count, int dims[4]);
 

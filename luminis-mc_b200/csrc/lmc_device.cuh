@@ -37,7 +37,16 @@ struct Layer {
   int n_species;                         // 0: HomogeneousLayer; else MixtureLayer species
   int mix_begin, pad;
   double mu_s, mu_t, mfp, albedo;        // albedo = mu_s / mu_t (1 if mu_t == 0: no split)
+  double absorb_prob;                    // mu_a / mu_t: the weight an event deposits
   float mu_t_f, mfp_f;
+};
+
+// Absorption recorder grid (src/absortion.cpp:13-32): [n_t][n_r][n_z] doubles at
+// `off` in the tally buffer.
+struct AbsorbGrid {
+  int on, n_t, n_r, n_z;
+  double radius, depth, d_r, d_z, d_t;
+  unsigned long long off;
 };
 
 struct Sensor {
@@ -80,6 +89,7 @@ struct __align__(16) Scene {
   Medium media[LMC_MAX_MEDIA];
   Sensor sensors[LMC_MAX_SENSORS];
   Laser laser;
+  AbsorbGrid absorb;
 };
 
 // Device scratch of one run: photon work counter, statistics, error word.

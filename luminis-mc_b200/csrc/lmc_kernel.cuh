@@ -1476,6 +1476,31 @@ enum Fate { kAlive = 0, kDetected = 1, kEscaped = 2, kStack = 3, kRoulette = 4, 
 // the run reports kErrAborted instead of spinning.
 constexpr int kMaxRejectionTrials = 1 << 16;
 
+// Absorption::record_absorption (src/absortion.cpp:54-91): an event's deposit at the
+// photon's position (x, y, z), into slice 0 and, time-resolved, into the slice of its
+// arrival time t.  Out of line and with scalar arguments, so that the photon state
+// stays in registers: only scenes with an Absorption recorder reach it.
+__device__ __noinline__ void record_absorption(const AbsorbGrid &g, double *tallies, double x, double y,
+                                               double z, double t, double d_weight)
+{
+  const double r = sqrt(x * x + y * y);
+  if (!(r <= g.radius) || !(z >= 0.0) || !(z <= g.depth))
+    return;
+  const double fr = floor(r / g.d_r), fz = floor(z / g.d_z);
+  if (!(fr < (double)g.n_r) || !(fz < (double)g.n_z))
+    return;
+  const unsigned long long cell = (unsigned long long)fr * (unsigned long long)g.n_z +
+                                  (unsigned long long)fz;
+  double *grid = tallies + g.off;
+  atomicAdd(grid + cell, d_weight);
+  if (g.d_t > 0.0) {
+    const double fk = floor(t / g.d_t) + 1.0;
+    if (fk >= 1.0 && fk < (double)g.n_t)
+      atomicAdd(grid + (unsigned long long)fk * (unsigned long long)g.n_r * (unsigned long long)g.n_z + cell,
+                d_weight);
+  }
+}
+
 // One loop iteration of run_photon (src/simulation.cpp:297-614).  Returns the
 // photon's fate (kAlive if it continues).
 template <typename R, bool kQueue, bool kAdj, bool kEst = false>
@@ -1694,6 +1719,11 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   }
   ph.events++;                                                // :578-587
   cnt.events++;
+  if (sc.absorb.on) {                                         // :589-592
+    const double t = sc.absorb.d_t > 0.0 ? launch_time<R>(sc, rp, ph) + ph.opath : 0.0;  // velocity 1
+    record_absorption(sc.absorb, rp.tallies, (double)ph.px, (double)ph.py, (double)ph.pz, t,
+                      SL.mu_t > 0 ? ph.w * SL.absorb_prob : 1.0);
+  }
   ph.w *= SL.albedo;                                          // the layer's aggregate albedo
   if (ph.w < 1e-4) {                                          // :596-607
     if (uniform<R>(ph.rng, rp) < R(0.1))

@@ -52,6 +52,8 @@ struct lmc_handle {
   size_t sensor_off[LMC_MAX_SENSORS] = {};
   size_t sensor_count[LMC_MAX_SENSORS] = {};
   int sensor_dims[LMC_MAX_SENSORS][4] = {};
+  size_t abs_off = 0, abs_count = 0;     // Absorption grid (LMC_TALLY_ABSORPTION)
+  int abs_dims[4] = {};
   int n_sensors = 0;
   int device = 0;
   int sm_count = 0;
@@ -74,6 +76,8 @@ struct lmc_handle {
     int n_sensors = 0;
     size_t off[LMC_MAX_SENSORS] = {}, count[LMC_MAX_SENSORS] = {};
     int dims[LMC_MAX_SENSORS][4] = {};
+    size_t abs_off = 0, abs_count = 0;
+    int abs_dims[4] = {};
   };
   std::vector<lmc::dev::Scene> scenes;   // host copies (device table pointers inside)
   std::vector<SceneLayout> layouts;
@@ -175,6 +179,19 @@ lmc_status validate(const lmc_scene *s)
     if (M.amp_n < 2 || !M.amp_s1 || !M.amp_s2 || !(M.amp_dtheta > 0.0))
       return fail(LMC_ERR_INVALID, "medium amplitude table missing");
   }
+  if (s->absorption.enabled) {                               // src/absortion.cpp:13-32
+    const lmc_absorption_desc &A = s->absorption;
+    if (!(A.d_r > 0.0) || !(A.d_z > 0.0) || !finite(A.d_r) || !finite(A.d_z))
+      return fail(LMC_ERR_INVALID, "Absorption: d_r and d_z must be positive");
+    if (!(A.radius >= 0.0) || !(A.depth >= 0.0) || !finite(A.radius) || !finite(A.depth))
+      return fail(LMC_ERR_INVALID, "Absorption: radius and depth must be finite and non-negative");
+    if (!(A.d_t >= 0.0) || !finite(A.d_t) || (A.d_t > 0.0 && (!(A.t_max >= 0.0) || !finite(A.t_max))))
+      return fail(LMC_ERR_INVALID, "Absorption: d_t and t_max must be finite and non-negative");
+    const double cells = (std::floor(A.radius / A.d_r) + 1.0) * (std::floor(A.depth / A.d_z) + 1.0) *
+                         (A.d_t > 0.0 ? std::ceil(A.t_max / A.d_t) + 1.0 : 1.0);
+    if (!(cells <= 1.0e9))
+      return fail(LMC_ERR_INVALID, "Absorption: the grid exceeds 1e9 cells");
+  }
   const lmc_laser_desc &L = s->laser;
   if (!(L.wavelength > 0.0))
     return fail(LMC_ERR_INVALID, "laser wavelength must be positive");
@@ -264,6 +281,8 @@ struct SceneBuild {
   size_t sensor_off[LMC_MAX_SENSORS] = {};
   size_t sensor_count[LMC_MAX_SENSORS] = {};
   int sensor_dims[LMC_MAX_SENSORS][4] = {};
+  size_t abs_off = 0, abs_count = 0;
+  int abs_dims[4] = {};
   unsigned cbs_mask = 0;
   bool queued = false;
   bool has_est = false;                  // an estimator-mode FarFieldCBS sensor
@@ -314,9 +333,11 @@ void fill_layers(const lmc_scene *s, dev::Scene &sc)
     dev::Layer &d = sc.layers[l];
     d.z_min = in.z_min;
     d.z_max = in.z_max;
+    double mu_a = 0.0;
     if (in.n_species == 0) {
       const lmc_medium_desc &M = s->media[in.medium];
       d.medium = in.medium;
+      mu_a = M.mu_a;
       d.mu_s = M.mu_s;
       d.mu_t = M.mu_a + M.mu_s;                             // src/medium.cpp:61-71
       d.mfp = M.mean_free_path;
@@ -333,6 +354,7 @@ void fill_layers(const lmc_scene *s, dev::Scene &sc)
       d.medium = in.species[0];
       d.n_species = in.n_species;
       d.mix_begin = mix;
+      mu_a = mu_a_total;
       d.mu_s = mu_s_total;
       d.mu_t = mu_s_total + mu_a_total;
       d.mfp = 1.0 / mu_s_total;
@@ -346,6 +368,7 @@ void fill_layers(const lmc_scene *s, dev::Scene &sc)
       mix += in.n_species;
     }
     d.albedo = d.mu_t > 0 ? d.mu_s / d.mu_t : 1.0;          // src/simulation.cpp:578-587
+    d.absorb_prob = d.mu_t > 0 ? mu_a / d.mu_t : 0.0;
     d.mu_t_f = (float)d.mu_t;
     d.mfp_f = (float)d.mfp;
     if (l > 0) {
@@ -354,6 +377,33 @@ void fill_layers(const lmc_scene *s, dev::Scene &sc)
       sc.n_interfaces++;
     }
   }
+}
+
+// The Absorption grid's shape and its place after the sensors (`off` doubles into the
+// scene's tallies, which start at tally_base); advances off.
+void fill_absorption(const lmc_scene *s, dev::Scene &sc, size_t tally_base, size_t &off,
+                     size_t &count, int dims[4])
+{
+  count = 0;
+  dims[0] = dims[1] = dims[2] = dims[3] = 0;
+  std::memset(&sc.absorb, 0, sizeof(sc.absorb));
+  const lmc_absorption_desc &A = s->absorption;
+  if (!A.enabled)
+    return;
+  dev::AbsorbGrid &g = sc.absorb;
+  g.on = 1;
+  g.n_t = (A.d_t > 0.0) ? (int)std::ceil(A.t_max / A.d_t) + 1 : 1;   // src/absortion.cpp:16-25
+  g.n_r = (int)(A.radius / A.d_r) + 1;
+  g.n_z = (int)(A.depth / A.d_z) + 1;
+  g.radius = A.radius;
+  g.depth = A.depth;
+  g.d_r = A.d_r;
+  g.d_z = A.d_z;
+  g.d_t = A.d_t;
+  g.off = tally_base + off;
+  count = (size_t)g.n_t * (size_t)g.n_r * (size_t)g.n_z;
+  dims[0] = g.n_t; dims[1] = g.n_r; dims[2] = g.n_z; dims[3] = 1;
+  off += count;
 }
 
 // tally_base: offset (doubles) of this scene's first sensor in the tally buffer.
@@ -425,6 +475,8 @@ void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned cha
   for (int i = 0; i < s->n_sensors; ++i)
     sc.sensors[i].plane = rank[sc.sensors[i].plane];
   sc.n_planes = (int)planes.size();
+  b.abs_off = off;
+  fill_absorption(s, sc, tally_base, off, b.abs_count, b.abs_dims);
   b.tally_doubles = off;
   // A photon below z = 0 has left the sample, so a plane at z <= 0 is crossed at
   // most once per photon: hits fit a queue of (photons x planes) entries and are
@@ -599,6 +651,10 @@ lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
   h->cbs_mask = b.cbs_mask;
   h->max_planes = b.sc.n_planes;
   h->has_est = b.has_est;
+  h->abs_off = b.abs_off;
+  h->abs_count = b.abs_count;
+  for (int k = 0; k < 4; ++k)
+    h->abs_dims[k] = b.abs_dims[k];
   for (int i = 0; i < LMC_MAX_SENSORS; ++i) {
     h->sensor_off[i] = b.sensor_off[i];
     h->sensor_count[i] = b.sensor_count[i];
@@ -647,6 +703,14 @@ lmc_status lmc_tally_layout(const lmc_handle *h, int sensor, size_t *offset, siz
   if (sensor == -1) {
     if (offset) *offset = 0;
     if (count) *count = h->tally_doubles;
+    return LMC_OK;
+  }
+  if (sensor == LMC_TALLY_ABSORPTION) {
+    if (offset) *offset = h->abs_off;
+    if (count) *count = h->abs_count;
+    if (dims)
+      for (int k = 0; k < 4; ++k)
+        dims[k] = h->abs_dims[k];
     return LMC_OK;
   }
   if (sensor < 0 || sensor >= h->n_sensors)
@@ -987,6 +1051,10 @@ lmc_status lmc_create_sweep(const lmc_scene *scenes, int n_scenes, lmc_handle **
       for (int j = 0; j < 4; ++j)
         L.dims[i][j] = builds[k].sensor_dims[i][j];
     }
+    L.abs_off = tally + builds[k].abs_off;
+    L.abs_count = builds[k].abs_count;
+    for (int j = 0; j < 4; ++j)
+      L.abs_dims[j] = builds[k].abs_dims[j];
     h->max_planes = std::max(h->max_planes, builds[k].sc.n_planes);
     tally += builds[k].tally_doubles;
   }
@@ -1037,6 +1105,14 @@ lmc_status lmc_sweep_layout(const lmc_handle *h, int scene, int sensor, size_t *
   if (scene < 0 || scene >= h->n_scenes)
     return fail(LMC_ERR_INVALID, "scene out of range");
   const lmc_handle::SceneLayout &L = h->layouts[scene];
+  if (sensor == LMC_TALLY_ABSORPTION) {
+    if (offset) *offset = L.abs_off;
+    if (count) *count = L.abs_count;
+    if (dims)
+      for (int k = 0; k < 4; ++k)
+        dims[k] = L.abs_dims[k];
+    return LMC_OK;
+  }
   if (sensor < 0 || sensor >= L.n_sensors)
     return fail(LMC_ERR_INVALID, "sensor out of range");
   if (offset)
@@ -1335,6 +1411,11 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
   for (int i = 0; i < s->n_sensors; ++i)
     sc.sensors[i].plane = rank[sc.sensors[i].plane];
   sc.n_planes = n_planes;
+  {
+    size_t abs_count = 0;
+    int abs_dims[4];
+    fill_absorption(s, sc, 0, tally_doubles, abs_count, abs_dims);
+  }
   const bool queued = n_planes == 0 || sc.plane_z[n_planes - 1] <= 0.0;
   sc.cbs_mask = cbs_mask;
   if (tally_doubles && !d_tallies)

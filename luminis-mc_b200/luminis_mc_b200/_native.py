@@ -60,10 +60,20 @@ class SensorDesc(C.Structure):
                 ("dtheta", C.c_double), ("dphi", C.c_double), ("theta_pp_max", C.c_double)]
 
 
+class AbsorptionDesc(C.Structure):
+    _fields_ = [("enabled", C.c_int), ("radius", C.c_double), ("depth", C.c_double),
+                ("d_r", C.c_double), ("d_z", C.c_double), ("d_t", C.c_double),
+                ("t_max", C.c_double)]
+
+
+TALLY_ABSORPTION = -2
+
+
 class SceneDesc(C.Structure):
     _fields_ = [("n_host", C.c_double), ("n_media", C.c_int), ("media", MediumDesc * MAX_MEDIA),
                 ("n_layers", C.c_int), ("layers", LayerDesc * MAX_LAYERS), ("laser", LaserDesc),
-                ("n_sensors", C.c_int), ("sensors", SensorDesc * MAX_SENSORS)]
+                ("n_sensors", C.c_int), ("sensors", SensorDesc * MAX_SENSORS),
+                ("absorption", AbsorptionDesc)]
 
 
 class RunOpts(C.Structure):

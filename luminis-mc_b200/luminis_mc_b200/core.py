@@ -946,10 +946,71 @@ class SensorsGroup:
 
 
 class Absorption:
-    """Cylindrical absorption recorder (include/luminis/core/absortion.hpp).  Not
-    supported by the GPU transport: runs with an Absorption raise."""
+    """Cylindrical absorption recorder (include/luminis/core/absortion.hpp:34-80,
+    src/absortion.cpp).  Every scattering event deposits w mu_a / mu_t of its layer at
+    the photon's position on an (r, z) grid of n_r = floor(radius/d_r)+1 by
+    n_z = floor(depth/d_z)+1 cells; with d_t > 0 there are n_t = ceil(t_max/d_t)+1
+    slices, slice 0 time-integrated and slice floor(t/d_t)+1 the arrival window.  The
+    GPU transport deposits into a device grid that run_simulation_parallel adds to
+    time_slices."""
 
     def __init__(self, radius, depth, d_r, d_z, d_t=0.0, t_max=0.0):
         self.radius, self.depth, self.d_r, self.d_z = map(float, (radius, depth, d_r, d_z))
         self.d_t, self.t_max = float(d_t), float(t_max)
-        self.n_t = 1 if self.d_t == 0 else int(math.ceil(self.t_max / self.d_t)) + 1
+        self.n_t = int(math.ceil(self.t_max / self.d_t)) + 1 if self.d_t > 0.0 else 1
+        n_r = int(self.radius / self.d_r) + 1
+        n_z = int(self.depth / self.d_z) + 1
+        self.time_slices = [Matrix(n_r, n_z) for _ in range(self.n_t)]
+
+    def clone(self) -> "Absorption":
+        return Absorption(self.radius, self.depth, self.d_r, self.d_z, self.d_t, self.t_max)
+
+    def merge_from(self, other: "Absorption") -> None:
+        for k in range(self.n_t):
+            self.time_slices[k] += other.time_slices[k]
+
+    def _grid(self) -> np.ndarray:
+        return np.stack([np.asarray(m) for m in self.time_slices])
+
+    def _add(self, grid: np.ndarray) -> None:
+        for k in range(self.n_t):
+            self.time_slices[k] += grid[k]
+
+    def record_absorption(self, photon, d_weight: float) -> None:
+        """Host-side deposit of one event (src/absortion.cpp:54-91); `photon` needs pos,
+        launch_time, opticalpath and velocity."""
+        pos = photon.pos
+        r = math.sqrt(pos.x * pos.x + pos.y * pos.y)
+        z = pos.z
+        if r > self.radius or z < 0.0 or z > self.depth:
+            return
+        i_r, i_z = int(math.floor(r / self.d_r)), int(math.floor(z / self.d_z))
+        n_r, n_z = self.time_slices[0].shape
+        if i_r >= n_r or i_z >= n_z:
+            return
+        self.time_slices[0][i_r, i_z] += d_weight
+        if self.d_t > 0.0:
+            t = photon.launch_time + photon.opticalpath / photon.velocity
+            k = int(math.floor(t / self.d_t)) + 1
+            if 1 <= k < self.n_t:
+                self.time_slices[k][i_r, i_z] += d_weight
+
+    def get_absorption_image(self, n_photons: int, time_index: int = 0) -> Matrix:
+        """(2 n_r) x n_z image mirrored about the axis, per photon and voxel volume
+        (src/absortion.cpp:93-119)."""
+        if time_index < 0 or time_index >= self.n_t:
+            return Matrix(0, 0)
+        grid = np.asarray(self.time_slices[time_index])
+        n_r, n_z = grid.shape
+        image = Matrix(2 * n_r, n_z)
+        for i in range(n_r):
+            r_in, r_out = i * self.d_r, (i + 1) * self.d_r
+            voxel = math.pi * (r_out * r_out - r_in * r_in) * self.d_z
+            row = grid[i] / (float(n_photons) * voxel)
+            image[n_r - i] = row
+            if i != 0:
+                image[n_r + i] = row
+        return image
+
+    def get_total_image(self, n_photons: int) -> Matrix:
+        return self.get_absorption_image(n_photons, 0)

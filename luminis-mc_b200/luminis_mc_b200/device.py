@@ -46,6 +46,11 @@ class DeviceRun:
             out = rec.cpu().numpy().view(RECORD_DTYPE)
         return stats, out
 
+    def host_absorption(self):
+        """The Absorption grid [n_t][n_r][n_z] of the device tallies (None without one)."""
+        self.torch.cuda.synchronize(self.device)
+        return self.transport.absorption_grid(self.tallies.cpu().numpy())
+
     def host_tallies(self):
         self.torch.cuda.synchronize(self.device)
         flat = self.tallies.cpu().numpy()[: self.transport.tally_size]

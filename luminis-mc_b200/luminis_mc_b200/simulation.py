@@ -131,8 +131,6 @@ def scene_desc(config: SimConfig):
     """Pack the config's Sample / Laser / SensorsGroup into the C scene.
     Returns (scene, keep-alive list, gpu sensors)."""
     validate_sim_config(config)
-    if config.absorption is not None:
-        raise NotImplementedError("the Absorption recorder is not supported by the GPU transport")
     sample, laser, group = config.sample, config.laser, config.detector
     sc = N.SceneDesc()
     keep: list = []
@@ -187,6 +185,12 @@ def scene_desc(config: SimConfig):
     for i, s in enumerate(sensors):
         _sensor_desc(sc.sensors[i], s)
     sc.n_sensors = len(sensors)
+    a = config.absorption
+    if a is not None:
+        A = sc.absorption
+        A.enabled = 1
+        A.radius, A.depth, A.d_r, A.d_z = a.radius, a.depth, a.d_r, a.d_z
+        A.d_t, A.t_max = a.d_t, a.t_max
     return sc, keep, sensors
 
 
@@ -212,6 +216,13 @@ class Transport:
             dims = (C.c_int * 4)()
             N.check(N.lib().lmc_tally_layout(self._h, i, C.byref(off), C.byref(cnt), dims))
             self.layout.append((int(off.value), int(cnt.value), tuple(dims)))
+        off, cnt = C.c_size_t(), C.c_size_t()
+        dims = (C.c_int * 4)()
+        N.check(N.lib().lmc_tally_layout(self._h, N.TALLY_ABSORPTION, C.byref(off), C.byref(cnt),
+                                         dims))
+        # Absorption grid (offset, count, (n_t, n_r, n_z)) or None
+        self.absorption_layout = ((int(off.value), int(cnt.value), tuple(dims[:3]))
+                                  if cnt.value else None)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -268,6 +279,13 @@ class Transport:
         """Per-sensor views of a flat tally buffer, in the sensor layouts."""
         return [tallies[o:o + c].reshape(d) for (o, c, d) in self.layout]
 
+    def absorption_grid(self, tallies: np.ndarray):
+        """The Absorption grid [n_t][n_r][n_z] inside a flat tally buffer (or None)."""
+        if self.absorption_layout is None:
+            return None
+        o, c, d = self.absorption_layout
+        return tallies[o:o + c].reshape(d)
+
 
 def run_simulation_parallel(config: SimConfig, *, precision: str = "fp32", block_size: int = 0,
                             blocks_per_sm: int = 0) -> None:
@@ -289,6 +307,8 @@ def run_simulation_parallel(config: SimConfig, *, precision: str = "fp32", block
         for i, (s, (off, cnt, _)) in enumerate(zip(t.sensors, t.layout)):
             s._tally += flat[off:off + cnt]
             s.hits += stats["hits"][i]
+        if config.absorption is not None:                 # src/simulation.cpp:237-242
+            config.absorption._add(t.absorption_grid(flat))
         _last_stats = stats
     finally:
         t.close()

@@ -104,6 +104,18 @@ class SweepRun:
         flat = self.tallies.cpu().numpy()
         return [flat[o:o + c].reshape(d) for (o, c, d) in self.layout[scene]]
 
+    def host_absorption(self, scene: int):
+        """Scene `scene`'s Absorption grid [n_t][n_r][n_z] (None without one)."""
+        off, cnt = C.c_size_t(), C.c_size_t()
+        dims = (C.c_int * 4)()
+        N.check(N.lib().lmc_sweep_layout(self._h, scene, N.TALLY_ABSORPTION, C.byref(off),
+                                         C.byref(cnt), dims))
+        if not cnt.value:
+            return None
+        self.torch.cuda.synchronize(self.device)
+        flat = self.tallies.cpu().numpy()
+        return flat[off.value:off.value + cnt.value].reshape(tuple(dims[:3]))
+
     def hits(self) -> np.ndarray:
         """[n_scenes, n_sensors max] hit counts of the last run."""
         out = np.zeros(self.n_scenes * N.MAX_SENSORS, dtype=np.uint64)

@@ -273,6 +273,12 @@ def build(lm, spec, n_photons=None, seed=None, n_threads=None):
     cfg.laser = laser
     cfg.detector = group
     keep += [sample, laser, group]
+    a = spec.get("absorption")
+    if a is not None:
+        rec = lm.Absorption(a["radius"], a["depth"], a["d_r"], a["d_z"], a.get("d_t", 0.0),
+                            a.get("t_max", 0.0))
+        cfg.absorption = rec
+        keep.append(rec)
     return cfg, handles, keep
 
 

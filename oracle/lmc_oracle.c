@@ -503,6 +503,7 @@ struct lmc_o_handle {
   osensor sensors[LMC_O_MAX_SENSORS];
   double plane_z[LMC_O_MAX_SENSORS]; /* z_layers keys, ascending */
   int n_planes;
+  int abs_nt, abs_nr, abs_nz;       /* Absorption grid shape (src/absortion.cpp:13-32) */
 };
 
 static int osensor_init(lmc_o_handle *h, osensor *s, const lmc_o_sensor *p, char *err, int err_len)
@@ -1405,6 +1406,28 @@ static void emit_photon(const lmc_o_handle *h, orng *rng, ophoton *ph)
   ph->current_layer = layer_index_at(h, ph->pos.z);
 }
 
+/* Absorption::record_absorption (src/absortion.cpp:54-91): the deposit at the
+ * photon's position in slice 0 and, time-resolved, in the slice of its arrival time. */
+static void record_absorption(const lmc_o_handle *h, const ophoton *ph, double d_weight, double *grid)
+{
+  const lmc_o_absorption *A = &h->scene.absorption;
+  const double r = sqrt(ph->pos.x * ph->pos.x + ph->pos.y * ph->pos.y);
+  const double z = ph->pos.z;
+  if (r > A->radius || z < 0.0 || z > A->depth)
+    return;
+  const double fr = floor(r / A->d_r), fz = floor(z / A->d_z);
+  if (fr >= (double)h->abs_nr || fz >= (double)h->abs_nz)
+    return;
+  const size_t cell = (size_t)fr * (size_t)h->abs_nz + (size_t)fz;
+  grid[cell] += d_weight;
+  if (A->d_t > 0.0) {
+    const double time = ph->launch_time + (ph->opticalpath / ph->velocity);
+    const double fk = floor(time / A->d_t) + 1.0;
+    if (fk >= 1.0 && fk < (double)h->abs_nt)
+      grid[(size_t)fk * (size_t)h->abs_nr * (size_t)h->abs_nz + cell] += d_weight;
+  }
+}
+
 /* run_photon, src/simulation.cpp:255-617 */
 static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track, int max_events,
                        double **tallies, uint64_t *hits, lmc_o_stats *st)
@@ -1613,10 +1636,15 @@ static void run_photon(const lmc_o_handle *h, ophoton *ph, orng *rng, int track,
     st->events++;
     const olayer *SL = layer_at(h, scatter_layer);             /* the layer's aggregate albedo */
     const double layer_mu_t = SL->mu_t;
+    double d_weight = 1.0;
     if (layer_mu_t > 0) {
+      const double absorption_prob = SL->mu_a / layer_mu_t;
       const double scattering_prob = SL->mu_s / layer_mu_t;
+      d_weight = ph->weight * absorption_prob;
       ph->weight *= scattering_prob;
     }
+    if (h->scene.absorption.enabled)                            /* :589-592 */
+      record_absorption(h, ph, d_weight, tallies[h->scene.n_sensors]);
     if (ph->weight < 1e-4) {                                    /* :596-607 */
       if (orng_uniform(rng) < 0.1) {
         ph->weight /= 0.1;
@@ -1676,6 +1704,20 @@ lmc_o_handle *lmc_oracle_create(const lmc_o_scene *scene, char *err, int err_len
   }
   for (int l = 1; l < scene->n_layers; ++l)                     /* sample.cpp:155-158 */
     h->interfaces[h->n_interfaces++] = scene->layers[l].z_min;
+  if (scene->absorption.enabled) {                             /* absortion.cpp:13-32 */
+    const lmc_o_absorption *A = &scene->absorption;
+    if (!(A->d_r > 0.0) || !(A->d_z > 0.0) || !(A->radius >= 0.0) || !(A->depth >= 0.0) ||
+        !(A->d_t >= 0.0) || (A->d_t > 0.0 && !(A->t_max >= 0.0)) ||
+        A->radius / A->d_r > 1e7 || A->depth / A->d_z > 1e7 ||
+        (A->d_t > 0.0 && A->t_max / A->d_t > 1e6)) {
+      snprintf(err, (size_t)err_len, "Absorption: bin widths must be positive and the grid bounded");
+      lmc_oracle_destroy(h);
+      return NULL;
+    }
+    h->abs_nt = (A->d_t > 0.0) ? (int)ceil(A->t_max / A->d_t) + 1 : 1;
+    h->abs_nr = (int)(A->radius / A->d_r) + 1;
+    h->abs_nz = (int)(A->depth / A->d_z) + 1;
+  }
   /* z_layers (detector.hpp:46-48, detector.cpp:166-176): a key per plane within 1e-9 */
   for (int si = 0; si < scene->n_sensors; ++si) {
     if (osensor_init(h, &h->sensors[si], &scene->sensors[si], err, err_len) != 0) {
@@ -1722,6 +1764,11 @@ void lmc_oracle_destroy(lmc_o_handle *h)
 
 int lmc_oracle_sensor_shape(const lmc_o_handle *h, int sensor, int dims[4], size_t *n_doubles)
 {
+  if (sensor == h->scene.n_sensors && h->scene.absorption.enabled) {
+    dims[0] = h->abs_nt; dims[1] = h->abs_nr; dims[2] = h->abs_nz; dims[3] = 1;
+    *n_doubles = (size_t)h->abs_nt * (size_t)h->abs_nr * (size_t)h->abs_nz;
+    return 0;
+  }
   if (sensor < 0 || sensor >= h->scene.n_sensors)
     return -1;
   const osensor *s = &h->sensors[sensor];

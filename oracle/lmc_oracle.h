@@ -115,6 +115,15 @@ typedef struct lmc_o_sensor {
   double theta_pp_max;                    /* estimator: theta cap of the grid (0: none) */
 } lmc_o_sensor;
 
+/* Absorption recorder (include/luminis/core/absortion.hpp:34-80): the weight each
+ * event deposits, binned on a cylindrical (r, z) grid of n_r = floor(radius/d_r)+1 by
+ * n_z = floor(depth/d_z)+1 cells; with d_t > 0 also by time, n_t = ceil(t_max/d_t)+1
+ * slices with slice 0 time-integrated. */
+typedef struct lmc_o_absorption {
+  int enabled;
+  double radius, depth, d_r, d_z, d_t, t_max;
+} lmc_o_absorption;
+
 typedef struct lmc_o_scene {
   double n_host;
   int n_phase; lmc_o_phase phase[LMC_O_MAX_PHASE];
@@ -122,6 +131,7 @@ typedef struct lmc_o_scene {
   int n_layers; lmc_o_layer layers[LMC_O_MAX_LAYERS];
   lmc_o_laser laser;
   int n_sensors; lmc_o_sensor sensors[LMC_O_MAX_SENSORS];
+  lmc_o_absorption absorption;
 } lmc_o_scene;
 
 /* Final state of one photon (per-photon replay comparison). */
@@ -147,14 +157,17 @@ typedef struct lmc_o_handle lmc_o_handle;
 lmc_o_handle *lmc_oracle_create(const lmc_o_scene *scene, char *err, int err_len);
 void lmc_oracle_destroy(lmc_o_handle *h);
 
-/* Doubles a sensor's tally occupies and its shape.  Layouts:
+/* Doubles a sensor's tally occupies and its shape.  Sensor index n_sensors is the
+ * Absorption grid when the scene has one: [n_t][n_r][n_z], dims {n_t, n_r, n_z, 1}.
+ * Layouts:
  *  FARFIELD_CBS      [8 stokes: S0..S3 coherent, S0..S3 incoherent][N_t][N_theta][N_phi]
  *  PLANAR_FLUENCE    [4][N_t][N_x][N_y]
  *  PLANAR_FIELD      [2: Ex, Ey][N_x][N_y][2: re, im]
  *  FARFIELD_FLUENCE  [4][N_t][N_theta][N_phi]                                     */
 int lmc_oracle_sensor_shape(const lmc_o_handle *h, int sensor, int dims[4], size_t *n_doubles);
 
-/* Photons [begin, begin+count) with seed; tallies[s] accumulate (caller zeroes);
+/* Photons [begin, begin+count) with seed; tallies[s] accumulate (caller zeroes),
+ * tallies[n_sensors] the Absorption grid when the scene has one;
  * records (optional) gets count entries; hits[s] incremented. */
 int lmc_oracle_run(lmc_o_handle *h, uint64_t seed, uint64_t begin, uint64_t count, int rng,
                    int max_events, int track_reverse, double **tallies, uint64_t *hits,

@@ -73,11 +73,17 @@ class Sensor(C.Structure):
                 ("dtheta", C.c_double), ("dphi", C.c_double), ("theta_pp_max", C.c_double)]
 
 
+class AbsorptionGrid(C.Structure):
+    _fields_ = [("enabled", C.c_int), ("radius", C.c_double), ("depth", C.c_double),
+                ("d_r", C.c_double), ("d_z", C.c_double), ("d_t", C.c_double),
+                ("t_max", C.c_double)]
+
+
 class Scene(C.Structure):
     _fields_ = [("n_host", C.c_double), ("n_phase", C.c_int), ("phase", Phase * MAXP),
                 ("n_media", C.c_int), ("media", Medium * MAXM), ("n_layers", C.c_int),
                 ("layers", Layer * MAXL), ("laser", Laser), ("n_sensors", C.c_int),
-                ("sensors", Sensor * MAXS)]
+                ("sensors", Sensor * MAXS), ("absorption", AbsorptionGrid)]
 
 
 class Record(C.Structure):
@@ -262,6 +268,12 @@ def scene_from_spec(spec: dict) -> Scene:
         if "events_limit" in s:
             q.f_events = 1
             q.events_min, q.events_max = map(int, s["events_limit"])
+    a = spec.get("absorption")
+    if a is not None:
+        sc.absorption.enabled = 1
+        sc.absorption.radius, sc.absorption.depth = float(a["radius"]), float(a["depth"])
+        sc.absorption.d_r, sc.absorption.d_z = float(a["d_r"]), float(a["d_z"])
+        sc.absorption.d_t, sc.absorption.t_max = float(a.get("d_t", 0.0)), float(a.get("t_max", 0.0))
     return sc
 
 
@@ -271,6 +283,7 @@ class OracleResult:
     hits: np.ndarray
     records: np.ndarray | None
     stats: dict
+    absorption: np.ndarray | None = None   # [n_t][n_r][n_z] deposited weight
 
 
 class Oracle:
@@ -289,6 +302,25 @@ class Oracle:
             n = C.c_size_t()
             lib().lmc_oracle_sensor_shape(self._h, s, dims, C.byref(n))
             self.shapes.append(tuple(dims))
+        self.absorption_shape = None
+        if self._scene.absorption.enabled:
+            dims = (C.c_int * 4)()
+            n = C.c_size_t()
+            lib().lmc_oracle_sensor_shape(self._h, self._scene.n_sensors, dims, C.byref(n))
+            self.absorption_shape = tuple(dims[:3])
+
+    def _buffers(self):
+        """Zeroed tallies, the pointer array the C side fills (the Absorption grid
+        after the sensors) and the grid (or None)."""
+        tallies = [np.zeros(int(np.prod(s)), dtype=np.float64) for s in self.shapes]
+        grid = (np.zeros(self.absorption_shape, dtype=np.float64)
+                if self.absorption_shape is not None else None)
+        ptrs = (C.POINTER(C.c_double) * (len(tallies) + 1))()
+        for i, t in enumerate(tallies):
+            ptrs[i] = t.ctypes.data_as(C.POINTER(C.c_double))
+        if grid is not None:
+            ptrs[len(tallies)] = grid.ctypes.data_as(C.POINTER(C.c_double))
+        return tallies, ptrs, grid
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -302,10 +334,7 @@ class Oracle:
         max_events = int(self.spec.get("max_events", 1000) if max_events is None else max_events)
         if track_reverse is None:
             track_reverse = bool(self.spec.get("track_reverse_paths", True))
-        tallies = [np.zeros(int(np.prod(s)), dtype=np.float64) for s in self.shapes]
-        ptrs = (C.POINTER(C.c_double) * max(1, len(tallies)))()
-        for i, t in enumerate(tallies):
-            ptrs[i] = t.ctypes.data_as(C.POINTER(C.c_double))
+        tallies, ptrs, grid = self._buffers()
         hits = np.zeros(max(1, len(tallies)), dtype=np.uint64)
         rec = np.zeros(n_photons, dtype=RECORD_DTYPE) if records else None
         st = Stats()
@@ -317,7 +346,7 @@ class Oracle:
             raise ValueError(f"oracle run failed ({rc}): launch position outside the sample")
         stats = {n: int(getattr(st, n)) for n, _ in Stats._fields_}
         return OracleResult([t.reshape(s) for t, s in zip(tallies, self.shapes)],
-                            hits[: len(tallies)], rec, stats)
+                            hits[: len(tallies)], rec, stats, grid)
 
     def run_adjoint(self, n_photons: int, seed: int, radial_sensor: int = -1,
                     radial_bins: int = 100, radial_max: float = 5.0, begin: int = 0,
@@ -336,10 +365,7 @@ class Oracle:
             raise ValueError("no adjoint outputs (radial sensor must be a PlanarFluenceSensor)")
         K = 4 * self._scene.n_media
         out = np.zeros((1 + K, n_out), dtype=np.float64)
-        tallies = [np.zeros(int(np.prod(s)), dtype=np.float64) for s in self.shapes]
-        ptrs = (C.POINTER(C.c_double) * max(1, len(tallies)))()
-        for i, t in enumerate(tallies):
-            ptrs[i] = t.ctypes.data_as(C.POINTER(C.c_double))
+        tallies, ptrs, grid = self._buffers()
         hits = np.zeros(max(1, len(tallies)), dtype=np.uint64)
         st = Stats()
         rc = lib().lmc_oracle_run_adjoint(self._h, seed, begin, n_photons, RNG[rng], max_events,
@@ -350,7 +376,7 @@ class Oracle:
             raise ValueError(f"oracle adjoint run failed ({rc})")
         stats = {n: int(getattr(st, n)) for n, _ in Stats._fields_}
         return OracleResult([t.reshape(s) for t, s in zip(tallies, self.shapes)],
-                            hits[: len(tallies)], None, stats), out
+                            hits[: len(tallies)], None, stats, grid), out
 
     def phase_table(self, medium: int):
         n = C.c_int()

@@ -19,6 +19,7 @@ tallies and hit counts:
     python tests/golden/make_golden.py farfield  (far-field fluence from reference records)
     python tests/golden/make_golden.py estimator (estimator-mode FarFieldCBS, Philox stream)
     python tests/golden/make_golden.py mixture   (MixtureLayer scenes, both streams)
+    python tests/golden/make_golden.py absorption (Absorption recorder scenes, both streams)
 
 The fixtures pin the oracle (tests/test_oracle_golden.py) and the GPU path
 (tests/test_gpu_golden.py) without the reference present at test time.
@@ -175,6 +176,36 @@ def mixture_scenes():
     return [a, b, c]
 
 
+def absorption_scenes():
+    """Absorption recorder scenes: the two-layer slab with a time-resolved (r, z, t)
+    grid whose depth ends inside the second layer, and the mixture slab with a
+    time-integrated grid (deposits use the layer's aggregate albedo)."""
+    a = W.bilayer_rgd_mie(1500, 51)
+    a["name"] = "absorption_bilayer"
+    a["media"][0].update(mu_a=2.0)
+    a["media"][1].update(mu_a=0.5)
+    a["sensors"] = [a["sensors"][0]]
+    a["absorption"] = {"radius": 2.0, "depth": 1.5, "d_r": 0.1, "d_z": 0.05, "d_t": 2.0,
+                       "t_max": 20.0}
+    b = W.mixture_bilayer(1200, 52)
+    b["name"] = "absorption_mixture"
+    b["sensors"] = [b["sensors"][0]]
+    b["absorption"] = {"radius": 3.0, "depth": 2.0, "d_r": 0.25, "d_z": 0.1}
+    return [a, b]
+
+
+def absorption_main():
+    meta = {}
+    for spec in absorption_scenes():
+        name = spec["name"]
+        np.savez_compressed(os.path.join(HERE, f"ref_philox_{name}.npz"),
+                            **run_flavour("replay", name, fmt=0, source="absorption_scenes"))
+        np.savez_compressed(os.path.join(HERE, f"ref_xoshiro_{name}.npz"),
+                            **run_flavour("pin", name, source="absorption_scenes"))
+        meta[name] = {"n_photons": spec["n_photons"], "seed": spec["seed"]}
+    print("wrote", meta)
+
+
 def mixture_main():
     meta = {}
     for spec in mixture_scenes():
@@ -289,7 +320,8 @@ def run_flavour(flavour, scene_name, fmt=None, source="golden_scenes"):
     code = f"""
 import sys, json, glob, ctypes, numpy as np
 sys.path.insert(0, {REPO!r}); sys.path.insert(0, {os.path.join(REPO, 'luminis-mc_b200')!r})
-from tests.golden.make_golden import golden_scenes, estimator_scenes, mixture_scenes
+from tests.golden.make_golden import (golden_scenes, estimator_scenes, mixture_scenes,
+                                     absorption_scenes)
 from luminis_mc_b200 import workloads as W
 from oracle import pyoracle as O
 lm = O.reference_module({flavour!r}); lm.set_log_level(lm.LogLevel.off)
@@ -303,6 +335,8 @@ out = {{}}
 for i, (h, s) in enumerate(zip(hs, spec["sensors"])):
     out[f"sensor{{i}}"] = W.tally_arrays(h, s["kind"])
 out["hits"] = np.array([h.hits for h in hs], dtype=np.int64)
+if cfg.absorption is not None:
+    out["absorption"] = np.stack([np.array(m, copy=True) for m in cfg.absorption.time_slices])
 np.savez(sys.argv[1], **out)
 """
     tmp = os.path.join(HERE, f"_tmp_{flavour}_{scene_name}.npz")
@@ -339,5 +373,7 @@ if __name__ == "__main__":
         estimator_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "mixture":
         mixture_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "absorption":
+        absorption_main()
     else:
         main()

@@ -47,17 +47,51 @@ def test_sample_validation_messages():
     assert s.is_inside(lm.Vec3(0, 0, 5.0)) and not s.is_inside(lm.Vec3(0, 0, -1e-9))
 
 
-@pytest.mark.parametrize("extra", ["photon_record", "statistics", "absorption"])
+@pytest.mark.parametrize("extra", ["photon_record", "statistics"])
 def test_unsupported_parts_raise_before_any_launch(extra):
     cfg, _, keep = W.build(lm, W.mie_cbs_small(10, 1))
     if extra == "photon_record":
         cfg.detector.add_detector(lm.PhotonRecordSensor(0.0))
     elif extra == "statistics":
         cfg.detector.add_detector(lm.StatisticsSensor(0.0))
-    elif extra == "absorption":
-        cfg.absorption = lm.Absorption(1.0, 1.0, 0.1, 0.1)
     with pytest.raises(NotImplementedError):
         scene_desc(cfg)
+
+
+def test_absorption_recorder_host_api():
+    """Absorption (src/absortion.cpp): grid shapes, host-side deposits into slice 0 and
+    the arrival-time slice, clone/merge and the mirrored per-volume image."""
+    a = lm.Absorption(1.0, 0.5, 0.25, 0.1, 2.0, 9.0)
+    assert a.n_t == 6 and a.time_slices[0].shape == (5, 6)
+
+    class P:
+        pos = lm.Vec3(0.3, 0.4, 0.25)          # r = 0.5 -> i_r = 2, i_z = 2
+        launch_time, opticalpath, velocity = 0.0, 5.0, 1.0
+
+    a.record_absorption(P, 0.75)
+    assert a.time_slices[0][2, 2] == 0.75 and a.time_slices[3][2, 2] == 0.75
+    P.pos = lm.Vec3(2.0, 0.0, 0.1)            # outside the radius
+    a.record_absorption(P, 1.0)
+    assert sum(float(m.sum()) for m in a.time_slices) == 1.5
+    b = a.clone()
+    assert float(b.time_slices[0].sum()) == 0.0
+    b.merge_from(a)
+    b.merge_from(a)
+    assert b.time_slices[0][2, 2] == 1.5
+    img = a.get_total_image(10)
+    assert img.shape == (10, 6)
+    vox = math.pi * (0.75 ** 2 - 0.5 ** 2) * 0.1
+    assert img[5 - 2, 2] == 0.75 / (10.0 * vox) and img[5 + 2, 2] == img[3, 2]
+    assert a.get_absorption_image(10, 7).shape == (0, 0)
+
+
+def test_absorption_packs_into_the_scene():
+    cfg, _, keep = W.build(lm, W.mie_cbs_small(10, 1))
+    cfg.absorption = lm.Absorption(2.0, 1.0, 0.1, 0.05, 0.5, 10.0)
+    sc, _, _ = scene_desc(cfg)
+    A = sc.absorption
+    assert A.enabled == 1 and (A.radius, A.depth, A.d_r, A.d_z, A.d_t, A.t_max) == (
+        2.0, 1.0, 0.1, 0.05, 0.5, 10.0)
 
 
 def test_mixture_layer_aggregates_and_packing():

@@ -67,6 +67,28 @@ def test_noalloc_matches_lmc_run_twice(make, precision, cuda):
     run.close()
 
 
+def test_noalloc_absorption_grid_matches_lmc_run(cuda):
+    """The Absorption grid sits after the sensors in the caller's tally buffer."""
+    from tests.golden.make_golden import absorption_scenes
+    for spec in absorption_scenes():
+        import torch
+        cfg, _, keep = W.build(lm, spec)
+        run = DeviceRun(cfg)
+        d = run.transport
+        buf = torch.zeros(max(d.tally_size, 1), dtype=torch.float64, device=run.device)
+        st = N.Stats()
+        o = d.opts(precision="fp64")
+        N.check(N.lib().lmc_run_noalloc(C.byref(d.scene), 31, 100, 900, C.byref(o),
+                                        C.c_void_p(buf.data_ptr()), C.byref(st)))
+        flat = buf.cpu().numpy()[: d.tally_size]
+        wst, _ = run.run(900, 31, 100, precision="fp64")
+        _same(d.split(flat), run.host_tallies(), st.as_dict(), wst)
+        ref = run.host_absorption()
+        np.testing.assert_allclose(d.absorption_grid(flat), ref, rtol=RTOL,
+                                   atol=RTOL * np.abs(ref).max())
+        run.close()
+
+
 def test_noalloc_several_queue_batches(cuda):
     """300k photons need several batches of the fixed-size hit queue."""
     spec = W.mie_cbs_small(300_000, 5)
