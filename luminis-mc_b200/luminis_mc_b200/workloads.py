@@ -238,6 +238,22 @@ def build(lm, spec, n_photons=None, seed=None, n_threads=None):
         elif kind == "planar_field":
             det = lm.PlanarFieldSensor(s["z"], s["len_x"], s["len_y"], s["dx"], s["dy"],
                                        s.get("absorb", True), s.get("estimator", False))
+        elif kind == "statistics":
+            det = lm.StatisticsSensor(s["z"], s.get("absorb", False))
+            if s.get("d_t", 0.0) > 0.0:
+                det.set_time_resolution(s["len_t"], s["d_t"])
+            if "events" in s:
+                det.set_events_histogram_bins(int(s["events"]))
+            if "theta" in s:
+                det.set_theta_histogram_bins(*s["theta"])
+            if "phi" in s:
+                det.set_phi_histogram_bins(*s["phi"])
+            if "depth" in s:
+                det.set_depth_histogram_bins(*s["depth"])
+            if "time" in s:
+                det.set_time_histogram_bins(*s["time"])
+            if "weight" in s:
+                det.set_weight_histogram_bins(*s["weight"])
         elif kind == "farfield_fluence":
             if not hasattr(lm, "FarFieldFluenceSensor"):
                 handles.append(None)
@@ -291,6 +307,13 @@ def tally_arrays(lm_sensor, kind):
     if kind in ("planar_fluence", "farfield_fluence"):
         grids = [lm_sensor.S0, lm_sensor.S1, lm_sensor.S2, lm_sensor.S3]
         return np.stack([np.stack([np.array(m, copy=True) for m in g]) for g in grids])
+    if kind == "statistics":
+        parts = []
+        for name in ("events", "theta", "phi", "depth", "time", "weight"):
+            if getattr(lm_sensor, f"{name}_histogram_bins_set"):
+                parts.append(np.asarray(getattr(lm_sensor, f"{name}_histogram"),
+                                        dtype=np.float64).ravel())
+        return np.concatenate(parts) if parts else np.zeros(0)
     if kind == "planar_field":
         ex = np.array(lm_sensor.Ex, copy=True)
         ey = np.array(lm_sensor.Ey, copy=True)

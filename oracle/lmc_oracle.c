@@ -480,6 +480,9 @@ typedef struct {
   double cos_min, cos_max;        /* set_theta_limit cache (src/detector.cpp:334-343) */
   int N_t, N_x, N_y, N_theta, N_phi;
   size_t n_doubles;
+  /* STATISTICS: bin widths (src/detector.cpp:1836-1888) and histogram offsets */
+  double st_dtheta, st_dphi, st_ddepth, st_dtime, st_dweight;
+  size_t st_off[6];
 } osensor;
 
 /* A layer's transport coefficients (Layer::mu_attenuation/mu_scattering/mu_absorption,
@@ -539,6 +542,34 @@ static int osensor_init(lmc_o_handle *h, osensor *s, const lmc_o_sensor *p, char
     s->N_y = (int)ceil(p->len_y / p->dy);
     s->n_doubles = (size_t)4 * s->N_x * s->N_y;
     break;
+  case LMC_O_SENSOR_STATISTICS: {                               /* :1571-1579, :1802-1888 */
+    const lmc_o_statistics *q = &p->stats;
+    s->p.estimator = 0;
+    s->N_t = (p->dt <= 0.0) ? 1 : (int)ceil(p->len_t / p->dt) + 1;
+    if (p->dt <= 0.0)
+      s->p.dt = 0.0;
+    if (q->n_events < 0 || q->n_theta < 0 || q->n_phi < 0 || q->n_depth < 0 || q->n_time < 0 ||
+        q->n_weight < 0) {
+      snprintf(err, (size_t)err_len, "StatisticsSensor: histogram sizes must be non-negative");
+      return -1;
+    }
+    const int set = q->set;
+    const size_t nt = (size_t)s->N_t;
+    size_t n = 0;
+    s->st_off[0] = n; n += (set & LMC_O_STAT_EVENTS) ? nt * (size_t)q->n_events : 0;
+    s->st_off[1] = n; n += (set & LMC_O_STAT_THETA) ? nt * (size_t)q->n_theta : 0;
+    s->st_off[2] = n; n += (set & LMC_O_STAT_PHI) ? nt * (size_t)q->n_phi : 0;
+    s->st_off[3] = n; n += (set & LMC_O_STAT_DEPTH) ? nt * (size_t)q->n_depth : 0;
+    s->st_off[4] = n; n += (set & LMC_O_STAT_TIME) ? (size_t)q->n_time : 0;
+    s->st_off[5] = n; n += (set & LMC_O_STAT_WEIGHT) ? (size_t)q->n_weight : 0;
+    s->n_doubles = n;
+    s->st_dtheta = (q->theta_max - q->theta_min) / q->n_theta;
+    s->st_dphi = (q->phi_max - q->phi_min) / q->n_phi;
+    s->st_ddepth = q->depth_max / q->n_depth;
+    s->st_dtime = q->time_max / q->n_time;
+    s->st_dweight = q->weight_max / q->n_weight;
+    break;
+  }
   default:
     snprintf(err, (size_t)err_len, "unknown sensor kind %d", p->kind);
     return -1;
@@ -1301,6 +1332,67 @@ static void estimate_farfield_cbs(const lmc_o_handle *h, const osensor *s, doubl
   *hits += 1;
 }
 
+/* StatisticsSensor::process_hit (src/detector.cpp:1720-1800): one count per active
+ * histogram, in bin 0 of its time axis and in the arrival-time window.  Bins that
+ * would fall past a histogram's end through rounding are skipped. */
+static void process_hit_statistics(const osensor *s, double *tally, const ophoton *ph,
+                                   const ointeraction *info, uint64_t *hits)
+{
+  const lmc_o_statistics *q = &s->p.stats;
+  const double arrival_time = ph->launch_time + (info->opticalpath_at_hit / ph->velocity);
+  int t_idx = -1;
+  if (s->N_t > 1 && s->p.dt > 0.0 && arrival_time >= 0.0 && arrival_time < s->p.len_t) {
+    t_idx = (int)(arrival_time / s->p.dt) + 1;
+    if (t_idx >= s->N_t)
+      t_idx = -1;
+  }
+#define DEPOSIT(off, nb, idx)                                                         \
+  do {                                                                                \
+    if ((idx) >= 0 && (idx) < (nb)) {                                                 \
+      tally[(off) + (size_t)(idx)] += 1.0;                                            \
+      if (t_idx >= 1 && t_idx < s->N_t)                                               \
+        tally[(off) + (size_t)t_idx * (size_t)(nb) + (size_t)(idx)] += 1.0;           \
+    }                                                                                 \
+  } while (0)
+  if (q->set & LMC_O_STAT_EVENTS) {
+    const int events = (int)ph->events;
+    if (events >= 0 && events < q->n_events)
+      DEPOSIT(s->st_off[0], q->n_events, events);
+  }
+  if (q->set & LMC_O_STAT_THETA) {
+    const double theta = acos(-ph->P.a[2][2]);
+    if (theta >= q->theta_min && theta < q->theta_max)
+      DEPOSIT(s->st_off[1], q->n_theta, (int)((theta - q->theta_min) / s->st_dtheta));
+  }
+  if (q->set & LMC_O_STAT_PHI) {
+    double phi = atan2(ph->P.a[2][1], ph->P.a[2][0]);
+    if (phi < 0)
+      phi += 2.0 * M_PI;
+    if (phi >= q->phi_min && phi < q->phi_max)
+      DEPOSIT(s->st_off[2], q->n_phi, (int)((phi - q->phi_min) / s->st_dphi));
+  }
+  if (q->set & LMC_O_STAT_DEPTH) {
+    const double depth = ph->penetration_depth;
+    if (depth >= 0 && depth < q->depth_max)
+      DEPOSIT(s->st_off[3], q->n_depth, (int)(depth / s->st_ddepth));
+  }
+#undef DEPOSIT
+  if (q->set & LMC_O_STAT_TIME) {
+    const double fi = arrival_time / s->st_dtime;
+    if (fi >= 1.0 && fi < (double)q->n_time)
+      tally[s->st_off[4] + (size_t)fi] += 1.0;
+  }
+  if (q->set & LMC_O_STAT_WEIGHT) {
+    const double weight = ph->weight;
+    if (weight >= 0 && weight < q->weight_max) {
+      const int idx = (int)(weight / s->st_dweight);
+      if (idx < q->n_weight)
+        tally[s->st_off[5] + (size_t)idx] += 1.0;
+    }
+  }
+  *hits += 1;
+}
+
 /* SensorsGroup::record_hit, src/detector.cpp:178-270 */
 static int record_hit(const lmc_o_handle *h, ophoton *ph, double **tallies, uint64_t *hits)
 {
@@ -1349,6 +1441,8 @@ static int record_hit(const lmc_o_handle *h, ophoton *ph, double **tallies, uint
         process_hit_fluence(s, tallies[si], ph, &info, &hits[si]);
       else if (s->p.kind == LMC_O_SENSOR_PLANAR_FIELD)
         process_hit_field(s, tallies[si], ph, &info, &hits[si]);
+      else if (s->p.kind == LMC_O_SENSOR_STATISTICS)
+        process_hit_statistics(s, tallies[si], ph, &info, &hits[si]);
       if (hits[si] != before) {
         ph->hit = hit;
         ph->n_hits++;
@@ -1779,6 +1873,8 @@ int lmc_oracle_sensor_shape(const lmc_o_handle *h, int sensor, int dims[4], size
     dims[0] = 4; dims[1] = s->N_t; dims[2] = s->N_theta; dims[3] = s->N_phi; break;
   case LMC_O_SENSOR_PLANAR_FLUENCE:
     dims[0] = 4; dims[1] = s->N_t; dims[2] = s->N_x; dims[3] = s->N_y; break;
+  case LMC_O_SENSOR_STATISTICS:
+    dims[0] = s->N_t; dims[1] = (int)s->n_doubles; dims[2] = 0; dims[3] = 0; break;
   default:
     dims[0] = 2; dims[1] = s->N_x; dims[2] = s->N_y; dims[3] = 2; break;
   }

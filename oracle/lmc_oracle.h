@@ -49,8 +49,25 @@ enum lmc_o_sensor_kind {
   LMC_O_SENSOR_FARFIELD_CBS = 0,
   LMC_O_SENSOR_PLANAR_FLUENCE = 1,
   LMC_O_SENSOR_PLANAR_FIELD = 2,
-  LMC_O_SENSOR_FARFIELD_FLUENCE = 3
+  LMC_O_SENSOR_FARFIELD_FLUENCE = 3,
+  LMC_O_SENSOR_STATISTICS = 4      /* src/detector.cpp:1569-1888 */
 };
+
+/* StatisticsSensor histograms (include/luminis/core/detector.hpp:595-699), each
+ * present when its bit of `set` is: 1 events [0, n_events), 2 theta, 4 phi,
+ * 8 penetration depth, 16 arrival time, 32 weight.  The time resolution is the
+ * sensor's len_t / dt (set_time_resolution). */
+enum { LMC_O_STAT_EVENTS = 1, LMC_O_STAT_THETA = 2, LMC_O_STAT_PHI = 4, LMC_O_STAT_DEPTH = 8,
+       LMC_O_STAT_TIME = 16, LMC_O_STAT_WEIGHT = 32 };
+typedef struct lmc_o_statistics {
+  int set;
+  int n_events;
+  int n_theta; double theta_min, theta_max;
+  int n_phi; double phi_min, phi_max;
+  int n_depth; double depth_max;
+  int n_time; double time_max;
+  int n_weight; double weight_max;
+} lmc_o_statistics;
 
 enum lmc_o_rng { LMC_O_RNG_XOSHIRO = 0, LMC_O_RNG_PHILOX_U53 = 1, LMC_O_RNG_PHILOX_U24 = 2 };
 
@@ -113,6 +130,7 @@ typedef struct lmc_o_sensor {
   /* far-field sensors (len_t and dt above are the time axis) */
   double theta_max_grid, phi_max_grid, dtheta, dphi;
   double theta_pp_max;                    /* estimator: theta cap of the grid (0: none) */
+  lmc_o_statistics stats;                 /* STATISTICS sensors                        */
 } lmc_o_sensor;
 
 /* Absorption recorder (include/luminis/core/absortion.hpp:34-80): the weight each
@@ -163,7 +181,11 @@ void lmc_oracle_destroy(lmc_o_handle *h);
  *  FARFIELD_CBS      [8 stokes: S0..S3 coherent, S0..S3 incoherent][N_t][N_theta][N_phi]
  *  PLANAR_FLUENCE    [4][N_t][N_x][N_y]
  *  PLANAR_FIELD      [2: Ex, Ey][N_x][N_y][2: re, im]
- *  FARFIELD_FLUENCE  [4][N_t][N_theta][N_phi]                                     */
+ *  FARFIELD_FLUENCE  [4][N_t][N_theta][N_phi]
+ *  STATISTICS        counts, the histograms present one after another:
+ *                    events [N_t][n_events], theta [N_t][n_theta], phi [N_t][n_phi],
+ *                    depth [N_t][n_depth], time [n_time], weight [n_weight];
+ *                    dims {N_t, n_doubles, 0, 0}                                  */
 int lmc_oracle_sensor_shape(const lmc_o_handle *h, int sensor, int dims[4], size_t *n_doubles);
 
 /* Photons [begin, begin+count) with seed; tallies[s] accumulate (caller zeroes),

@@ -21,7 +21,9 @@ MAXP, MAXM, MAXL, MAXS = 16, 16, 16, 8
 
 PHASE_KIND = {"uniform": 0, "rayleigh": 1, "hg": 2, "rd": 3, "rdemc": 4, "draine": 5, "mie": 6}
 MEDIUM_KIND = {"rgd": 0, "mie": 1}
-SENSOR_KIND = {"farfield_cbs": 0, "planar_fluence": 1, "planar_field": 2, "farfield_fluence": 3}
+SENSOR_KIND = {"farfield_cbs": 0, "planar_fluence": 1, "planar_field": 2, "farfield_fluence": 3,
+               "statistics": 4}
+STAT_BITS = {"events": 1, "theta": 2, "phi": 4, "depth": 8, "time": 16, "weight": 32}
 RNG = {"xoshiro": 0, "philox_u53": 1, "philox_u24": 2}
 SOURCE = {"point": 0, "uniform": 1, "gaussian": 2}
 TEMPORAL = {"delta": 0, "gaussian": 1, "tophat": 2, "exponential": 3, "pulsetrain": 4, "cw": 5}
@@ -59,6 +61,15 @@ class Laser(C.Structure):
                 ("repetition_rate", C.c_double), ("time_offset", C.c_double)]
 
 
+class Statistics(C.Structure):
+    _fields_ = [("set", C.c_int), ("n_events", C.c_int),
+                ("n_theta", C.c_int), ("theta_min", C.c_double), ("theta_max", C.c_double),
+                ("n_phi", C.c_int), ("phi_min", C.c_double), ("phi_max", C.c_double),
+                ("n_depth", C.c_int), ("depth_max", C.c_double),
+                ("n_time", C.c_int), ("time_max", C.c_double),
+                ("n_weight", C.c_int), ("weight_max", C.c_double)]
+
+
 class Sensor(C.Structure):
     _fields_ = [("kind", C.c_int), ("z", C.c_double), ("absorb", C.c_int), ("estimator", C.c_int),
                 ("f_theta", C.c_int), ("theta_min", C.c_double), ("theta_max", C.c_double),
@@ -70,7 +81,8 @@ class Sensor(C.Structure):
                 ("len_x", C.c_double), ("len_y", C.c_double), ("len_t", C.c_double),
                 ("dx", C.c_double), ("dy", C.c_double), ("dt", C.c_double),
                 ("theta_max_grid", C.c_double), ("phi_max_grid", C.c_double),
-                ("dtheta", C.c_double), ("dphi", C.c_double), ("theta_pp_max", C.c_double)]
+                ("dtheta", C.c_double), ("dphi", C.c_double), ("theta_pp_max", C.c_double),
+                ("stats", Statistics)]
 
 
 class AbsorptionGrid(C.Structure):
@@ -243,6 +255,28 @@ def scene_from_spec(spec: dict) -> Scene:
             q.dphi = float(s["d_phi"])
             q.theta_pp_max = float(s.get("theta_pp_max", 0.0))
             q.dt = float(s.get("d_t", 0.0))
+        elif kind == "statistics":
+            q.z = float(s["z"])
+            q.absorb = int(bool(s.get("absorb", False)))
+            q.len_t, q.dt = float(s.get("len_t", 0.0)), float(s.get("d_t", 0.0))
+            st = q.stats
+            for key, bit in STAT_BITS.items():
+                if key in s:
+                    st.set |= bit
+            if "events" in s:
+                st.n_events = int(s["events"])
+            if "theta" in s:
+                lo, hi, nb = s["theta"]
+                st.theta_min, st.theta_max, st.n_theta = float(lo), float(hi), int(nb)
+            if "phi" in s:
+                lo, hi, nb = s["phi"]
+                st.phi_min, st.phi_max, st.n_phi = float(lo), float(hi), int(nb)
+            if "depth" in s:
+                st.depth_max, st.n_depth = float(s["depth"][0]), int(s["depth"][1])
+            if "time" in s:
+                st.time_max, st.n_time = float(s["time"][0]), int(s["time"][1])
+            if "weight" in s:
+                st.weight_max, st.n_weight = float(s["weight"][0]), int(s["weight"][1])
         else:
             q.z = float(s["z"])
             q.absorb = int(bool(s.get("absorb", True)))
@@ -301,7 +335,10 @@ class Oracle:
             dims = (C.c_int * 4)()
             n = C.c_size_t()
             lib().lmc_oracle_sensor_shape(self._h, s, dims, C.byref(n))
-            self.shapes.append(tuple(dims))
+            if self._scene.sensors[s].kind == SENSOR_KIND["statistics"]:
+                self.shapes.append((int(n.value),))     # histograms one after another
+            else:
+                self.shapes.append(tuple(dims))
         self.absorption_shape = None
         if self._scene.absorption.enabled:
             dims = (C.c_int * 4)()

@@ -20,6 +20,7 @@ tallies and hit counts:
     python tests/golden/make_golden.py estimator (estimator-mode FarFieldCBS, Philox stream)
     python tests/golden/make_golden.py mixture   (MixtureLayer scenes, both streams)
     python tests/golden/make_golden.py absorption (Absorption recorder scenes, both streams)
+    python tests/golden/make_golden.py statistics (StatisticsSensor scenes, both streams)
 
 The fixtures pin the oracle (tests/test_oracle_golden.py) and the GPU path
 (tests/test_gpu_golden.py) without the reference present at test time.
@@ -194,6 +195,39 @@ def absorption_scenes():
     return [a, b]
 
 
+def statistics_scenes():
+    """StatisticsSensor scenes: on the two-layer slab a time-resolved sensor with all
+    six histograms beside the FarFieldCBS sensor at z = 0, and a non-absorbing one
+    inside the sample (z = 0.25, crossed any number of times, backward crossings
+    only); on the Mie medium a sensor with theta and event filters."""
+    a = W.bilayer_rgd_mie(1500, 61)
+    a["name"] = "stats_bilayer"
+    a["sensors"] = [a["sensors"][0],
+                    {"kind": "statistics", "z": 0.0, "absorb": True, "len_t": 20.0, "d_t": 2.0,
+                     "events": 200, "theta": (0.0, W.PI / 2, 30), "phi": (0.0, 2 * W.PI, 12),
+                     "depth": (3.0, 30), "time": (30.0, 30), "weight": (1.0, 20)},
+                    {"kind": "statistics", "z": 0.25, "absorb": False, "events": 60,
+                     "depth": (2.0, 40), "direction_limit": "backward"}]
+    b = W.mie_cbs_small(2500, 62)
+    b["name"] = "stats_mie"
+    b["sensors"] = [{"kind": "statistics", "z": 0.0, "absorb": True, "events": 100,
+                     "theta": (0.0, 1.2, 24), "weight": (0.5, 25), "theta_limit": (0.1, 1.0),
+                     "events_limit": (2, 80)}]
+    return [a, b]
+
+
+def statistics_main():
+    meta = {}
+    for spec in statistics_scenes():
+        name = spec["name"]
+        np.savez_compressed(os.path.join(HERE, f"ref_philox_{name}.npz"),
+                            **run_flavour("replay", name, fmt=0, source="statistics_scenes"))
+        np.savez_compressed(os.path.join(HERE, f"ref_xoshiro_{name}.npz"),
+                            **run_flavour("pin", name, source="statistics_scenes"))
+        meta[name] = {"n_photons": spec["n_photons"], "seed": spec["seed"]}
+    print("wrote", meta)
+
+
 def absorption_main():
     meta = {}
     for spec in absorption_scenes():
@@ -321,7 +355,7 @@ def run_flavour(flavour, scene_name, fmt=None, source="golden_scenes"):
 import sys, json, glob, ctypes, numpy as np
 sys.path.insert(0, {REPO!r}); sys.path.insert(0, {os.path.join(REPO, 'luminis-mc_b200')!r})
 from tests.golden.make_golden import (golden_scenes, estimator_scenes, mixture_scenes,
-                                     absorption_scenes)
+                                     absorption_scenes, statistics_scenes)
 from luminis_mc_b200 import workloads as W
 from oracle import pyoracle as O
 lm = O.reference_module({flavour!r}); lm.set_log_level(lm.LogLevel.off)
@@ -375,5 +409,7 @@ if __name__ == "__main__":
         mixture_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "absorption":
         absorption_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "statistics":
+        statistics_main()
     else:
         main()
