@@ -120,9 +120,29 @@ typedef enum lmc_sensor_kind {
   LMC_SENSOR_FARFIELD_CBS = 0,      /* FarFieldCBSSensor (src/detector.cpp:851-1310)  */
   LMC_SENSOR_PLANAR_FLUENCE = 1,    /* PlanarFluenceSensor (src/detector.cpp:704-841) */
   LMC_SENSOR_PLANAR_FIELD = 2,      /* PlanarFieldSensor (src/detector.cpp:490-568)   */
-  LMC_SENSOR_FARFIELD_FLUENCE = 3   /* far-field |E_f|^2 Stokes on (theta, phi); no
+  LMC_SENSOR_FARFIELD_FLUENCE = 3,  /* far-field |E_f|^2 Stokes on (theta, phi); no
                                        counterpart in the reference's sources         */
+  LMC_SENSOR_STATISTICS = 4         /* StatisticsSensor (src/detector.cpp:1569-1888)  */
 } lmc_sensor_kind;
+
+/* StatisticsSensor histograms (include/luminis/core/detector.hpp:595-699): counts of
+ * the crossings a sensor takes, each histogram present when its bit of `set` is:
+ *  events [0, n_events); theta = acos(-s_z) on [theta_min, theta_max) in n_theta bins;
+ *  phi = atan2(s_y, s_x) in [0, 2 pi) on [phi_min, phi_max); penetration depth on
+ *  [0, depth_max); arrival time t on bins [1, n_time) of width time_max / n_time;
+ *  weight on [0, weight_max).  The first four have the sensor's time axis (len_t, dt:
+ *  slice 0 integrated, slice floor(t/dt)+1 the window), time and weight do not. */
+enum { LMC_STAT_EVENTS = 1, LMC_STAT_THETA = 2, LMC_STAT_PHI = 4, LMC_STAT_DEPTH = 8,
+       LMC_STAT_TIME = 16, LMC_STAT_WEIGHT = 32 };
+typedef struct lmc_statistics_desc {
+  int set;
+  int n_events;
+  int n_theta; double theta_min, theta_max;
+  int n_phi; double phi_min, phi_max;
+  int n_depth; double depth_max;
+  int n_time; double time_max;
+  int n_weight; double weight_max;
+} lmc_statistics_desc;
 
 /* One sensor (Sensor + subclass fields, include/luminis/core/detector.hpp:95-562).
  * Filters follow Sensor::check_conditions (src/detector.cpp:374-417). */
@@ -139,6 +159,7 @@ typedef struct lmc_sensor_desc {
   double theta_max_grid, phi_max_grid, dtheta, dphi;   /* far-field sensors         */
   double theta_pp_max;          /* estimator-mode FarFieldCBS: theta cap of the estimated
                                    grid, <= 0 none (FarFieldCBSSensor::theta_pp_max)   */
+  lmc_statistics_desc stats;    /* LMC_SENSOR_STATISTICS                               */
 } lmc_sensor_desc;
 
 /* Absorption recorder (include/luminis/core/absortion.hpp:34-80,
@@ -230,7 +251,10 @@ LMC_API void lmc_destroy(lmc_handle *h);
  * sensor = -1 returns the total size in *count; LMC_TALLY_ABSORPTION the Absorption
  * grid (count 0 without one).  dims as in the oracle:
  *  FARFIELD_CBS [8][N_t][N_theta][N_phi], PLANAR_FLUENCE [4][N_t][N_x][N_y],
- *  PLANAR_FIELD [2][N_x][N_y][2], FARFIELD_FLUENCE [4][N_t][N_theta][N_phi]. */
+ *  PLANAR_FIELD [2][N_x][N_y][2], FARFIELD_FLUENCE [4][N_t][N_theta][N_phi],
+ *  STATISTICS counts (as doubles) of the histograms present, one after another:
+ *  events [N_t][n_events], theta [N_t][n_theta], phi [N_t][n_phi], depth
+ *  [N_t][n_depth], time [n_time], weight [n_weight]; dims {N_t, count, 0, 0}. */
 LMC_API lmc_status lmc_tally_layout(const lmc_handle *h, int sensor, size_t *offset, size_t *count,
                             int dims[4]);
 

@@ -49,6 +49,15 @@ struct AbsorbGrid {
   unsigned long long off;
 };
 
+// StatisticsSensor histograms (src/detector.cpp:1720-1888): bin parameters and the
+// offsets (doubles) of the histograms present from the sensor's tally_off.
+struct StatHist {
+  int set, n_events, n_theta, n_phi, n_depth, n_time, n_weight, pad;
+  double theta_min, theta_max, phi_min, phi_max, depth_max, weight_max;
+  double dtheta, dphi, ddepth, dtime, dweight;
+  unsigned long long off[6];             // events, theta, phi, depth, time, weight
+};
+
 struct Sensor {
   int kind, plane, absorb, estimator;
   int f_theta, f_phi, f_pos, f_dir, f_events, direction, events_min, events_max;
@@ -58,7 +67,10 @@ struct Sensor {
   int est_n;                             // estimator-mode FarFieldCBS: bins estimated
   unsigned long long tally_off;          // offset in doubles into the tally buffer
   unsigned long long plane_stride;       // doubles between Stokes planes
-  const double4 *est_bins;               // per estimated bin: s_out (x, y, z), dOmega dphi
+  union {                                // device memory, by kind:
+    const double4 *est_bins;             //  estimator FarFieldCBS: per bin s_out, dOmega dphi
+    const StatHist *stat;                //  StatisticsSensor: its histograms
+  };
 };
 
 struct Laser {
@@ -90,6 +102,7 @@ struct __align__(16) Scene {
   Sensor sensors[LMC_MAX_SENSORS];
   Laser laser;
   AbsorbGrid absorb;
+  unsigned stat_mask;                    // StatisticsSensors (hits carry the penetration depth)
 };
 
 // Device scratch of one run: photon work counter, statistics, error word.
@@ -106,7 +119,7 @@ struct Scratch {
 // filters, written by the transport kernel and consumed by the tally kernel.
 // Struct-of-arrays, `cap` entries per field.
 enum QueueU32 { kQPhotonLo = 0, kQPhotonHi, kQEvents, kQMask, kQMedia, kQScene, kQU32Fields };
-enum QueueF64 { kQWeight = 0, kQOpath, kQF64Fields };
+enum QueueF64 { kQWeight = 0, kQOpath, kQPen, kQF64Fields };
 enum QueueR {
   kQHit = 0,                  // 3: hit point
   kQP = 3,                    // 9: P_local at the crossing (rows m, n, s)

@@ -652,6 +652,7 @@ __device__ __forceinline__ double launch_time(const Scene &sc, const RunParams &
 template <typename R> struct HitData {
   uint32_t p_lo, p_hi, events, first_med, last_med;
   double w, opath;             // weight, geometric path length at the hit point
+  double pen;                  // penetration depth (StatisticsSensor)
   R hx, hy, hz;                // hit point
   R P[9];                      // P_local rows m, n, s
   Cx<R> Em, En;
@@ -925,6 +926,64 @@ __device__ bool hit_field(const Scene &sc, const RunParams &rp, const Sensor &s,
   return true;
 }
 
+// StatisticsSensor::process_hit (src/detector.cpp:1720-1800): one count in every
+// histogram the hit falls in, in slice 0 and in the arrival-time window of the four
+// time-resolved ones.  Bins past a histogram's end are skipped.  Always counted.
+// Out of line with scalar arguments (arrival time, events, exit direction s,
+// penetration depth, weight), so that the callers' hit state stays in registers.
+__device__ __noinline__ void hit_statistics(const Sensor &s, double *tallies, double arrival,
+                                            uint32_t events, double sx, double sy, double sz,
+                                            double pen, double w)
+{
+  const StatHist &q = *s.stat;
+  int t_idx = -1;
+  if (s.N_t > 1 && s.dt > 0.0 && arrival >= 0.0 && arrival < s.len_t) {
+    t_idx = (int)(arrival / s.dt) + 1;
+    if (t_idx >= s.N_t)
+      t_idx = -1;
+  }
+  double *base = tallies + s.tally_off;
+  auto deposit = [&](unsigned long long off, int nb, int idx) {
+    if (idx >= 0 && idx < nb) {
+      atomicAdd(base + off + idx, 1.0);
+      if (t_idx >= 1)
+        atomicAdd(base + off + (unsigned long long)t_idx * nb + idx, 1.0);
+    }
+  };
+  if (q.set & LMC_STAT_EVENTS) {
+    if ((int)events >= 0 && (int)events < q.n_events)
+      deposit(q.off[0], q.n_events, (int)events);
+  }
+  if (q.set & LMC_STAT_THETA) {
+    const double theta = acos(-sz);
+    if (theta >= q.theta_min && theta < q.theta_max)
+      deposit(q.off[1], q.n_theta, (int)((theta - q.theta_min) / q.dtheta));
+  }
+  if (q.set & LMC_STAT_PHI) {
+    double phi = atan2(sy, sx);
+    if (phi < 0)
+      phi += 2.0 * 3.141592653589793;
+    if (phi >= q.phi_min && phi < q.phi_max)
+      deposit(q.off[2], q.n_phi, (int)((phi - q.phi_min) / q.dphi));
+  }
+  if (q.set & LMC_STAT_DEPTH) {
+    if (pen >= 0 && pen < q.depth_max)
+      deposit(q.off[3], q.n_depth, (int)(pen / q.ddepth));
+  }
+  if (q.set & LMC_STAT_TIME) {
+    const double fi = arrival / q.dtime;
+    if (fi >= 1.0 && fi < (double)q.n_time)
+      atomicAdd(base + q.off[4] + (unsigned long long)fi, 1.0);
+  }
+  if (q.set & LMC_STAT_WEIGHT) {
+    if (w >= 0 && w < q.weight_max) {
+      const int idx = (int)(w / q.dweight);
+      if (idx < q.n_weight)
+        atomicAdd(base + q.off[5] + idx, 1.0);
+    }
+  }
+}
+
 // process_hit of every sensor in `mask` (all on the plane of this hit), in
 // insertion order, as SensorsGroup::record_hit calls them (src/detector.cpp:244-265).
 template <typename R, bool kAdj>
@@ -943,6 +1002,13 @@ __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData
       counted = hit_fluence<R, kAdj>(sc, rp, s, h, si, hs, s_rad);
     else if (s.kind == LMC_SENSOR_PLANAR_FIELD)
       counted = hit_field<R>(sc, rp, s, h);
+    else if (s.kind == LMC_SENSOR_STATISTICS) {
+      const double arrival = (s.dt > 0 || (s.stat->set & LMC_STAT_TIME))
+                                 ? hit_launch_time<R>(sc, rp, h) + h.opath : 0.0;
+      hit_statistics(s, rp.tallies, arrival, h.events, (double)h.P[6], (double)h.P[7],
+                     (double)h.P[8], h.pen, h.w);
+      counted = true;
+    }
     else
       counted = hit_farfield<R, kAdj>(sc, rp, s, h, rec, si, hs);
     if (counted) {
@@ -1299,6 +1365,7 @@ __device__ __forceinline__ void fill_hit(const Photon<R> &ph, const Side<R> &sid
   h.last_med = ph.last_med;
   h.w = ph.w;
   h.opath = opath;
+  h.pen = (double)ph.pen;
   h.hx = hx; h.hy = hy; h.hz = hz;
 #pragma unroll
   for (int j = 0; j < 9; ++j) {
@@ -1348,6 +1415,8 @@ __device__ __forceinline__ void enqueue_hit(const Scene &sc, const RunParams &rp
   q.u32[kQScene * C + slot] = (uint32_t)ph.scene;
   q.f64[kQWeight * C + slot] = ph.w;
   q.f64[kQOpath * C + slot] = opath;
+  if (mask & sc.stat_mask)
+    q.f64[kQPen * C + slot] = (double)ph.pen;
   R *r = static_cast<R *>(q.r);
   r[(kQHit + 0) * C + slot] = hx;
   r[(kQHit + 1) * C + slot] = hy;
@@ -1933,6 +2002,7 @@ __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__
     h.last_med = media >> 16;
     h.w = q.f64[kQWeight * C + i];
     h.opath = q.f64[kQOpath * C + i];
+    h.pen = (mask & sc.stat_mask) ? q.f64[kQPen * C + i] : 0.0;
     h.hx = r[(kQHit + 0) * C + i];
     h.hy = r[(kQHit + 1) * C + i];
     h.hz = r[(kQHit + 2) * C + i];

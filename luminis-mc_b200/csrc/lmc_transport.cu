@@ -204,8 +204,19 @@ lmc_status validate(const lmc_scene *s)
                                  "std::out_of_range from Sample::get_layer)");
   for (int i = 0; i < s->n_sensors; ++i) {
     const lmc_sensor_desc &S = s->sensors[i];
-    if (S.kind < 0 || S.kind > 3)
+    if (S.kind < 0 || S.kind > 4)
       return fail(LMC_ERR_INVALID, "unknown sensor kind");
+    if (S.kind == LMC_SENSOR_STATISTICS) {                 // src/detector.cpp:1802-1888
+      const lmc_statistics_desc &q = S.stats;
+      if (q.n_events < 0 || q.n_theta < 0 || q.n_phi < 0 || q.n_depth < 0 || q.n_time < 0 ||
+          q.n_weight < 0)
+        return fail(LMC_ERR_INVALID, "StatisticsSensor: histogram sizes must be non-negative");
+      if (!finite(S.len_t) || !finite(S.dt))
+        return fail(LMC_ERR_INVALID, "StatisticsSensor: time resolution must be finite");
+      if (S.dt > 0 && S.len_t / S.dt > 1e6)
+        return fail(LMC_ERR_INVALID, "StatisticsSensor: at most 1e6 time windows");
+      continue;
+    }
     if (S.kind == LMC_SENSOR_FARFIELD_CBS || S.kind == LMC_SENSOR_FARFIELD_FLUENCE) {
       if (!(S.dtheta > 0) || !(S.dphi > 0) || !(S.theta_max_grid > 0) || !(S.phi_max_grid > 0))
         return fail(LMC_ERR_INVALID, "far-field sensor bin widths and extents must be positive");
@@ -248,6 +259,22 @@ void fill_sensor(const lmc_sensor_desc &S, dev::Sensor &d, size_t &count, int di
     d.plane_stride = (unsigned long long)d.N_t * d.N_theta * d.N_phi;
     count = (size_t)planes * d.plane_stride;
     dims[0] = planes; dims[1] = d.N_t; dims[2] = d.N_theta; dims[3] = d.N_phi;
+  } else if (S.kind == LMC_SENSOR_STATISTICS) {
+    d.estimator = 0;                                        // Sensor(z, absorb, false)
+    d.N_t = (S.dt <= 0.0) ? 1 : (int)std::ceil(S.len_t / S.dt) + 1;   // :1802-1817
+    if (S.dt <= 0.0)
+      d.dt = 0.0;
+    const lmc_statistics_desc &q = S.stats;
+    const size_t nt = (size_t)d.N_t;
+    size_t n = 0;
+    n += (q.set & LMC_STAT_EVENTS) ? nt * (size_t)q.n_events : 0;
+    n += (q.set & LMC_STAT_THETA) ? nt * (size_t)q.n_theta : 0;
+    n += (q.set & LMC_STAT_PHI) ? nt * (size_t)q.n_phi : 0;
+    n += (q.set & LMC_STAT_DEPTH) ? nt * (size_t)q.n_depth : 0;
+    n += (q.set & LMC_STAT_TIME) ? (size_t)q.n_time : 0;
+    n += (q.set & LMC_STAT_WEIGHT) ? (size_t)q.n_weight : 0;
+    count = n;
+    dims[0] = d.N_t; dims[1] = (int)n; dims[2] = 0; dims[3] = 0;
   } else if (S.kind == LMC_SENSOR_PLANAR_FLUENCE) {
     d.N_t = (S.dt == 0) ? 1 : (int)std::ceil(S.len_t / S.dt) + 1;
     d.N_x = (int)std::ceil(S.len_x / S.dx);
@@ -287,8 +314,43 @@ struct SceneBuild {
   bool queued = false;
   bool has_est = false;                  // an estimator-mode FarFieldCBS sensor
   size_t est_off[LMC_MAX_SENSORS] = {};  // its bin table in the arena
+  size_t stat_off[LMC_MAX_SENSORS] = {}; // StatisticsSensor histograms in the arena
   MedOff mo[LMC_MAX_MEDIA] = {};
 };
+
+// A StatisticsSensor's histogram parameters (src/detector.cpp:1836-1888: bin widths
+// (max - min) / n) and the offsets of the histograms present, in layout order.
+dev::StatHist stat_hist(const lmc_sensor_desc &S, int N_t)
+{
+  dev::StatHist h;
+  std::memset(&h, 0, sizeof(h));
+  const lmc_statistics_desc &q = S.stats;
+  h.set = q.set;
+  h.n_events = q.n_events;
+  h.n_theta = q.n_theta;
+  h.n_phi = q.n_phi;
+  h.n_depth = q.n_depth;
+  h.n_time = q.n_time;
+  h.n_weight = q.n_weight;
+  h.theta_min = q.theta_min; h.theta_max = q.theta_max;
+  h.phi_min = q.phi_min; h.phi_max = q.phi_max;
+  h.depth_max = q.depth_max;
+  h.weight_max = q.weight_max;
+  h.dtheta = (q.theta_max - q.theta_min) / q.n_theta;
+  h.dphi = (q.phi_max - q.phi_min) / q.n_phi;
+  h.ddepth = q.depth_max / q.n_depth;
+  h.dtime = q.time_max / q.n_time;
+  h.dweight = q.weight_max / q.n_weight;
+  const unsigned long long nt = (unsigned long long)N_t;
+  unsigned long long o = 0;
+  h.off[0] = o; o += (q.set & LMC_STAT_EVENTS) ? nt * q.n_events : 0;
+  h.off[1] = o; o += (q.set & LMC_STAT_THETA) ? nt * q.n_theta : 0;
+  h.off[2] = o; o += (q.set & LMC_STAT_PHI) ? nt * q.n_phi : 0;
+  h.off[3] = o; o += (q.set & LMC_STAT_DEPTH) ? nt * q.n_depth : 0;
+  h.off[4] = o; o += (q.set & LMC_STAT_TIME) ? (unsigned long long)q.n_time : 0;
+  h.off[5] = o;
+  return h;
+}
 
 // int_0^pi (|S1|^2 + |S2|^2) sin(theta) dtheta over the medium's amplitude table,
 // midpoint rule with 2048 points (src/detector.cpp:106-118); the table lookup is
@@ -487,6 +549,9 @@ void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned cha
     if (s->sensors[i].kind == LMC_SENSOR_FARFIELD_CBS)
       b.cbs_mask |= 1u << i;
   sc.cbs_mask = b.cbs_mask;
+  for (int i = 0; i < s->n_sensors; ++i)
+    if (s->sensors[i].kind == LMC_SENSOR_STATISTICS)
+      sc.stat_mask |= 1u << i;
 
   // table arena: per medium double/float theta tables, guide tables, amplitudes
   auto put = [&](const void *src, size_t bytes) -> size_t {
@@ -569,6 +634,11 @@ void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned cha
     b.est_off[i] = bins.empty() ? 0 : put(bins.data(), bins.size() * sizeof(double4));
     b.has_est = true;
   }
+  for (int i = 0; i < s->n_sensors; ++i)
+    if (s->sensors[i].kind == LMC_SENSOR_STATISTICS) {
+      const dev::StatHist hh = stat_hist(s->sensors[i], sc.sensors[i].N_t);
+      b.stat_off[i] = put(&hh, sizeof(hh));
+    }
 }
 
 // Device table pointers of a built scene, given the device copy of the arena.
@@ -586,9 +656,12 @@ void patch_tables(SceneBuild &b, unsigned char *base)
     d.amp_d = reinterpret_cast<const double4 *>(base + o.ad);
     d.amp_f = reinterpret_cast<const float4 *>(base + o.af);
   }
-  for (int i = 0; i < b.sc.n_sensors; ++i)
+  for (int i = 0; i < b.sc.n_sensors; ++i) {
     if (b.sc.sensors[i].est_n > 0)
       b.sc.sensors[i].est_bins = reinterpret_cast<const double4 *>(base + b.est_off[i]);
+    if (b.sc.sensors[i].kind == LMC_SENSOR_STATISTICS)
+      b.sc.sensors[i].stat = reinterpret_cast<const dev::StatHist *>(base + b.stat_off[i]);
+  }
 }
 
 // Device allocations shared by lmc_create and lmc_create_sweep: arena, scenes,
@@ -1387,6 +1460,8 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
       sc.need_phase = 1;
     if (S.kind == LMC_SENSOR_FARFIELD_CBS)
       cbs_mask |= 1u << i;
+    if (S.kind == LMC_SENSOR_STATISTICS)
+      sc.stat_mask |= 1u << i;
     int g = -1;
     for (int k = 0; k < n_planes; ++k)
       if (!(planes[k] < z - 1e-9) && !(z < planes[k] - 1e-9))
@@ -1440,6 +1515,14 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     p.amp_d = toff; toff = align(toff + (size_t)M.amp_n * sizeof(double4));
     p.amp_f = toff; toff = align(toff + (size_t)M.amp_n * sizeof(float4));
   }
+  dev::StatHist stat[LMC_MAX_SENSORS];                       // StatisticsSensor histograms
+  size_t stat_toff[LMC_MAX_SENSORS] = {};
+  for (int i = 0; i < s->n_sensors; ++i)
+    if (s->sensors[i].kind == LMC_SENSOR_STATISTICS) {
+      stat[i] = stat_hist(s->sensors[i], sc.sensors[i].N_t);
+      stat_toff[i] = toff;
+      toff = align(toff + sizeof(dev::StatHist));
+    }
   if (toff > kNaTablesBytes)
     return fail(LMC_ERR_INVALID, "lmc_run_noalloc: the scene's tables need " + std::to_string(toff) +
                                      " bytes of device memory; this entry point holds at most " +
@@ -1494,6 +1577,12 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     derive_tables<<<64, 256, 0, stream>>>(a);
     LMC_CUDA(cudaGetLastError());
   }
+  for (int i = 0; i < s->n_sensors; ++i)
+    if (s->sensors[i].kind == LMC_SENSOR_STATISTICS) {
+      sc.sensors[i].stat = reinterpret_cast<const dev::StatHist *>(tb + stat_toff[i]);
+      LMC_CUDA(cudaMemcpyAsync(tb + stat_toff[i], &stat[i], sizeof(dev::StatHist),
+                               cudaMemcpyHostToDevice, stream));
+    }
   dev::Scene *d_scene = reinterpret_cast<dev::Scene *>(base + kNaSceneOff);
   dev::Scratch *d_counters = reinterpret_cast<dev::Scratch *>(base + kNaCountersOff);
   LMC_CUDA(cudaMemcpyAsync(d_scene, &sc, sizeof(sc), cudaMemcpyHostToDevice, stream));

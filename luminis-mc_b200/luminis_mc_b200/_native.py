@@ -16,7 +16,9 @@ MAX_SPECIES, MAX_MIX_ENTRIES = 8, 32
 
 LMC_OK, LMC_ERR_INVALID, LMC_ERR_CUDA, LMC_ERR_NOMEM, LMC_ERR_KERNEL, LMC_ERR_UNSUPPORTED = range(6)
 THETA_TABLE, THETA_TABLE_COS, THETA_HG, THETA_UNIFORM = range(4)
-SENSOR_FARFIELD_CBS, SENSOR_PLANAR_FLUENCE, SENSOR_PLANAR_FIELD, SENSOR_FARFIELD_FLUENCE = range(4)
+(SENSOR_FARFIELD_CBS, SENSOR_PLANAR_FLUENCE, SENSOR_PLANAR_FIELD, SENSOR_FARFIELD_FLUENCE,
+ SENSOR_STATISTICS) = range(5)
+STAT_EVENTS, STAT_THETA, STAT_PHI, STAT_DEPTH, STAT_TIME, STAT_WEIGHT = 1, 2, 4, 8, 16, 32
 PDF_RAYLEIGH, PDF_RD, PDF_RDEMC, PDF_DRAINE, PDF_MIE = 1, 3, 4, 5, 6
 AMP_RGD, AMP_MIE = 0, 1
 PRECISION = {"fp32": 0, "fp64": 1}
@@ -46,6 +48,15 @@ class LaserDesc(C.Structure):
                 ("repetition_rate", C.c_double), ("time_offset", C.c_double)]
 
 
+class StatisticsDesc(C.Structure):
+    _fields_ = [("set", C.c_int), ("n_events", C.c_int),
+                ("n_theta", C.c_int), ("theta_min", C.c_double), ("theta_max", C.c_double),
+                ("n_phi", C.c_int), ("phi_min", C.c_double), ("phi_max", C.c_double),
+                ("n_depth", C.c_int), ("depth_max", C.c_double),
+                ("n_time", C.c_int), ("time_max", C.c_double),
+                ("n_weight", C.c_int), ("weight_max", C.c_double)]
+
+
 class SensorDesc(C.Structure):
     _fields_ = [("kind", C.c_int), ("z", C.c_double), ("absorb", C.c_int), ("estimator", C.c_int),
                 ("f_theta", C.c_int), ("theta_min", C.c_double), ("theta_max", C.c_double),
@@ -57,7 +68,8 @@ class SensorDesc(C.Structure):
                 ("len_x", C.c_double), ("len_y", C.c_double), ("len_t", C.c_double),
                 ("dx", C.c_double), ("dy", C.c_double), ("dt", C.c_double),
                 ("theta_max_grid", C.c_double), ("phi_max_grid", C.c_double),
-                ("dtheta", C.c_double), ("dphi", C.c_double), ("theta_pp_max", C.c_double)]
+                ("dtheta", C.c_double), ("dphi", C.c_double), ("theta_pp_max", C.c_double),
+                ("stats", StatisticsDesc)]
 
 
 class AbsorptionDesc(C.Structure):

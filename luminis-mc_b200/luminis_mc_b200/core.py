@@ -923,11 +923,114 @@ class PhotonRecordSensor(Sensor):
 
 
 class StatisticsSensor(Sensor):
-    """Histograms of detected photons; not transported on the GPU (runs raise)."""
-    _gpu = False
+    """Histograms of the photons crossing plane z (include/luminis/core/detector.hpp:595-699,
+    src/detector.cpp:1569-1888): counts by scattering events, exit theta = acos(-s_z),
+    exit phi, penetration depth, arrival time and weight.  Each histogram exists once its
+    set_*_histogram_bins was called; events, theta, phi and depth have the time axis of
+    set_time_resolution (slice 0 integrated, slices 1.. the windows of width dt)."""
+    _kind = N.SENSOR_STATISTICS
+    _NAMES = ("events", "theta", "phi", "depth", "time", "weight")
 
     def __init__(self, z, absorb=False):
         super().__init__(float(z), absorb, False)
+        self.N_t, self.dt, self.t_max = 1, 0.0, 0.0
+        for name in self._NAMES:
+            setattr(self, f"{name}_histogram_bins_set", False)
+        self.max_events = 0
+        self.min_theta = self.max_theta = self.dtheta = 0.0
+        self.n_bins_theta = 0
+        self.min_phi = self.max_phi = self.dphi = 0.0
+        self.n_bins_phi = 0
+        self.max_depth = self.ddepth = 0.0
+        self.n_bins_depth = 0
+        self.h_max_time = self.h_dtime = 0.0
+        self.n_bins_time = self._time_bins = 0
+        self.max_weight = self.dweight = 0.0
+        self.n_bins_weight = 0
+        self._tally = np.zeros(0)
+
+    # histogram sizes in layout order: (name, time slices, bins)
+    def _parts(self):
+        out = []
+        for name, n in (("events", self.max_events), ("theta", self.n_bins_theta),
+                        ("phi", self.n_bins_phi), ("depth", self.n_bins_depth)):
+            if getattr(self, f"{name}_histogram_bins_set"):
+                out.append((name, self.N_t, n))
+        if self.time_histogram_bins_set:
+            out.append(("time", 0, self._time_bins))
+        if self.weight_histogram_bins_set:
+            out.append(("weight", 0, self.n_bins_weight))
+        return out
+
+    def _reset(self):
+        self._tally = np.zeros(sum(max(t, 1) * n for _, t, n in self._parts()))
+
+    def _shape(self):
+        return (self._tally.size,)
+
+    def _hist(self, name):
+        off = 0
+        for nm, t, n in self._parts():
+            size = max(t, 1) * n
+            if nm == name:
+                a = self._tally[off:off + size]
+                return ([[int(v) for v in row] for row in a.reshape(t, n)] if t
+                        else [int(v) for v in a])
+            off += size
+        return []
+
+    events_histogram = property(lambda self: self._hist("events"))
+    theta_histogram = property(lambda self: self._hist("theta"))
+    phi_histogram = property(lambda self: self._hist("phi"))
+    depth_histogram = property(lambda self: self._hist("depth"))
+    time_histogram = property(lambda self: self._hist("time"))
+    weight_histogram = property(lambda self: self._hist("weight"))
+
+    def set_time_resolution(self, len_t, dt):                 # src/detector.cpp:1802-1834
+        self.t_max, self.dt = float(len_t), float(dt)
+        if self.dt <= 0.0:
+            self.N_t, self.dt = 1, 0.0
+        else:
+            self.N_t = int(math.ceil(self.t_max / self.dt)) + 1
+        self._reset()
+
+    def set_events_histogram_bins(self, max_events):
+        self.max_events = int(max_events)
+        self.events_histogram_bins_set = True
+        self._reset()
+
+    def set_theta_histogram_bins(self, min_theta, max_theta, n_bins):
+        self.min_theta, self.max_theta = float(min_theta), float(max_theta)
+        self.n_bins_theta = int(n_bins)
+        self.dtheta = (self.max_theta - self.min_theta) / self.n_bins_theta if n_bins else math.inf
+        self.theta_histogram_bins_set = True
+        self._reset()
+
+    def set_phi_histogram_bins(self, min_phi, max_phi, n_bins):
+        self.min_phi, self.max_phi, self.n_bins_phi = float(min_phi), float(max_phi), int(n_bins)
+        self.dphi = (self.max_phi - self.min_phi) / self.n_bins_phi if n_bins else math.inf
+        self.phi_histogram_bins_set = True
+        self._reset()
+
+    def set_depth_histogram_bins(self, max_depth, n_bins):
+        self.max_depth, self.n_bins_depth = float(max_depth), int(n_bins)
+        self.ddepth = self.max_depth / self.n_bins_depth if n_bins else math.inf
+        self.depth_histogram_bins_set = True
+        self._reset()
+
+    def set_time_histogram_bins(self, max_time, n_bins):
+        self.h_max_time = float(max_time)
+        self._time_bins = int(n_bins)
+        self.n_bins_time = max(1, int(n_bins))
+        self.h_dtime = self.h_max_time / int(n_bins) if n_bins else math.inf
+        self.time_histogram_bins_set = True
+        self._reset()
+
+    def set_weight_histogram_bins(self, max_weight, n_bins):
+        self.max_weight, self.n_bins_weight = float(max_weight), int(n_bins)
+        self.dweight = self.max_weight / self.n_bins_weight if n_bins else math.inf
+        self.weight_histogram_bins_set = True
+        self._reset()
 
 
 class SensorsGroup:

@@ -18,7 +18,8 @@ import numpy as np
 from . import _native as N
 from .core import (FarFieldCBSSensor, FarFieldFluenceSensor, HenyeyGreensteinPhaseFunction,
                    Matrix, MixtureLayer, PlanarFieldSensor, PlanarFluenceSensor,
-                   UniformPhaseFunction, _TablePhase, solid_angle_bin)  # noqa: F401
+                   StatisticsSensor, UniformPhaseFunction, _TablePhase,
+                   solid_angle_bin)  # noqa: F401
 
 
 class SimConfig:
@@ -123,6 +124,20 @@ def _sensor_desc(d: N.SensorDesc, s) -> None:
     elif isinstance(s, PlanarFluenceSensor):
         d.len_x, d.len_y, d.len_t = s.len_x, s.len_y, s.len_t
         d.dx, d.dy, d.dt = s.dx, s.dy, s.dt
+    elif isinstance(s, StatisticsSensor):
+        d.len_t, d.dt = s.t_max, s.dt
+        q = d.stats
+        bits = {"events": N.STAT_EVENTS, "theta": N.STAT_THETA, "phi": N.STAT_PHI,
+                "depth": N.STAT_DEPTH, "time": N.STAT_TIME, "weight": N.STAT_WEIGHT}
+        for name, bit in bits.items():
+            if getattr(s, f"{name}_histogram_bins_set"):
+                q.set |= bit
+        q.n_events = s.max_events
+        q.n_theta, q.theta_min, q.theta_max = s.n_bins_theta, s.min_theta, s.max_theta
+        q.n_phi, q.phi_min, q.phi_max = s.n_bins_phi, s.min_phi, s.max_phi
+        q.n_depth, q.depth_max = s.n_bins_depth, s.max_depth
+        q.n_time, q.time_max = (s._time_bins if s.time_histogram_bins_set else 0), s.h_max_time
+        q.n_weight, q.weight_max = s.n_bins_weight, s.max_weight
     else:
         d.len_x, d.len_y, d.dx, d.dy = s.len_x, s.len_y, s.dx, s.dy
 

@@ -47,15 +47,35 @@ def test_sample_validation_messages():
     assert s.is_inside(lm.Vec3(0, 0, 5.0)) and not s.is_inside(lm.Vec3(0, 0, -1e-9))
 
 
-@pytest.mark.parametrize("extra", ["photon_record", "statistics"])
-def test_unsupported_parts_raise_before_any_launch(extra):
+def test_photon_record_sensor_raises_before_any_launch():
     cfg, _, keep = W.build(lm, W.mie_cbs_small(10, 1))
-    if extra == "photon_record":
-        cfg.detector.add_detector(lm.PhotonRecordSensor(0.0))
-    elif extra == "statistics":
-        cfg.detector.add_detector(lm.StatisticsSensor(0.0))
+    cfg.detector.add_detector(lm.PhotonRecordSensor(0.0))
     with pytest.raises(NotImplementedError):
         scene_desc(cfg)
+
+
+def test_statistics_sensor_settings_and_packing():
+    """StatisticsSensor (src/detector.cpp:1802-1888): histogram sizes follow the
+    set_* calls (time-resolved ones get N_t = ceil(len_t/dt)+1 slices) and pack into
+    the C description with the set bits and bin parameters."""
+    s = lm.StatisticsSensor(0.0)
+    assert not s.absorb_photons and s._tally.size == 0
+    s.set_events_histogram_bins(50)
+    s.set_time_resolution(10.0, 2.5)
+    s.set_theta_histogram_bins(0.0, 1.0, 10)
+    s.set_time_histogram_bins(20.0, 8)
+    assert s.N_t == 5 and s._tally.size == 5 * 50 + 5 * 10 + 8
+    assert len(s.events_histogram) == 5 and len(s.events_histogram[0]) == 50
+    assert s.time_histogram == [0] * 8 and s.weight_histogram == []
+    assert s.dtheta == 0.1 and s.h_dtime == 2.5 and s.n_bins_time == 8
+    cfg, _, keep = W.build(lm, W.mie_cbs_small(10, 1))
+    h = cfg.detector.add_detector(s)
+    h.set_direction_limit(lm.CrossingDirection.Backward)
+    sc, _, sensors = scene_desc(cfg)
+    d = sc.sensors[1]
+    assert d.kind == 4 and d.stats.set == 1 | 2 | 16
+    assert (d.stats.n_events, d.stats.n_theta, d.stats.n_time) == (50, 10, 8)
+    assert (d.len_t, d.dt, d.f_dir) == (10.0, 2.5, 1)
 
 
 def test_absorption_recorder_host_api():

@@ -89,6 +89,20 @@ def test_noalloc_absorption_grid_matches_lmc_run(cuda):
         run.close()
 
 
+def test_noalloc_statistics_sensors_match_lmc_run(cuda):
+    """StatisticsSensor histograms (their bin tables sit in the array's table region),
+    queued at z = 0 and tallied in the transport kernel inside the sample."""
+    from tests.golden.make_golden import statistics_scenes
+    for spec in statistics_scenes():
+        cfg, _, keep = W.build(lm, spec)
+        run = DeviceRun(cfg)
+        for n, seed, begin in ((600, 5, 0), (500, 6, 900)):
+            got, gst = _noalloc(run, n, seed, begin, "fp64")
+            want, wst = _lmc_run(cfg, n, seed, begin, "fp64")
+            _same(got, want, gst, wst)
+        run.close()
+
+
 def test_noalloc_several_queue_batches(cuda):
     """300k photons need several batches of the fixed-size hit queue."""
     spec = W.mie_cbs_small(300_000, 5)
