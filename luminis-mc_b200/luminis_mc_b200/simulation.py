@@ -209,6 +209,13 @@ def scene_desc(config: SimConfig):
     return sc, keep, sensors
 
 
+def layout_shape(count, dims) -> tuple:
+    """Array shape of a tally-layout entry: the 4 dims, or a flat run of counts for a
+    StatisticsSensor (dims {N_t, count, 0, 0})."""
+    d = tuple(dims)
+    return (int(getattr(count, "value", count)),) if d[2] == 0 and d[3] == 0 else d
+
+
 class Transport:
     """A created scene (lmc_create) that can run many photon ranges.
 
@@ -230,7 +237,7 @@ class Transport:
             off, cnt = C.c_size_t(), C.c_size_t()
             dims = (C.c_int * 4)()
             N.check(N.lib().lmc_tally_layout(self._h, i, C.byref(off), C.byref(cnt), dims))
-            self.layout.append((int(off.value), int(cnt.value), tuple(dims)))
+            self.layout.append((int(off.value), int(cnt.value), layout_shape(cnt, dims)))
         off, cnt = C.c_size_t(), C.c_size_t()
         dims = (C.c_int * 4)()
         N.check(N.lib().lmc_tally_layout(self._h, N.TALLY_ABSORPTION, C.byref(off), C.byref(cnt),

@@ -15,7 +15,7 @@ import ctypes as C
 import numpy as np
 
 from . import _native as N
-from .simulation import SimConfig, scene_desc
+from .simulation import SimConfig, layout_shape, scene_desc
 
 
 class SweepRun:
@@ -49,7 +49,7 @@ class SweepRun:
                 off, cnt = C.c_size_t(), C.c_size_t()
                 dims = (C.c_int * 4)()
                 N.check(N.lib().lmc_sweep_layout(h, k, i, C.byref(off), C.byref(cnt), dims))
-                rows.append((int(off.value), int(cnt.value), tuple(dims)))
+                rows.append((int(off.value), int(cnt.value), layout_shape(cnt, dims)))
             self.layout.append(rows)
         self.tallies = torch.zeros(max(self.tally_size, 1), dtype=torch.float64, device=self.device)
         self.n_scenes = n
