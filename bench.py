@@ -447,11 +447,26 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
     torch.cuda.synchronize()
     graph_ms = max_ms(e0.elapsed_time(e1))
     del g
+    # the same sweep with each medium's CBS S0 grids and their derivatives with respect
+    # to its (mu_a, mu_s, mean free path, g): one launch, against one adjoint launch
+    # per medium (sum of their device times)
+    sw.run_adjoint(2029 + rank * 7919, precision="fp32", stream=stream.cuda_stream)
+    flush.zero_()
+    _, st = sw.run_adjoint(2030 + rank * 7919, precision="fp32", stream=stream.cuda_stream)
+    sweep_adj_ms = max_ms(st["kernel_ms"])
     sw.close()
+    seq_adj_ms = 0.0
+    offs = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    for c, n, o in zip(scfgs, counts, offs):
+        tr = AdjointTransport(c, device=f"cuda:{local}")
+        _, _, st = tr.run(int(n), 2030 + rank * 7919, precision="fp32", begin=int(o),
+                          stream=stream.cuda_stream)
+        seq_adj_ms += st["kernel_ms"]
+        tr.close()
+    seq_adj_ms = max_ms(seq_adj_ms)
     trs = [Transport(c) for c in scfgs]
     bufs = [torch.zeros(max(t.tally_size, 1), dtype=torch.float64, device=f"cuda:{local}")
             for t in trs]
-    offs = np.concatenate([[0], np.cumsum(counts)[:-1]])
     flush.zero_()
     torch.cuda.synchronize()
     e0.record(stream)
@@ -467,6 +482,9 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
         "value": total * world / (sweep_ms * 1e-3), "unit": "photons/s", "precision": "fp32",
         "photons": total, "media": len(counts), "graph_replay": total * world / (graph_ms * 1e-3),
         "sequential_launches": total * world / (seq_ms * 1e-3),
+        "with_gradients": total * world / (sweep_adj_ms * 1e-3),
+        "with_gradients_sequential_device_time": total * world / (seq_adj_ms * 1e-3),
+        "gradients": "CBS S0 coherent + incoherent grids and d/d(mu_a, mu_s, mfp, g) per medium",
         "workload": "256 single-layer Mie media, FarFieldCBS 100x1 each, seeded draws "
                     "(numpy default_rng(2026))"}
 

@@ -356,6 +356,23 @@ LMC_API lmc_status lmc_run_adjoint(lmc_handle *h, uint64_t seed, uint64_t photon
                                    const lmc_adjoint_opts *a, double *d_tallies, double *d_adjoint,
                                    lmc_stats *stats);
 
+/* Likelihood-ratio outputs of a sweep (lmc_create_sweep): scene s has its own block of
+ * (1 + n_params_s) rows of n_out_s doubles (layout as lmc_adjoint_layout for that scene,
+ * n_params_s = 4 x its media) at *offset in the sweep's adjoint buffer; scene = -1
+ * returns the buffer's total size in *n_out and the largest n_params.  One set of options
+ * for every scene (radial_sensor >= 0 must name a PlanarFluenceSensor in each). */
+LMC_API lmc_status lmc_sweep_adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a, int scene,
+                                            size_t *offset, size_t *n_out, int *n_params);
+
+/* lmc_run_sweep that also ADDS every scene's outputs and derivatives into its block of
+ * d_adjoint (device, size from lmc_sweep_adjoint_layout(-1)).  Scene s's block equals
+ * lmc_run_adjoint on a handle of that scene alone over photons [P_s, P_s + n_s).  The
+ * first run with a set of options uploads the per-scene layouts synchronously; later
+ * runs with the same options enqueue device work only (graph-capturable). */
+LMC_API lmc_status lmc_run_sweep_adjoint(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts,
+                                         const lmc_adjoint_opts *a, double *d_tallies,
+                                         double *d_adjoint, lmc_stats *stats);
+
 /* Backward pass: d_grad_params[k] = sum_j d_adjoint[(1 + k) n_out + j] * d_grad_out[j]
  * (all device pointers; enqueued on `stream`, NULL = legacy default stream). */
 LMC_API lmc_status lmc_adjoint_contract(const double *d_adjoint, const double *d_grad_out,

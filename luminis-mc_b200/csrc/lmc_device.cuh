@@ -153,6 +153,15 @@ enum ErrorFlag : unsigned int {
   kErrQueueOverflow = 1u << 2,     // more hits than the queue holds (tallies incomplete)
 };
 
+// Likelihood-ratio output layout of one scene of a sweep: its block of (1 + K) rows of
+// n_out doubles starts at out_off in RunParams::adj_out.
+struct AdjScene {
+  unsigned long long out_off, n_out;
+  int K, radial_sensor, radial_bins, pad;
+  double radial_max;
+  unsigned long long cbs_off[LMC_MAX_SENSORS];
+};
+
 struct RunParams {
   unsigned long long photon_begin, n_photons;
   uint32_t key0, key1;
@@ -176,6 +185,8 @@ struct RunParams {
   // hit counts per scene and sensor in sweep_hits[s * LMC_MAX_SENSORS + sensor]
   const unsigned long long *sweep_prefix;
   unsigned long long *sweep_hits;
+  // sweep with likelihood-ratio outputs: per-scene layouts (adj_K above is the largest K)
+  const AdjScene *adj_scenes;
 };
 
 }  // namespace dev

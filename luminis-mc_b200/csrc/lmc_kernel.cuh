@@ -746,25 +746,51 @@ __device__ __forceinline__ double hit_launch_time(const Scene &sc, const RunPara
   return emission_time<R>(sc.laser, rp, ((unsigned long long)h.p_hi << 32) | h.p_lo);
 }
 
+// The likelihood-ratio output layout a hit contributes to: the run's (one scene), or
+// its scene's block of a sweep.
+struct AdjView {
+  double *out;                 // row 0 of the block; row 1 + k at out + (1 + k) n_out
+  unsigned long long n_out;
+  int K, radial_sensor, radial_bins;
+  double radial_max;
+  const unsigned long long *cbs_off;
+};
+
+template <bool kSweep>
+__device__ __forceinline__ AdjView adj_view(const RunParams &rp, unsigned scene)
+{
+  if (kSweep) {
+    const AdjScene &a = rp.adj_scenes[scene];
+    return {rp.adj_out + a.out_off, a.n_out, a.K, a.radial_sensor, a.radial_bins, a.radial_max,
+            a.cbs_off};
+  }
+  return {rp.adj_out, rp.adj_n_out, rp.adj_K, rp.adj_radial_sensor, rp.adj_radial_bins,
+          rp.adj_radial_max, rp.adj_cbs_off};
+}
+
 // Likelihood-ratio outputs of one hit contribution v: row 0 += v, row 1 + k +=
-// v * score_k.  Global atomics (FarFieldCBS bins), or the block's shared-memory copy
-// of the radial outputs (rows of adj_radial_bins + 1 doubles).
+// v * score_k.  Global atomics (FarFieldCBS bins; the radial outputs of a sweep), or
+// the block's shared-memory copy of the radial outputs (rows of radial_bins + 1).
 template <typename R>
-__device__ __forceinline__ void adj_add_global(const RunParams &rp, unsigned long long idx, double v,
+__device__ __forceinline__ void adj_add_global(const AdjView &A, unsigned long long idx, double v,
                                                const R *hs)
 {
-  atomicAdd(rp.adj_out + idx, v);
-  for (int k = 0; k < rp.adj_K; ++k)
-    atomicAdd(rp.adj_out + (unsigned long long)(1 + k) * rp.adj_n_out + idx, v * (double)hs[k]);
+  atomicAdd(A.out + idx, v);
+  for (int k = 0; k < A.K; ++k)
+    atomicAdd(A.out + (unsigned long long)(1 + k) * A.n_out + idx, v * (double)hs[k]);
 }
 
 template <typename R>
-__device__ __forceinline__ void adj_add_shared(const RunParams &rp, double *s_rad, int idx, double v,
+__device__ __forceinline__ void adj_add_radial(const AdjView &A, double *s_rad, int idx, double v,
                                                const R *hs)
 {
-  const int row = rp.adj_radial_bins + 1;
+  if (!s_rad) {
+    adj_add_global<R>(A, (unsigned long long)idx, v, hs);
+    return;
+  }
+  const int row = A.radial_bins + 1;
   atomicAdd(s_rad + idx, v);
-  for (int k = 0; k < rp.adj_K; ++k)
+  for (int k = 0; k < A.K; ++k)
     atomicAdd(s_rad + (1 + k) * row + idx, v * (double)hs[k]);
 }
 
@@ -773,7 +799,7 @@ __device__ __forceinline__ void adj_add_shared(const RunParams &rp, double *s_ra
 // and E_r alike and cancels in every Stokes parameter, so it is not formed.
 template <typename R, bool kAdj>
 __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor &s,
-                             const HitData<R> &h, lmc_record *rec, int si, const R *hs)
+                             const HitData<R> &h, lmc_record *rec, int si, const R *hs, const AdjView *A)
 {
   const double t_launch = (s.dt > 0) ? hit_launch_time<R>(sc, rp, h) : 0.0;
   const int t_idx = time_bin(s, t_launch + h.opath);
@@ -845,12 +871,12 @@ __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor 
     add4(base + 4 * P, P, t_idx * tstride + cell, i0, i1, i2, i3);
   }
   if (kAdj && s.kind == LMC_SENSOR_FARFIELD_CBS) {     // S0 coherent, S0 incoherent
-    const unsigned long long o = rp.adj_cbs_off[si];
-    adj_add_global<R>(rp, o + cell, c0, hs);
-    adj_add_global<R>(rp, o + P + cell, i0, hs);
+    const unsigned long long o = A->cbs_off[si];
+    adj_add_global<R>(*A, o + cell, c0, hs);
+    adj_add_global<R>(*A, o + P + cell, i0, hs);
     if (t_idx >= 1) {
-      adj_add_global<R>(rp, o + t_idx * tstride + cell, c0, hs);
-      adj_add_global<R>(rp, o + P + t_idx * tstride + cell, i0, hs);
+      adj_add_global<R>(*A, o + t_idx * tstride + cell, c0, hs);
+      adj_add_global<R>(*A, o + P + t_idx * tstride + cell, i0, hs);
     }
   }
   return true;
@@ -860,7 +886,7 @@ __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor 
 // with E_x negated; exp(i k L) cancels and is not formed.
 template <typename R, bool kAdj>
 __device__ bool hit_fluence(const Scene &sc, const RunParams &rp, const Sensor &s, const HitData<R> &h,
-                            int si, const R *hs, double *s_rad)
+                            int si, const R *hs, double *s_rad, const AdjView *A)
 {
   int t_idx = -1;
   if (s.dt > 0) {
@@ -888,13 +914,13 @@ __device__ bool hit_fluence(const Scene &sc, const RunParams &rp, const Sensor &
   if (s.dt > 0)
     add4(base, s.plane_stride, t_idx * tstride + cell, q0, q1, q2, q3);
   add4(base, s.plane_stride, cell, q0, q1, q2, q3);
-  if (kAdj && si == rp.adj_radial_sensor) {            // total S0 and its radial profile
-    adj_add_shared<R>(rp, s_rad, 0, q0, hs);
+  if (kAdj && si == A->radial_sensor) {                // total S0 and its radial profile
+    adj_add_radial<R>(*A, s_rad, 0, q0, hs);
     const double r = sqrt((double)h.hx * (double)h.hx + (double)h.hy * (double)h.hy);
-    if (r < rp.adj_radial_max) {
-      const int ir = (int)(r / (rp.adj_radial_max / rp.adj_radial_bins));
-      if (ir >= 0 && ir < rp.adj_radial_bins)
-        adj_add_shared<R>(rp, s_rad, 1 + ir, q0, hs);
+    if (r < A->radial_max) {
+      const int ir = (int)(r / (A->radial_max / A->radial_bins));
+      if (ir >= 0 && ir < A->radial_bins)
+        adj_add_radial<R>(*A, s_rad, 1 + ir, q0, hs);
     }
   }
   return true;
@@ -988,7 +1014,8 @@ __device__ __noinline__ void hit_statistics(const Sensor &s, double *tallies, do
 // insertion order, as SensorsGroup::record_hit calls them (src/detector.cpp:244-265).
 template <typename R, bool kAdj>
 __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData<R> &h,
-                             unsigned mask, unsigned long long *hits, const R *hs, double *s_rad)
+                             unsigned mask, unsigned long long *hits, const R *hs, double *s_rad,
+                             const AdjView *A)
 {
   lmc_record *rec = rp.records ? rp.records + ((((unsigned long long)h.p_hi << 32) | h.p_lo) -
                                                rp.photon_begin)
@@ -999,7 +1026,7 @@ __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData
     const Sensor &s = sc.sensors[si];
     bool counted;
     if (s.kind == LMC_SENSOR_PLANAR_FLUENCE)
-      counted = hit_fluence<R, kAdj>(sc, rp, s, h, si, hs, s_rad);
+      counted = hit_fluence<R, kAdj>(sc, rp, s, h, si, hs, s_rad, A);
     else if (s.kind == LMC_SENSOR_PLANAR_FIELD)
       counted = hit_field<R>(sc, rp, s, h);
     else if (s.kind == LMC_SENSOR_STATISTICS) {
@@ -1010,7 +1037,7 @@ __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData
       counted = true;
     }
     else
-      counted = hit_farfield<R, kAdj>(sc, rp, s, h, rec, si, hs);
+      counted = hit_farfield<R, kAdj>(sc, rp, s, h, rec, si, hs, A);
     if (counted) {
       atomicAdd(hits + si, 1ull);
       if (rec) {
@@ -1489,7 +1516,7 @@ __device__ __forceinline__ bool record_hit(const Scene &sc, const RunParams &rp,
       } else {
         HitData<R> h;
         fill_hit<R>(ph, side, hx, hy, hz, opath, h);
-        process_hits<R, false>(sc, rp, h, mask, s_hits, nullptr, nullptr);
+        process_hits<R, false>(sc, rp, h, mask, s_hits, nullptr, nullptr, nullptr);
       }
     }
   }
@@ -1974,7 +2001,9 @@ __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__
   __shared__ unsigned long long s_hits[LMC_MAX_SENSORS];
   extern __shared__ __align__(16) unsigned char s_dyn[];
   double *s_rad = reinterpret_cast<double *>(s_dyn);
-  const int rad_n = (kAdj && rp.adj_radial_sensor >= 0) ? (1 + rp.adj_K) * (rp.adj_radial_bins + 1) : 0;
+  // radial outputs in shared memory (one scene per launch); a sweep adds them globally
+  const int rad_n = (kAdj && !kSweep && rp.adj_radial_sensor >= 0)
+                        ? (1 + rp.adj_K) * (rp.adj_radial_bins + 1) : 0;
   if (!kSweep)
     load_scene(s_raw, g_scene);
   if (threadIdx.x < LMC_MAX_SENSORS)
@@ -2027,12 +2056,15 @@ __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__
         h.T[qd] = {r[(kQT + 2 * qd) * C + i], r[(kQT + 2 * qd + 1) * C + i]};
     }
     R hs[kAdj ? kAdjMaxK : 1];
-    if (kAdj)
-      for (int k = 0; k < rp.adj_K; ++k)
+    AdjView A;
+    if (kAdj) {
+      A = adj_view<kSweep>(rp, scene);
+      for (int k = 0; k < A.K; ++k)
         hs[k] = r[(kQScore + k) * C + i];
+    }
     process_hits<R, kAdj>(sc, rp, h, mask,
                           kSweep ? rp.sweep_hits + (unsigned long long)scene * LMC_MAX_SENSORS : s_hits,
-                          hs, s_rad);
+                          hs, rad_n ? s_rad : nullptr, kAdj ? &A : nullptr);
   }
   __syncthreads();
   if (threadIdx.x < LMC_MAX_SENSORS && s_hits[threadIdx.x])

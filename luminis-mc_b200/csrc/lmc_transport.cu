@@ -84,6 +84,9 @@ struct lmc_handle {
   unsigned long long *d_prefix = nullptr;      // n_scenes + 1 photon offsets
   unsigned long long *d_sweep_hits = nullptr;  // n_scenes x LMC_MAX_SENSORS, last run
   unsigned long long total_photons = 0;        // photons of one sweep run
+  std::vector<lmc::dev::AdjScene> adj_scenes;  // sweep likelihood-ratio layouts (last run)
+  void *d_adj_scenes = nullptr;
+  size_t adj_scenes_bytes = 0;
 };
 
 namespace lmc {
@@ -761,6 +764,7 @@ void lmc_destroy(lmc_handle *h)
   cudaFree(h->d_queue);
   cudaFree(h->d_prefix);
   cudaFree(h->d_sweep_hits);
+  cudaFree(h->d_adj_scenes);
   for (cudaEvent_t e : h->kev)
     cudaEventDestroy(e);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -796,29 +800,25 @@ lmc_status lmc_tally_layout(const lmc_handle *h, int sensor, size_t *offset, siz
   return LMC_OK;
 }
 
-// Layout of the likelihood-ratio outputs of a handle (lmc_adjoint_layout).
-static lmc_status adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a, size_t *n_out,
-                                 unsigned long long cbs_off[LMC_MAX_SENSORS])
+// Layout of the likelihood-ratio outputs of one scene (lmc_adjoint_layout, and each
+// scene of lmc_sweep_adjoint_layout).
+static lmc_status scene_adjoint_layout(const lmc::dev::Scene &sc, const lmc_adjoint_opts *a,
+                                       size_t *n_out, unsigned long long cbs_off[LMC_MAX_SENSORS])
 {
   using namespace lmc;
-  if (!h || !a)
-    return fail(LMC_ERR_INVALID, "handle and adjoint options must not be null");
-  if (!h->queued)
-    return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs need every sensor plane at z <= 0");
-  if (h->scene.n_media > dev::kAdjMaxMedia)
+  if (sc.n_media > dev::kAdjMaxMedia)
     return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs support at most 4 media");
-  for (int l = 0; l < h->scene.n_layers; ++l)
-    if (h->scene.layers[l].n_species > 0)
+  for (int l = 0; l < sc.n_layers; ++l)
+    if (sc.layers[l].n_species > 0)
       return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs model HomogeneousLayers only");
-  for (int i = 0; i < h->scene.n_media; ++i) {
-    const dev::Medium &m = h->scene.media[i];
+  for (int i = 0; i < sc.n_media; ++i) {
+    const dev::Medium &m = sc.media[i];
     if (!(m.mu_t > 0) || !(m.mu_s > 0))
       return fail(LMC_ERR_INVALID, "likelihood-ratio outputs need mu_s > 0 in every medium");
   }
   size_t n = 0;
   if (a->radial_sensor >= 0) {
-    if (a->radial_sensor >= h->scene.n_sensors ||
-        h->scene.sensors[a->radial_sensor].kind != LMC_SENSOR_PLANAR_FLUENCE)
+    if (a->radial_sensor >= sc.n_sensors || sc.sensors[a->radial_sensor].kind != LMC_SENSOR_PLANAR_FLUENCE)
       return fail(LMC_ERR_INVALID, "radial_sensor must be a PlanarFluenceSensor");
     if (a->radial_bins < 1 || a->radial_bins > dev::kAdjMaxRadialBins || !(a->radial_max > 0))
       return fail(LMC_ERR_INVALID, "radial_bins must be in [1, 512] and radial_max > 0");
@@ -826,8 +826,8 @@ static lmc_status adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a,
   }
   for (int i = 0; i < LMC_MAX_SENSORS; ++i)
     cbs_off[i] = 0;
-  for (int i = 0; i < h->scene.n_sensors; ++i) {
-    const dev::Sensor &s = h->scene.sensors[i];
+  for (int i = 0; i < sc.n_sensors; ++i) {
+    const dev::Sensor &s = sc.sensors[i];
     if (s.kind != LMC_SENSOR_FARFIELD_CBS)
       continue;
     cbs_off[i] = n;
@@ -836,6 +836,53 @@ static lmc_status adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a,
   if (n == 0)
     return fail(LMC_ERR_INVALID, "no likelihood-ratio outputs: no radial sensor and no FarFieldCBSSensor");
   *n_out = n;
+  return LMC_OK;
+}
+
+// Layout of the likelihood-ratio outputs of a handle (lmc_adjoint_layout).
+static lmc_status adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a, size_t *n_out,
+                                 unsigned long long cbs_off[LMC_MAX_SENSORS])
+{
+  using namespace lmc;
+  if (!h || !a)
+    return fail(LMC_ERR_INVALID, "handle and adjoint options must not be null");
+  if (h->sweep)
+    return fail(LMC_ERR_INVALID, "a sweep handle lays its outputs out with lmc_sweep_adjoint_layout");
+  if (!h->queued)
+    return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs need every sensor plane at z <= 0");
+  return scene_adjoint_layout(h->scene, a, n_out, cbs_off);
+}
+
+// Per-scene blocks of a sweep's likelihood-ratio outputs, one after another; the
+// total size (doubles) and the largest parameter count.
+static lmc_status sweep_adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a,
+                                       std::vector<lmc::dev::AdjScene> &out, size_t *total, int *max_K)
+{
+  using namespace lmc;
+  if (!h || !a)
+    return fail(LMC_ERR_INVALID, "handle and adjoint options must not be null");
+  if (!h->sweep)
+    return fail(LMC_ERR_INVALID, "not a sweep handle");
+  out.assign(h->n_scenes, dev::AdjScene{});
+  size_t off = 0;
+  int kmax = 0;
+  for (int k = 0; k < h->n_scenes; ++k) {
+    dev::AdjScene &A = out[k];
+    size_t n = 0;
+    const lmc_status st = scene_adjoint_layout(h->scenes[k], a, &n, A.cbs_off);
+    if (st != LMC_OK)
+      return fail(st, "scene " + std::to_string(k) + ": " + last_error());
+    A.out_off = off;
+    A.n_out = n;
+    A.K = 4 * h->scenes[k].n_media;
+    A.radial_sensor = a->radial_sensor;
+    A.radial_bins = a->radial_bins;
+    A.radial_max = a->radial_max;
+    off += (size_t)(1 + A.K) * n;
+    kmax = std::max(kmax, A.K);
+  }
+  *total = off;
+  *max_K = kmax;
   return LMC_OK;
 }
 
@@ -855,8 +902,6 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     return fail(LMC_ERR_INVALID, "max_events must be non-negative");
   const bool sw = h->sweep;
   const bool est = h->has_est;
-  if (sw && adj)
-    return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio outputs are not available for sweeps");
   if (est && (adj || !h->queued))
     return fail(LMC_ERR_UNSUPPORTED, "estimator-mode FarFieldCBS runs need every sensor plane at "
                                      "z <= 0 and no likelihood-ratio outputs");
@@ -898,7 +943,39 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   const size_t rbytes = fp32 ? sizeof(float) : sizeof(double);
   size_t dyn_transport = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
   size_t dyn_tally = 0;
-  if (adj) {
+  if (adj && sw) {
+    size_t total = 0;
+    int kmax = 0;
+    std::vector<dev::AdjScene> lay;
+    const lmc_status ls = sweep_adjoint_layout(h, adj, lay, &total, &kmax);
+    if (ls != LMC_OK)
+      return ls;
+    if (!d_adj)
+      return fail(LMC_ERR_INVALID, "device adjoint buffer must not be null");
+    // upload the layouts only when they change (synchronously), so that a run with
+    // the layouts of the previous one enqueues device work only and can be captured
+    const size_t bytes = sizeof(dev::AdjScene) * lay.size();
+    if (!h->d_adj_scenes || h->adj_scenes.size() != lay.size() ||
+        std::memcmp(h->adj_scenes.data(), lay.data(), bytes) != 0) {
+      if (h->adj_scenes_bytes < bytes) {
+        cudaFree(h->d_adj_scenes);
+        h->d_adj_scenes = nullptr;
+        h->adj_scenes_bytes = 0;
+        const cudaError_t e = cudaMalloc(&h->d_adj_scenes, bytes);
+        if (e != cudaSuccess)
+          return fail(LMC_ERR_NOMEM, std::string("sweep adjoint layout: ") + cudaGetErrorString(e));
+        h->adj_scenes_bytes = bytes;
+      }
+      LMC_CUDA(cudaMemcpy(h->d_adj_scenes, lay.data(), bytes, cudaMemcpyHostToDevice));
+      h->adj_scenes = lay;
+    }
+    rp.adj_scenes = static_cast<const dev::AdjScene *>(h->d_adj_scenes);
+    rp.adj_out = d_adj;
+    rp.adj_n_out = total;
+    rp.adj_K = kmax;
+    rp.adj_radial_sensor = -1;           // per scene in adj_scenes, added globally
+    dyn_transport += (size_t)rp.adj_K * dev::kBlock * rbytes;
+  } else if (adj) {
     size_t n_out = 0;
     const lmc_status ls = adjoint_layout(h, adj, &n_out, rp.adj_cbs_off);
     if (ls != LMC_OK)
@@ -921,6 +998,8 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   const void *tk =
       est ? (fp32 ? (const void *)dev::transport_kernel<float, true, 2, false, false, true>
                   : (const void *)dev::transport_kernel<double, true, 1, false, false, true>)
+      : (sw && adj) ? (fp32 ? (const void *)dev::transport_kernel<float, true, 2, true, true>
+                            : (const void *)dev::transport_kernel<double, true, 1, true, true>)
       : sw ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, false, true>
                  : (const void *)dev::transport_kernel<double, true, 2, false, true>)
       : adj ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, true>
@@ -931,7 +1010,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
                  : (h->queued ? (const void *)dev::transport_kernel<double, true, 2>
                               : (const void *)dev::transport_kernel<double, false, 1>);
   LMC_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_transport));
-  if (adj) {
+  if (adj && !sw) {
     const void *tl = fp32 ? (const void *)dev::tally_kernel<float, true>
                           : (const void *)dev::tally_kernel<double, true>;
     LMC_CUDA(cudaFuncSetAttribute(tl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_tally));
@@ -996,6 +1075,11 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
         dev::transport_kernel<float, true, 2, false, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
       else
         dev::transport_kernel<double, true, 1, false, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
+    } else if (sw && adj) {
+      if (fp32)
+        dev::transport_kernel<float, true, 2, true, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
+      else
+        dev::transport_kernel<double, true, 1, true, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
     } else if (sw) {
       if (fp32)
         dev::transport_kernel<float, true, 3, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
@@ -1026,7 +1110,12 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
       const int tgrid = (int)std::max<unsigned long long>(
           1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * 8,
                                              (rp.queue.cap + dev::kBlock - 1) / dev::kBlock));
-      if (sw) {
+      if (sw && adj) {
+        if (fp32)
+          dev::tally_kernel<float, true, true><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
+        else
+          dev::tally_kernel<double, true, true><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
+      } else if (sw) {
         if (fp32)
           dev::tally_kernel<float, false, true><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
         else
@@ -1220,6 +1309,41 @@ lmc_status lmc_run_sweep(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts,
   if (!h || !h->sweep)
     return lmc::fail(LMC_ERR_INVALID, "not a sweep handle");
   return run_impl(h, seed, 0, h->total_photons, opts, nullptr, nullptr, d_tallies, stats);
+}
+
+lmc_status lmc_sweep_adjoint_layout(const lmc_handle *h, const lmc_adjoint_opts *a, int scene,
+                                    size_t *offset, size_t *n_out, int *n_params)
+{
+  using namespace lmc;
+  std::vector<dev::AdjScene> lay;
+  size_t total = 0;
+  int kmax = 0;
+  const lmc_status st = sweep_adjoint_layout(h, a, lay, &total, &kmax);
+  if (st != LMC_OK)
+    return st;
+  if (scene == -1) {
+    if (offset) *offset = 0;
+    if (n_out) *n_out = total;
+    if (n_params) *n_params = kmax;
+    return LMC_OK;
+  }
+  if (scene < 0 || scene >= h->n_scenes)
+    return fail(LMC_ERR_INVALID, "scene out of range");
+  if (offset) *offset = lay[scene].out_off;
+  if (n_out) *n_out = lay[scene].n_out;
+  if (n_params) *n_params = lay[scene].K;
+  return LMC_OK;
+}
+
+lmc_status lmc_run_sweep_adjoint(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts,
+                                 const lmc_adjoint_opts *a, double *d_tallies, double *d_adjoint,
+                                 lmc_stats *stats)
+{
+  if (!h || !h->sweep)
+    return lmc::fail(LMC_ERR_INVALID, "not a sweep handle");
+  if (!a)
+    return lmc::fail(LMC_ERR_INVALID, "adjoint options must not be null");
+  return run_impl(h, seed, 0, h->total_photons, opts, a, d_adjoint, d_tallies, stats);
 }
 
 lmc_status lmc_sweep_hits(lmc_handle *h, uint64_t *hits)

@@ -138,7 +138,7 @@ EXPORTED = ["lmc_create", "lmc_destroy", "lmc_tally_layout", "lmc_run", "lmc_run
             "lmc_amplitude_table", "lmc_probe_fp32_peak", "lmc_run_noalloc",
             "lmc_adjoint_layout", "lmc_run_adjoint", "lmc_adjoint_contract",
             "lmc_create_sweep", "lmc_sweep_layout", "lmc_sweep_set_photons", "lmc_run_sweep",
-            "lmc_sweep_hits"]
+            "lmc_sweep_hits", "lmc_sweep_adjoint_layout", "lmc_run_sweep_adjoint"]
 
 _lib = None
 
@@ -205,6 +205,13 @@ def lib():
     L.lmc_sweep_set_photons.restype = C.c_int
     L.lmc_run_sweep.argtypes = [vp, C.c_uint64, C.POINTER(RunOpts), vp, C.POINTER(Stats)]
     L.lmc_run_sweep.restype = C.c_int
+    L.lmc_sweep_adjoint_layout.argtypes = [vp, C.POINTER(AdjointOpts), C.c_int,
+                                           C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                           C.POINTER(C.c_int)]
+    L.lmc_sweep_adjoint_layout.restype = C.c_int
+    L.lmc_run_sweep_adjoint.argtypes = [vp, C.c_uint64, C.POINTER(RunOpts), C.POINTER(AdjointOpts),
+                                        vp, vp, C.POINTER(Stats)]
+    L.lmc_run_sweep_adjoint.restype = C.c_int
     L.lmc_sweep_hits.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.lmc_sweep_hits.restype = C.c_int
     _lib = L

@@ -86,6 +86,45 @@ class SweepRun:
                                       C.byref(st) if want_stats else None))
         return st.as_dict() if want_stats else {}
 
+    def adjoint_layout(self, radial_sensor: int = -1, radial_bins: int = 100,
+                       radial_max: float = 5.0):
+        """Options and per-scene blocks [(offset, n_out, n_params)] of the likelihood-ratio
+        outputs (lmc_sweep_adjoint_layout), and the buffer's total size."""
+        a = N.AdjointOpts(int(radial_sensor), int(radial_bins), float(radial_max))
+        off, n, k = C.c_size_t(), C.c_size_t(), C.c_int()
+        N.check(N.lib().lmc_sweep_adjoint_layout(self._h, C.byref(a), -1, C.byref(off),
+                                                 C.byref(n), C.byref(k)))
+        total = int(n.value)
+        blocks = []
+        for s in range(self.n_scenes):
+            N.check(N.lib().lmc_sweep_adjoint_layout(self._h, C.byref(a), s, C.byref(off),
+                                                     C.byref(n), C.byref(k)))
+            blocks.append((int(off.value), int(n.value), int(k.value)))
+        return a, blocks, total
+
+    def run_adjoint(self, seed: int, precision: str = "fp32", adjoint=None, stream=None,
+                    want_stats: bool = True, **layout):
+        """Transport every scene's photons with likelihood-ratio outputs: adds the tallies
+        into self.tallies and returns (per scene (outputs [n_out], jacobian [n_params, n_out])
+        as sums over its photons, stats).  `adjoint`: a device buffer to add into instead."""
+        if self.photons is None:
+            raise ValueError("set_photons() first")
+        torch = self.torch
+        a, blocks, total = self.adjoint_layout(**layout)
+        buf = adjoint if adjoint is not None else torch.zeros(max(total, 1), dtype=torch.float64,
+                                                              device=self.device)
+        o = self.opts(precision, stream)
+        st = N.Stats()
+        N.check(N.lib().lmc_run_sweep_adjoint(self._h, int(seed) & (2 ** 64 - 1), C.byref(o),
+                                              C.byref(a), C.c_void_p(self.tallies.data_ptr()),
+                                              C.c_void_p(buf.data_ptr()),
+                                              C.byref(st) if want_stats else None))
+        out = []
+        for off, n, k in blocks:
+            blk = buf[off:off + (1 + k) * n].view(1 + k, n)
+            out.append((blk[0], blk[1:]))
+        return out, (st.as_dict() if want_stats else {})
+
     def capture(self, seed: int, precision: str = "fp32"):
         """A CUDA graph of one run (after one uncaptured run of the same size has grown
         the hit queue): replay() adds another run's tallies."""

@@ -82,3 +82,63 @@ def test_sweep_rejects_planes_inside_the_sample(cuda):
     spec["sensors"][1]["z"] = 0.25
     with pytest.raises(NotImplementedError):
         SweepRun([W.build(lm, s)[0] for s in (_specs()[0], spec)])
+
+
+def _lone_adjoint(spec, n, seed, begin, precision, **radial):
+    from luminis_mc_b200.adjoint import AdjointTransport
+    cfg, _, keep = W.build(lm, spec)
+    tr = AdjointTransport(cfg, **radial)
+    out, jac, _ = tr.run(n, seed, precision=precision, begin=begin)
+    tr.close()
+    return out.cpu().numpy() * n, jac.cpu().numpy() * n      # sums over the photons
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_sweep_adjoint_equals_lone_adjoint_runs(precision, cuda):
+    """Each scene's block of lmc_run_sweep_adjoint (its CBS S0 grids and their
+    derivatives with respect to its medium's mu_a, mu_s, mfp, g) equals
+    lmc_run_adjoint on that scene alone over its photon range."""
+    specs = [W.mie_sweep(i, seed=7) for i in (0, 5, 17, 200)]
+    counts = [3000, 1200, 2200, 900]
+    sw = SweepRun([W.build(lm, s)[0] for s in specs])
+    sw.set_photons(counts)
+    blocks, st = sw.run_adjoint(13, precision=precision)
+    assert st["error_flags"] == 0
+    tol = RTOL if precision == "fp64" else FP32_TOL
+    for k, (spec, n, p0) in enumerate(zip(specs, counts, sw.offsets())):
+        out, jac = blocks[k]
+        want_out, want_jac = _lone_adjoint(spec, n, 13, int(p0), precision)
+        assert jac.shape == want_jac.shape == (4, want_out.size)
+        np.testing.assert_allclose(out.cpu().numpy(), want_out, rtol=tol,
+                                   atol=tol * np.abs(want_out).max())
+        for r in range(4):
+            np.testing.assert_allclose(jac[r].cpu().numpy(), want_jac[r], rtol=tol,
+                                       atol=tol * max(np.abs(want_jac[r]).max(), 1e-300))
+    sw.close()
+
+
+def test_sweep_adjoint_radial_outputs_and_media_counts(cuda):
+    """Scenes with different media counts (K = 4 and 8) and the radial reflectance
+    profile of a PlanarFluenceSensor, added globally in a sweep."""
+    from tests.test_oracle_adjoint import adjoint_scene
+    a = adjoint_scene()
+    b = W.bilayer_hg(0, 5)
+    b["sensors"][1].update(len_x=4.0, len_y=4.0, dx=0.25, dy=0.25, len_t=0.0, d_t=0.0)
+    b["sensors"].pop(2)
+    c = W.mie_cbs_small(0, 5)
+    c["sensors"].append({"kind": "planar_fluence", "z": 0.0, "len_x": 4.0, "len_y": 4.0,
+                         "len_t": 0.0, "dx": 0.5, "dy": 0.5, "d_t": 0.0, "absorb": True})
+    specs, counts = [a, b, c], [1500, 1000, 1200]
+    radial = dict(radial_sensor=1, radial_bins=10, radial_max=5.0)
+    sw = SweepRun([W.build(lm, s)[0] for s in specs])
+    sw.set_photons(counts)
+    blocks, st = sw.run_adjoint(3, precision="fp64", **radial)
+    for k, (spec, n, p0) in enumerate(zip(specs, counts, sw.offsets())):
+        out, jac = blocks[k]
+        want_out, want_jac = _lone_adjoint(spec, n, 3, int(p0), "fp64", **radial)
+        assert jac.shape[0] == 4 * len(spec["media"])
+        np.testing.assert_allclose(out.cpu().numpy(), want_out, rtol=RTOL,
+                                   atol=RTOL * np.abs(want_out).max())
+        np.testing.assert_allclose(jac.cpu().numpy(), want_jac, rtol=RTOL,
+                                   atol=RTOL * np.abs(want_jac).max())
+    sw.close()
