@@ -434,6 +434,7 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
     sw = SweepRun(scfgs, device=f"cuda:{local}")
     sw.set_photons(counts)
     total = int(counts.sum())
+    tuned = sw.autotune(2025 + rank * 7919, precision="fp32", sample_photons=20_000_000)
     sw.run(2026 + rank * 7919, precision="fp32", stream=stream.cuda_stream)   # grows the queue
     flush.zero_()
     st = sw.run(2027 + rank * 7919, precision="fp32", stream=stream.cuda_stream)
@@ -485,6 +486,9 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
         "with_gradients": total * world / (sweep_adj_ms * 1e-3),
         "with_gradients_sequential_device_time": total * world / (seq_adj_ms * 1e-3),
         "gradients": "CBS S0 coherent + incoherent grids and d/d(mu_a, mu_s, mfp, g) per medium",
+        "launch_shape": {"picked_by": "lmc_autotune on a 2e7-photon scaled copy of the sweep",
+                         **{k: tuned[k] for k in ("block_size", "blocks_per_sm", "batch_photons",
+                                                  "n_tried")}},
         "workload": "256 single-layer Mie media, FarFieldCBS 100x1 each, seeded draws "
                     "(numpy default_rng(2026))"}
 

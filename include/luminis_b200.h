@@ -324,6 +324,25 @@ LMC_API lmc_status lmc_sweep_set_photons(lmc_handle *h, const uint64_t *n_photon
 LMC_API lmc_status lmc_run_sweep(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts,
                                  double *d_tallies, lmc_stats *stats);
 
+/* Launch shape picked by lmc_autotune. */
+typedef struct lmc_tune_result {
+  int block_size;               /* threads per block                                   */
+  int blocks_per_sm;            /* 0: as many as fit                                   */
+  uint64_t batch_photons;       /* photons per hit-queue batch                         */
+  double photons_per_s;         /* the shape's rate on the sample (device time)        */
+  uint64_t sample_photons;      /* photons of the sample                               */
+  int n_tried, pad;
+} lmc_tune_result;
+
+/* Times candidate launch shapes -- threads per block (256, 128), resident blocks per SM
+ * (as many as fit, 2, 1: the persistent grid, hence photons per thread) and photons per
+ * hit-queue batch (8 Mi, 2 Mi) -- on a sample of about sample_photons photons (a
+ * sweep: every scene's count scaled down, restored afterwards) with the rest of `opts`,
+ * and returns the fastest; copy its fields into lmc_run_opts for the real runs.  Runs
+ * into a scratch tally buffer (allocates it); synchronous. */
+LMC_API lmc_status lmc_autotune(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts,
+                                uint64_t sample_photons, lmc_tune_result *out);
+
 /* Sensor hit counts of the last lmc_run_sweep, [n_scenes][LMC_MAX_SENSORS] (synchronises). */
 LMC_API lmc_status lmc_sweep_hits(lmc_handle *h, uint64_t *hits);
 

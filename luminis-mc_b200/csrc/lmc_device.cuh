@@ -31,11 +31,14 @@ struct Medium {
 // sample_free_path): its medium's for a HomogeneousLayer, the MixtureLayer aggregates
 // otherwise (src/sample.cpp:41-94).  A mixture's species and selection CDF are the
 // entries [mix_begin, mix_begin + n_species) of Scene::mix_cdf / mix_species.
+enum LayerFlag { kLayerMixture = 1, kLayerAbsorb = 2 };   // Layer::flags
+
 struct Layer {
   double z_min, z_max;
   int medium;                            // HomogeneousLayer: its medium
   int n_species;                         // 0: HomogeneousLayer; else MixtureLayer species
-  int mix_begin, pad;
+  int mix_begin;
+  int flags;                             // kLayerMixture; kLayerAbsorb (the scene records)
   double mu_s, mu_t, mfp, albedo;        // albedo = mu_s / mu_t (1 if mu_t == 0: no split)
   double absorb_prob;                    // mu_a / mu_t: the weight an event deposits
   float mu_t_f, mfp_f;

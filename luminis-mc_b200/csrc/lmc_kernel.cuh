@@ -1673,8 +1673,9 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   // medium without a draw, or a MixtureLayer species by one uniform and lower_bound
   // on its selection CDF (src/sample.cpp:96-104), compared in binary64
   const Layer &SL = sc.layers[ph.layer];
+  const int lflags = SL.flags;
   int med_idx = SL.medium;
-  if (SL.n_species > 0) {
+  if (lflags & kLayerMixture) {
     const double u = (double)uniform<R>(ph.rng, rp);
     int i = 0;
     while (i < SL.n_species - 1 && sc.mix_cdf[SL.mix_begin + i] < u)
@@ -1815,7 +1816,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   }
   ph.events++;                                                // :578-587
   cnt.events++;
-  if (sc.absorb.on) {                                         // :589-592
+  if (lflags & kLayerAbsorb) {                                // :589-592
     const double t = sc.absorb.d_t > 0.0 ? launch_time<R>(sc, rp, ph) + ph.opath : 0.0;  // velocity 1
     record_absorption(sc.absorb, rp.tallies, (double)ph.px, (double)ph.py, (double)ph.pz, t,
                       SL.mu_t > 0 ? ph.w * SL.absorb_prob : 1.0);

@@ -84,6 +84,7 @@ struct lmc_handle {
   unsigned long long *d_prefix = nullptr;      // n_scenes + 1 photon offsets
   unsigned long long *d_sweep_hits = nullptr;  // n_scenes x LMC_MAX_SENSORS, last run
   unsigned long long total_photons = 0;        // photons of one sweep run
+  std::vector<uint64_t> sweep_counts;          // photons per scene (host copy)
   std::vector<lmc::dev::AdjScene> adj_scenes;  // sweep likelihood-ratio layouts (last run)
   void *d_adj_scenes = nullptr;
   size_t adj_scenes_bytes = 0;
@@ -419,6 +420,7 @@ void fill_layers(const lmc_scene *s, dev::Scene &sc)
       d.medium = in.species[0];
       d.n_species = in.n_species;
       d.mix_begin = mix;
+      d.flags |= dev::kLayerMixture;
       mu_a = mu_a_total;
       d.mu_s = mu_s_total;
       d.mu_t = mu_s_total + mu_a_total;
@@ -457,6 +459,8 @@ void fill_absorption(const lmc_scene *s, dev::Scene &sc, size_t tally_base, size
     return;
   dev::AbsorbGrid &g = sc.absorb;
   g.on = 1;
+  for (int l = 0; l < sc.n_layers; ++l)
+    sc.layers[l].flags |= dev::kLayerAbsorb;
   g.n_t = (A.d_t > 0.0) ? (int)std::ceil(A.t_max / A.d_t) + 1 : 1;   // src/absortion.cpp:16-25
   g.n_r = (int)(A.radius / A.d_r) + 1;
   g.n_z = (int)(A.depth / A.d_z) + 1;
@@ -1300,6 +1304,89 @@ lmc_status lmc_sweep_set_photons(lmc_handle *h, const uint64_t *n_photons)
   LMC_CUDA(cudaMemcpy(h->d_prefix, prefix.data(), sizeof(unsigned long long) * (h->n_scenes + 1),
                       cudaMemcpyHostToDevice));
   h->total_photons = prefix[h->n_scenes];
+  h->sweep_counts.assign(n_photons, n_photons + h->n_scenes);
+  return LMC_OK;
+}
+
+lmc_status lmc_autotune(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts, uint64_t sample_photons,
+                        lmc_tune_result *out)
+{
+  using namespace lmc;
+  if (!h || !opts || !out)
+    return fail(LMC_ERR_INVALID, "handle, options and result must not be null");
+  if (sample_photons == 0)
+    return fail(LMC_ERR_INVALID, "sample_photons must be positive");
+  if (h->sweep && h->sweep_counts.empty())
+    return fail(LMC_ERR_INVALID, "lmc_sweep_set_photons() first");
+  LMC_CUDA(cudaSetDevice(h->device));
+  // the sample: photons [0, sample) of a single scene; for a sweep every scene's count
+  // scaled to a total of about sample_photons (at least one photon each), restored after
+  const std::vector<uint64_t> counts = h->sweep_counts;
+  unsigned long long n_sample = sample_photons;
+  if (h->sweep) {
+    const double f = std::min(1.0, (double)sample_photons / (double)std::max<uint64_t>(1, h->total_photons));
+    std::vector<uint64_t> scaled(counts.size());
+    for (size_t k = 0; k < counts.size(); ++k)
+      scaled[k] = counts[k] ? std::max<uint64_t>(1, (uint64_t)std::llround((double)counts[k] * f)) : 0;
+    const lmc_status st = lmc_sweep_set_photons(h, scaled.data());
+    if (st != LMC_OK)
+      return st;
+    n_sample = h->total_photons;
+  }
+  double *d_t = nullptr;
+  cudaError_t e = cudaMalloc(&d_t, std::max<size_t>(h->tally_doubles, 1) * sizeof(double));
+  if (e != cudaSuccess) {
+    if (h->sweep)
+      lmc_sweep_set_photons(h, counts.data());
+    return fail(LMC_ERR_NOMEM, std::string("lmc_autotune: ") + cudaGetErrorString(e));
+  }
+  // candidates: threads per block x resident blocks per SM (the grid, hence photons per
+  // thread of the persistent kernel) x photons per hit-queue batch
+  const int blocks[] = {256, 128};
+  const int per_sm[] = {0, 2, 1};
+  const unsigned long long batches[] = {8ull << 20, 2ull << 20};
+  lmc_tune_result best;
+  std::memset(&best, 0, sizeof(best));
+  lmc_status result = LMC_OK;
+  int tried = 0;
+  for (int b : blocks)
+    for (int p : per_sm)
+      for (unsigned long long q : batches) {
+        if (q != batches[0] && (!h->queued || n_sample <= batches[1]))
+          continue;                              // the batch size only matters past it
+        lmc_run_opts o = *opts;
+        o.block_size = b;
+        o.blocks_per_sm = p;
+        o.batch_photons = q;
+        o.records = nullptr;
+        lmc_stats st;
+        double ms = 0.0;
+        for (int rep = 0; rep < 2 && result == LMC_OK; ++rep) {   // warm-up, then timed
+          result = run_impl(h, seed, 0, n_sample, &o, nullptr, nullptr, d_t, &st);
+          ms = st.kernel_ms;
+        }
+        if (result != LMC_OK)
+          break;
+        ++tried;
+        const double rate = ms > 0 ? (double)n_sample / (ms * 1e-3) : 0.0;
+        if (rate > best.photons_per_s) {
+          best.block_size = b;
+          best.blocks_per_sm = p;
+          best.batch_photons = q;
+          best.photons_per_s = rate;
+        }
+      }
+  cudaFree(d_t);
+  if (h->sweep) {
+    const lmc_status st = lmc_sweep_set_photons(h, counts.data());
+    if (result == LMC_OK)
+      result = st;
+  }
+  if (result != LMC_OK)
+    return result;
+  best.n_tried = tried;
+  best.sample_photons = n_sample;
+  *out = best;
   return LMC_OK;
 }
 

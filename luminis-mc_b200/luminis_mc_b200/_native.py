@@ -88,6 +88,15 @@ class SceneDesc(C.Structure):
                 ("absorption", AbsorptionDesc)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("block_size", C.c_int), ("blocks_per_sm", C.c_int),
+                ("batch_photons", C.c_uint64), ("photons_per_s", C.c_double),
+                ("sample_photons", C.c_uint64), ("n_tried", C.c_int), ("pad", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "pad"}
+
+
 class RunOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("max_events", C.c_int), ("track_reverse_paths", C.c_int),
                 ("block_size", C.c_int), ("blocks_per_sm", C.c_int), ("records", C.c_void_p),
@@ -138,7 +147,8 @@ EXPORTED = ["lmc_create", "lmc_destroy", "lmc_tally_layout", "lmc_run", "lmc_run
             "lmc_amplitude_table", "lmc_probe_fp32_peak", "lmc_run_noalloc",
             "lmc_adjoint_layout", "lmc_run_adjoint", "lmc_adjoint_contract",
             "lmc_create_sweep", "lmc_sweep_layout", "lmc_sweep_set_photons", "lmc_run_sweep",
-            "lmc_sweep_hits", "lmc_sweep_adjoint_layout", "lmc_run_sweep_adjoint"]
+            "lmc_sweep_hits", "lmc_sweep_adjoint_layout", "lmc_run_sweep_adjoint",
+            "lmc_autotune"]
 
 _lib = None
 
@@ -212,6 +222,9 @@ def lib():
     L.lmc_run_sweep_adjoint.argtypes = [vp, C.c_uint64, C.POINTER(RunOpts), C.POINTER(AdjointOpts),
                                         vp, vp, C.POINTER(Stats)]
     L.lmc_run_sweep_adjoint.restype = C.c_int
+    L.lmc_autotune.argtypes = [vp, C.c_uint64, C.POINTER(RunOpts), C.c_uint64,
+                               C.POINTER(TuneResult)]
+    L.lmc_autotune.restype = C.c_int
     L.lmc_sweep_hits.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.lmc_sweep_hits.restype = C.c_int
     _lib = L

@@ -297,6 +297,16 @@ class Transport:
                                 C.byref(st) if want_stats else None))
         return st.as_dict() if want_stats else {}
 
+    def autotune(self, seed: int, precision: str = "fp32", sample_photons: int = 4_000_000,
+                 **kw) -> dict:
+        """Launch shape (block_size, blocks_per_sm, batch_photons) that ran a sample of
+        this scene fastest (lmc_autotune); pass it to run_device / run_host."""
+        r = N.TuneResult()
+        N.check(N.lib().lmc_autotune(self._h, int(seed) & (2 ** 64 - 1),
+                                     C.byref(self.opts(precision=precision, **kw)),
+                                     int(sample_photons), C.byref(r)))
+        return r.as_dict()
+
     def split(self, tallies: np.ndarray):
         """Per-sensor views of a flat tally buffer, in the sensor layouts."""
         return [tallies[o:o + c].reshape(d) for (o, c, d) in self.layout]

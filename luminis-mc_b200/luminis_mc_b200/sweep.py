@@ -54,6 +54,7 @@ class SweepRun:
         self.tallies = torch.zeros(max(self.tally_size, 1), dtype=torch.float64, device=self.device)
         self.n_scenes = n
         self.photons = None
+        self.launch = {}                 # launch shape from autotune(), used by every run
 
     def set_photons(self, counts) -> None:
         """Photons per scene for the following runs."""
@@ -73,7 +74,24 @@ class SweepRun:
         o.max_events = int(c.MAX_EVENTS if max_events is None else max_events)
         o.track_reverse_paths = int(any(bool(cfg.track_reverse_paths) for cfg in self.configs))
         o.stream = stream
+        for key, value in self.launch.items():
+            setattr(o, key, value)
         return o
+
+    def autotune(self, seed: int, precision: str = "fp32", sample_photons: int = 10_000_000) -> dict:
+        """Pick the launch shape (threads per block, blocks per SM, photons per batch) by
+        timing candidates on a scaled-down copy of the sweep (lmc_autotune); later runs
+        use it.  Returns the chosen shape and its rate on the sample."""
+        if self.photons is None:
+            raise ValueError("set_photons() first")
+        self.launch = {}
+        r = N.TuneResult()
+        N.check(N.lib().lmc_autotune(self._h, int(seed) & (2 ** 64 - 1),
+                                     C.byref(self.opts(precision)), int(sample_photons),
+                                     C.byref(r)))
+        self.launch = {"block_size": r.block_size, "blocks_per_sm": r.blocks_per_sm,
+                       "batch_photons": r.batch_photons}
+        return r.as_dict()
 
     def run(self, seed: int, precision: str = "fp32", stream=None, want_stats: bool = True):
         """Transport every scene's photons, adding into self.tallies; stats or {}."""

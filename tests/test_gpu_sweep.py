@@ -142,3 +142,30 @@ def test_sweep_adjoint_radial_outputs_and_media_counts(cuda):
         np.testing.assert_allclose(jac.cpu().numpy(), want_jac, rtol=RTOL,
                                    atol=RTOL * np.abs(want_jac).max())
     sw.close()
+
+
+def test_autotune_picks_a_shape_and_keeps_results(cuda):
+    """lmc_autotune times its candidate launch shapes on a scaled-down sweep, restores the
+    photon counts, and the tuned shape gives the same FP64 tallies (results do not
+    depend on the launch shape)."""
+    specs = _specs()[:4]
+    counts = [30000, 5000, 22000, 900]
+    sw = SweepRun([W.build(lm, s)[0] for s in specs])
+    sw.set_photons(counts)
+    st0 = sw.run(5, precision="fp64")
+    base = [sw.host_tallies(k) for k in range(4)]
+    r = sw.autotune(5, precision="fp64", sample_photons=20000)
+    assert r["block_size"] in (128, 256) and r["blocks_per_sm"] in (0, 1, 2)
+    assert r["n_tried"] >= 6 and r["photons_per_s"] > 0 and 4 <= r["sample_photons"] <= 25000
+    sw.zero()
+    st = sw.run(5, precision="fp64")
+    assert st["photons"] == st0["photons"] == sum(counts)
+    for k in range(4):
+        for a, b in zip(sw.host_tallies(k), base[k]):
+            np.testing.assert_allclose(a, b, rtol=RTOL, atol=RTOL * max(np.abs(b).max(), 1e-300))
+    sw.close()
+    from luminis_mc_b200.simulation import Transport
+    t = Transport(W.build(lm, W.mie_cbs_small(0, 1))[0])
+    r = t.autotune(1, precision="fp32", sample_photons=50000)
+    assert r["sample_photons"] == 50000 and r["photons_per_s"] > 0
+    t.close()
