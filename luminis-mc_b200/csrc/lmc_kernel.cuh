@@ -1599,7 +1599,9 @@ __device__ __noinline__ void record_absorption(const AbsorbGrid &g, double *tall
 
 // One loop iteration of run_photon (src/simulation.cpp:297-614).  Returns the
 // photon's fate (kAlive if it continues).
-template <typename R, bool kQueue, bool kAdj, bool kEst = false>
+// kExtras: the MixtureLayer species draw and the Absorption recorder are compiled in
+// (scenes without either run the variant without their code).
+template <typename R, bool kQueue, bool kAdj, bool kEst = false, bool kExtras = false>
 __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, Photon<R> &ph,
                                           Side<R> &side, Flight<R> &fl, Counters &cnt,
                                           unsigned long long *s_hits)
@@ -1675,7 +1677,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   const Layer &SL = sc.layers[ph.layer];
   const int lflags = SL.flags;
   int med_idx = SL.medium;
-  if (lflags & kLayerMixture) {
+  if (kExtras && (lflags & kLayerMixture)) {
     const double u = (double)uniform<R>(ph.rng, rp);
     int i = 0;
     while (i < SL.n_species - 1 && sc.mix_cdf[SL.mix_begin + i] < u)
@@ -1816,7 +1818,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   }
   ph.events++;                                                // :578-587
   cnt.events++;
-  if (lflags & kLayerAbsorb) {                                // :589-592
+  if (kExtras && (lflags & kLayerAbsorb)) {                   // :589-592
     const double t = sc.absorb.d_t > 0.0 ? launch_time<R>(sc, rp, ph) + ph.opath : 0.0;  // velocity 1
     record_absorption(sc.absorb, rp.tallies, (double)ph.px, (double)ph.py, (double)ph.pz, t,
                       SL.mu_t > 0 ? ph.w * SL.absorb_prob : 1.0);
@@ -1895,7 +1897,8 @@ __device__ __forceinline__ int sweep_scene(const RunParams &rp, unsigned long lo
 // vertex).  kAdj: likelihood-ratio run (queued mode only).  kSweep: g_scene is an array of
 // rp.n_scenes scenes read from global memory (L1-cached), photon g belongs to scene
 // sweep_scene(g), and each lane follows its own photon's scene.
-template <typename R, bool kQueue, int kMinBlocks, bool kAdj = false, bool kSweep = false, bool kEst = false>
+template <typename R, bool kQueue, int kMinBlocks, bool kAdj = false, bool kSweep = false, bool kEst = false,
+          bool kExtras = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
   __shared__ __align__(16) unsigned char s_raw[kSweep ? 16 : sizeof(Scene)];
@@ -1948,7 +1951,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
     if (__all_sync(kFull, done))
       break;
     if (alive) {
-      const int fate = event_step<R, kQueue, kAdj, kEst>(*scp, rp, ph, side, fl, cnt, s_hits);
+      const int fate = event_step<R, kQueue, kAdj, kEst, kExtras>(*scp, rp, ph, side, fl, cnt, s_hits);
       if (fate != kAlive) {
         alive = false;
         cnt.draws += ph.rng.draw;

@@ -890,6 +890,63 @@ static lmc_status sweep_adjoint_layout(const lmc_handle *h, const lmc_adjoint_op
   return LMC_OK;
 }
 
+}  // extern "C"
+
+// The transport and tally kernels of a run.  `extras`: a scene has a MixtureLayer or an
+// Absorption recorder (the variants with their code; the others leave it out).
+using KernelFn = void (*)(const lmc::dev::Scene *, lmc::dev::RunParams);
+
+template <bool E>
+static KernelFn pick_transport_e(bool fp32, bool queued, bool three, bool adj, bool sw, bool est)
+{
+  using namespace lmc::dev;
+  if (est)
+    return fp32 ? transport_kernel<float, true, 2, false, false, true, E>
+                : transport_kernel<double, true, 1, false, false, true, E>;
+  if (sw && adj)
+    return fp32 ? transport_kernel<float, true, 2, true, true> : transport_kernel<double, true, 1, true, true>;
+  if (sw)
+    return fp32 ? transport_kernel<float, true, 3, false, true, false, E>
+                : transport_kernel<double, true, 2, false, true, false, E>;
+  if (adj)
+    return fp32 ? transport_kernel<float, true, 3, true> : transport_kernel<double, true, 1, true>;
+  if (fp32)
+    return queued ? (three ? transport_kernel<float, true, 3, false, false, false, E>
+                           : transport_kernel<float, true, 2, false, false, false, E>)
+                  : transport_kernel<float, false, 1, false, false, false, E>;
+  return queued ? transport_kernel<double, true, 2, false, false, false, E>
+                : transport_kernel<double, false, 1, false, false, false, E>;
+}
+
+static KernelFn pick_transport(bool fp32, bool queued, bool three, bool adj, bool sw, bool est, bool extras)
+{
+  return extras ? pick_transport_e<true>(fp32, queued, three, adj, sw, est)
+                : pick_transport_e<false>(fp32, queued, three, adj, sw, est);
+}
+
+static KernelFn pick_tally(bool fp32, bool adj, bool sw)
+{
+  using namespace lmc::dev;
+  if (sw && adj)
+    return fp32 ? tally_kernel<float, true, true> : tally_kernel<double, true, true>;
+  if (sw)
+    return fp32 ? tally_kernel<float, false, true> : tally_kernel<double, false, true>;
+  if (adj)
+    return fp32 ? tally_kernel<float, true> : tally_kernel<double, true>;
+  return fp32 ? tally_kernel<float> : tally_kernel<double>;
+}
+
+// Whether any of a scene's layers draws species or records absorption.
+static bool scene_extras(const lmc::dev::Scene &sc)
+{
+  for (int l = 0; l < sc.n_layers; ++l)
+    if (sc.layers[l].flags & (lmc::dev::kLayerMixture | lmc::dev::kLayerAbsorb))
+      return true;
+  return false;
+}
+
+extern "C" {
+
 // lmc_run and lmc_run_adjoint (adj == nullptr: plain run).
 static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
                            const lmc_run_opts *opts, const lmc_adjoint_opts *adj, double *d_adj,
@@ -999,28 +1056,20 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   // binary32 queued transport: a 3-block (<=85 registers, the default) and a
   // 2-block (<=128 registers) variant; blocks_per_sm == 1 or 2 selects the latter
   const bool three = fp32 && h->queued && !adj && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
-  const void *tk =
-      est ? (fp32 ? (const void *)dev::transport_kernel<float, true, 2, false, false, true>
-                  : (const void *)dev::transport_kernel<double, true, 1, false, false, true>)
-      : (sw && adj) ? (fp32 ? (const void *)dev::transport_kernel<float, true, 2, true, true>
-                            : (const void *)dev::transport_kernel<double, true, 1, true, true>)
-      : sw ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, false, true>
-                 : (const void *)dev::transport_kernel<double, true, 2, false, true>)
-      : adj ? (fp32 ? (const void *)dev::transport_kernel<float, true, 3, true>
-                  : (const void *)dev::transport_kernel<double, true, 1, true>)
-          : fp32 ? (h->queued ? (three ? (const void *)dev::transport_kernel<float, true, 3>
-                                       : (const void *)dev::transport_kernel<float, true, 2>)
-                              : (const void *)dev::transport_kernel<float, false, 1>)
-                 : (h->queued ? (const void *)dev::transport_kernel<double, true, 2>
-                              : (const void *)dev::transport_kernel<double, false, 1>);
-  LMC_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_transport));
-  if (adj && !sw) {
-    const void *tl = fp32 ? (const void *)dev::tally_kernel<float, true>
-                          : (const void *)dev::tally_kernel<double, true>;
-    LMC_CUDA(cudaFuncSetAttribute(tl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_tally));
-  }
+  bool extras = false;
+  for (int k = 0; k < h->n_scenes; ++k)
+    extras = extras || scene_extras(sw ? h->scenes[k] : h->scene);
+  if (adj && extras)                     // (MixtureLayers are refused by the layout already)
+    return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio runs do not record an Absorption grid");
+  const KernelFn tk = pick_transport(fp32, h->queued, three, adj != nullptr, sw, est, extras);
+  const KernelFn tl = pick_tally(fp32, adj != nullptr, sw);
+  LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)dyn_transport));
+  if (adj && !sw)
+    LMC_CUDA(cudaFuncSetAttribute((const void *)tl, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)dyn_tally));
   int per_sm = 0;
-  LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tk, block, dyn_transport));
+  LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)tk, block, dyn_transport));
   if (opts->blocks_per_sm > 0)
     per_sm = std::min(per_sm, opts->blocks_per_sm);
   per_sm = std::max(per_sm, 1);
@@ -1074,39 +1123,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     const size_t pair = 2 * (size_t)(done / batch);
     if (stats)
       LMC_CUDA(cudaEventRecord(h->kev[pair], stream));
-    if (est) {
-      if (fp32)
-        dev::transport_kernel<float, true, 2, false, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-      else
-        dev::transport_kernel<double, true, 1, false, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-    } else if (sw && adj) {
-      if (fp32)
-        dev::transport_kernel<float, true, 2, true, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-      else
-        dev::transport_kernel<double, true, 1, true, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-    } else if (sw) {
-      if (fp32)
-        dev::transport_kernel<float, true, 3, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-      else
-        dev::transport_kernel<double, true, 2, false, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-    } else if (adj) {
-      if (fp32)
-        dev::transport_kernel<float, true, 3, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-      else
-        dev::transport_kernel<double, true, 1, true><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-    } else if (fp32) {
-      if (h->queued && three)
-        dev::transport_kernel<float, true, 3><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-      else if (h->queued)
-        dev::transport_kernel<float, true, 2><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-      else
-        dev::transport_kernel<float, false, 1><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-    } else {
-      if (h->queued)
-        dev::transport_kernel<double, true, 2><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-      else
-        dev::transport_kernel<double, false, 1><<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
-    }
+    tk<<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
     LMC_CUDA(cudaGetLastError());
     if (stats)
       LMC_CUDA(cudaEventRecord(h->kev[pair + 1], stream));
@@ -1114,26 +1131,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
       const int tgrid = (int)std::max<unsigned long long>(
           1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * 8,
                                              (rp.queue.cap + dev::kBlock - 1) / dev::kBlock));
-      if (sw && adj) {
-        if (fp32)
-          dev::tally_kernel<float, true, true><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
-        else
-          dev::tally_kernel<double, true, true><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
-      } else if (sw) {
-        if (fp32)
-          dev::tally_kernel<float, false, true><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
-        else
-          dev::tally_kernel<double, false, true><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
-      } else if (adj) {
-        if (fp32)
-          dev::tally_kernel<float, true><<<tgrid, dev::kBlock, dyn_tally, stream>>>(h->d_scene, rp);
-        else
-          dev::tally_kernel<double, true><<<tgrid, dev::kBlock, dyn_tally, stream>>>(h->d_scene, rp);
-      } else if (fp32) {
-        dev::tally_kernel<float><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
-      } else {
-        dev::tally_kernel<double><<<tgrid, dev::kBlock, 0, stream>>>(h->d_scene, rp);
-      }
+      tl<<<tgrid, dev::kBlock, (adj && !sw) ? dyn_tally : 0, stream>>>(h->d_scene, rp);
       LMC_CUDA(cudaGetLastError());
     }
   }
@@ -1816,10 +1814,14 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     return fail(LMC_ERR_INVALID, "stream_format must be 0 or 1");
   rp.stream_u24 = (!fp32 && opts->stream_format == 1) ? 1 : 0;
   const int block = dev::kBlock;
-  const void *tk = fp32 ? (queued ? (const void *)dev::transport_kernel<float, true, 2>
-                                  : (const void *)dev::transport_kernel<float, false, 1>)
-                        : (queued ? (const void *)dev::transport_kernel<double, true, 1>
-                                  : (const void *)dev::transport_kernel<double, false, 1>);
+  const bool extras = scene_extras(sc);
+  const KernelFn tk =
+      extras ? (fp32 ? (queued ? dev::transport_kernel<float, true, 2, false, false, false, true>
+                               : dev::transport_kernel<float, false, 1, false, false, false, true>)
+                     : (queued ? dev::transport_kernel<double, true, 1, false, false, false, true>
+                               : dev::transport_kernel<double, false, 1, false, false, false, true>))
+             : (fp32 ? (queued ? dev::transport_kernel<float, true, 2> : dev::transport_kernel<float, false, 1>)
+                     : (queued ? dev::transport_kernel<double, true, 1> : dev::transport_kernel<double, false, 1>));
   const size_t dyn_transport = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
   LMC_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_transport));
   int per_sm = 0;
@@ -1850,17 +1852,7 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     LMC_CUDA(cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned long long), stream));
     const int grid = (int)std::max<unsigned long long>(
         1ull, std::min<unsigned long long>((unsigned long long)sm_count * per_sm, (nb + block - 1) / block));
-    if (fp32) {
-      if (queued)
-        dev::transport_kernel<float, true, 2><<<grid, block, dyn_transport, stream>>>(d_scene, rp);
-      else
-        dev::transport_kernel<float, false, 1><<<grid, block, dyn_transport, stream>>>(d_scene, rp);
-    } else {
-      if (queued)
-        dev::transport_kernel<double, true, 1><<<grid, block, dyn_transport, stream>>>(d_scene, rp);
-      else
-        dev::transport_kernel<double, false, 1><<<grid, block, dyn_transport, stream>>>(d_scene, rp);
-    }
+    tk<<<grid, block, dyn_transport, stream>>>(d_scene, rp);
     LMC_CUDA(cudaGetLastError());
     if (queued && s->n_sensors > 0) {
       const int tgrid = (int)std::max<unsigned long long>(

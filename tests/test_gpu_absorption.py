@@ -76,3 +76,14 @@ def test_sweep_holds_the_lone_run_grid(cuda):
                                    atol=1e-12 * np.abs(want).max())
         run.close()
     sw.close()
+
+
+def test_adjoint_refuses_absorption(cuda):
+    """Likelihood-ratio runs carry no Absorption grid: refused, not silently dropped."""
+    from luminis_mc_b200.adjoint import AdjointTransport
+    spec = absorption_scenes()[0]
+    cfg, _, keep = W.build(lm, spec)
+    tr = AdjointTransport(cfg)
+    with pytest.raises(NotImplementedError):
+        tr.run(100, 1, precision="fp64")
+    tr.close()
