@@ -34,9 +34,9 @@ sys.path.insert(0, REPO)
 FLOP_PER_EVENT = 300        # FP32 flops per scattering event (add/mul = 1, FMA = 2)
 METRIC = "photons/s"
 # DRAM bytes (read + write) per photon of one transport launch on bilayer_rgd_mie in
-# FP32: 863.4 MB for an 8 M-photon launch in one ncu capture
+# FP32: 89.8 MB read + 763.0 MB written for an 8 M-photon launch in one ncu capture
 # (profiles/transport_kernel_bilayer_rgd_mie.md); traffic grows with photons.
-TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": 863.42e6 / 8e6}
+TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": (89.845e6 + 763.017e6) / 8e6}
 
 
 def parse():
