@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--batch-photons", type=int, default=0)
     ap.add_argument("--variant-steps", type=int, default=2,
                     help="timed steps of the FP64 and FP32+adjoint variants (0: skip them)")
+    ap.add_argument("--variants", default="fp64,differentiable,sweep,estimator",
+                    help="comma-separated subset of the variant arms to measure")
+    ap.add_argument("--estimator-photons", type=int, default=200_000,
+                    help="photons of the estimator-mode variant")
     ap.add_argument("--precision-report", action="store_true",
                     help="instead of timing: FP32 tallies against FP64 on the same random "
                          "numbers, per sensor, for the named workloads")
@@ -361,14 +365,8 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
     differentiable configuration (HG bilayer, 1e7 photons, radial fluence profile of
     100 bins to 5 mm, CBS cone); and the batched sweep of 256 Mie media in one launch
     (plain, replayed from a CUDA graph, and as one launch per medium).  photons/s from
-    the device time of the runs."""
-    import numpy as np
+    the device time of the runs.  `--variants` picks a subset."""
     import torch
-
-    import luminis_mc_b200 as lm
-    from luminis_mc_b200 import workloads as W
-    from luminis_mc_b200.adjoint import AdjointTransport
-    from luminis_mc_b200.device import DeviceRun
 
     def max_ms(ms):
         t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
@@ -377,6 +375,24 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
         return float(t.item())
 
     out = {}
+    sel = set(args.variants.split(","))
+    if "fp64" in sel:
+        out.update(measure_fp64(args, spec, local, stream, flush, world, rank, max_ms))
+    if "differentiable" in sel:
+        out.update(measure_differentiable(args, local, stream, flush, world, rank, max_ms))
+    if "sweep" in sel:
+        out.update(measure_sweep(args, local, stream, flush, world, rank, max_ms))
+    if "estimator" in sel:
+        out.update(measure_estimator(args, local, stream, flush, world, rank, max_ms))
+    return out
+
+
+def measure_fp64(args, spec, local, stream, flush, world, rank, max_ms):
+    """FP64 throughout on the headline workload."""
+    import luminis_mc_b200 as lm
+    from luminis_mc_b200 import workloads as W
+    from luminis_mc_b200.device import DeviceRun
+
     P = int(spec["n_photons"])
     cfg, _, keep = W.build(lm, spec)
     run = DeviceRun(cfg, device=f"cuda:{local}")
@@ -389,8 +405,19 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
             ms += st["kernel_ms"]
     run.close()
     ms = max_ms(ms)
-    out["fp64"] = {"value": P * world * args.variant_steps / (ms * 1e-3), "unit": "photons/s",
-                   "workload": spec["name"], "steps": args.variant_steps}
+    return {"fp64": {"value": P * world * args.variant_steps / (ms * 1e-3), "unit": "photons/s",
+                     "workload": spec["name"], "steps": args.variant_steps}}
+
+
+def measure_differentiable(args, local, stream, flush, world, rank, max_ms):
+    """FP32 on the differentiable workload, without and with the likelihood-ratio
+    derivatives (HG bilayer, 1e7 photons, radial fluence profile, CBS cone)."""
+    import luminis_mc_b200 as lm
+    from luminis_mc_b200 import workloads as W
+    from luminis_mc_b200.adjoint import AdjointTransport
+    from luminis_mc_b200.device import DeviceRun
+
+    out = {}
 
     aspec = W.bilayer_hg(10_000_000, 2024)
     acfg, _, akeep = W.build(lm, aspec)
@@ -424,8 +451,21 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
                            "parameters": 8, "outputs": "total + 100 radial bins + CBS S0 cone",
                            "steps": args.variant_steps}
 
-    # batched sweep: 256 single-layer Mie media (seeded radius, mu_s, mu_a, photon counts
-    # log-uniform 1e5..1e7) in one launch, against one launch per medium
+    return out
+
+
+def measure_sweep(args, local, stream, flush, world, rank, max_ms):
+    """The batched sweep: 256 single-layer Mie media (seeded radius, mu_s, mu_a, photon
+    counts log-uniform 1e5..1e7) in one launch, against one launch per medium; with and
+    without each medium's gradients; launch shape from the autotuner."""
+    import numpy as np
+    import torch
+
+    import luminis_mc_b200 as lm
+    from luminis_mc_b200 import workloads as W
+    from luminis_mc_b200.adjoint import AdjointTransport
+
+    out = {}
     from luminis_mc_b200.sweep import SweepRun
     from luminis_mc_b200.simulation import Transport
     _, _, _, counts = W.mie_sweep_parameters()
@@ -492,10 +532,19 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
         "workload": "256 single-layer Mie media, FarFieldCBS 100x1 each, seeded draws "
                     "(numpy default_rng(2026))"}
 
-    # estimator-mode FarFieldCBS (the reference's last-flight CBS estimate at every
-    # vertex), mie_cbs_small geometry with its 100-bin grid, against the reference's own
-    # estimator on this host's cores
-    espec = W.mie_cbs_small(200_000, 4242)
+    return out
+
+
+def measure_estimator(args, local, stream, flush, world, rank, max_ms):
+    """Estimator-mode FarFieldCBS (the reference's last-flight CBS estimate at every
+    vertex), mie_cbs_small geometry with its 100-bin grid, against the reference's own
+    estimator on this host's cores."""
+    import luminis_mc_b200 as lm
+    from luminis_mc_b200 import workloads as W
+    from luminis_mc_b200.device import DeviceRun
+
+    out = {}
+    espec = W.mie_cbs_small(args.estimator_photons, 4242)
     espec["sensors"] = [dict(espec["sensors"][0], estimator=True)]
     ecfg, _, ekeep = W.build(lm, espec)
     PE = int(espec["n_photons"])

@@ -1101,63 +1101,70 @@ __device__ __forceinline__ V3<double> drow(const double *P, int r)
   return v3<double>(P[3 * r], P[3 * r + 1], P[3 * r + 2]);
 }
 
+template <typename T> __device__ __forceinline__ V3<T> trow(const T *P, int r)
+{
+  return v3<T>(P[3 * r], P[3 * r + 1], P[3 * r + 2]);
+}
+
 // Stages A + B of the reverse path with P_{n-1} = the current frame
 // (src/detector.cpp:1079-1118).
-__device__ __forceinline__ void est_prefix(const Scene &sc, const double *Pnm1, const Cx<double> *T,
-                                           int med_n, Cx<double> &Om, Cx<double> &On)
+template <typename T>
+__device__ __forceinline__ void est_prefix(const Scene &sc, const T *Pnm1, const Cx<T> *Tm,
+                                           int med_n, Cx<T> &Om, Cx<T> &On)
 {
   const Laser &L = sc.laser;
-  const V3<double> m0 = v3<double>(L.m[0], L.m[1], L.m[2]);
-  const V3<double> n0 = v3<double>(L.n[0], L.n[1], L.n[2]);
-  const V3<double> s0 = v3<double>(L.dir[0], L.dir[1], L.dir[2]);
-  const Cx<double> E0m = {L.E[0], L.E[1]}, E0n = {L.E[2], L.E[3]};
-  const V3<double> mnm1 = drow(Pnm1, 0), nnm1 = drow(Pnm1, 1), snm1 = drow(Pnm1, 2);
-  const V3<double> s_out_a = vscale(snm1, -1.0);
-  Cx<double> Sa2, Sa1;
-  amplitudes<double>(sc.media[med_n], unit_angle(s0, s_out_a), Sa2, Sa1);
-  const V3<double> np_ = safe_unit(vcross_unit(s0, s_out_a), n0);
-  const V3<double> mp_in = safe_unit(vcross_unit(np_, s0), m0);
-  const V3<double> mp_out = safe_unit(vcross_unit(np_, s_out_a), mnm1);
-  double r00 = vdot(mp_in, m0), r01 = vdot(mp_in, n0), r10 = vdot(np_, m0), r11 = vdot(np_, n0);
-  Cx<double> Em = cadd(cmul(cscale(Sa2, r00), E0m), cmul(cscale(Sa2, r01), E0n));
-  Cx<double> En = cadd(cmul(cscale(Sa1, r10), E0m), cmul(cscale(Sa1, r11), E0n));
-  const V3<double> nn1 = vscale(nnm1, -1.0);
+  const V3<T> m0 = v3<T>(T(L.m[0]), T(L.m[1]), T(L.m[2]));
+  const V3<T> n0 = v3<T>(T(L.n[0]), T(L.n[1]), T(L.n[2]));
+  const V3<T> s0 = v3<T>(T(L.dir[0]), T(L.dir[1]), T(L.dir[2]));
+  const Cx<T> E0m = {T(L.E[0]), T(L.E[1])}, E0n = {T(L.E[2]), T(L.E[3])};
+  const V3<T> mnm1 = trow<T>(Pnm1, 0), nnm1 = trow<T>(Pnm1, 1), snm1 = trow<T>(Pnm1, 2);
+  const V3<T> s_out_a = vscale(snm1, T(-1));
+  Cx<T> Sa2, Sa1;
+  amplitudes<T>(sc.media[med_n], unit_angle(s0, s_out_a), Sa2, Sa1);
+  const V3<T> np_ = safe_unit(vcross_unit(s0, s_out_a), n0);
+  const V3<T> mp_in = safe_unit(vcross_unit(np_, s0), m0);
+  const V3<T> mp_out = safe_unit(vcross_unit(np_, s_out_a), mnm1);
+  T r00 = vdot(mp_in, m0), r01 = vdot(mp_in, n0), r10 = vdot(np_, m0), r11 = vdot(np_, n0);
+  Cx<T> Em = cadd(cmul(cscale(Sa2, r00), E0m), cmul(cscale(Sa2, r01), E0n));
+  Cx<T> En = cadd(cmul(cscale(Sa1, r10), E0m), cmul(cscale(Sa1, r11), E0n));
+  const V3<T> nn1 = vscale(nnm1, T(-1));
   r00 = vdot(mnm1, mp_out); r01 = vdot(mnm1, np_); r10 = vdot(nn1, mp_out); r11 = vdot(nn1, np_);
-  Cx<double> tm = cadd(cscale(Em, r00), cscale(En, r01));
-  Cx<double> tn = cadd(cscale(Em, r10), cscale(En, r11));
+  Cx<T> tm = cadd(cscale(Em, r00), cscale(En, r01));
+  Cx<T> tn = cadd(cscale(Em, r10), cscale(En, r11));
   tn = {-tn.re, -tn.im};
-  Em = cadd(cmul(T[0], tm), cmul(T[2], tn));
-  En = cadd(cmul(T[1], tm), cmul(T[3], tn));
+  Em = cadd(cmul(Tm[0], tm), cmul(Tm[2], tn));
+  En = cadd(cmul(Tm[1], tm), cmul(Tm[3], tn));
   Om = Em;
   On = {-En.re, -En.im};
 }
 
 // Stage C and the normalisation (src/detector.cpp:1122-1161).
-__device__ __forceinline__ void est_suffix(const Scene &sc, const double *P1, const double *Pn, int med_1,
-                                           Cx<double> Em, Cx<double> En, Cx<double> &Om, Cx<double> &On)
+template <typename T>
+__device__ __forceinline__ void est_suffix(const Scene &sc, const T *P1, const T *Pn, int med_1,
+                                           Cx<T> Em, Cx<T> En, Cx<T> &Om, Cx<T> &On)
 {
-  const V3<double> m1 = drow(P1, 0), n1 = drow(P1, 1), s1 = drow(P1, 2);
-  const V3<double> mn = drow(Pn, 0), nn = drow(Pn, 1), sn = drow(Pn, 2);
-  const V3<double> s_in_c = vscale(s1, -1.0);
-  const V3<double> n1m = vscale(n1, -1.0);
-  Cx<double> Sc2, Sc1;
-  amplitudes<double>(sc.media[med_1], unit_angle(s_in_c, sn), Sc2, Sc1);
-  const V3<double> npp = safe_unit(vcross_unit(s_in_c, sn), n1m);
-  const V3<double> mpp_in = safe_unit(vcross_unit(npp, s_in_c), m1);
-  const V3<double> mpp_out = safe_unit(vcross_unit(npp, sn), mn);
-  double r00 = vdot(mpp_in, m1), r01 = vdot(mpp_in, n1m), r10 = vdot(npp, m1), r11 = vdot(npp, n1m);
-  const Cx<double> Fm = cadd(cmul(cscale(Sc2, r00), Em), cmul(cscale(Sc2, r01), En));
-  const Cx<double> Fn = cadd(cmul(cscale(Sc1, r10), Em), cmul(cscale(Sc1, r11), En));
+  const V3<T> m1 = trow<T>(P1, 0), n1 = trow<T>(P1, 1), s1 = trow<T>(P1, 2);
+  const V3<T> mn = trow<T>(Pn, 0), nn = trow<T>(Pn, 1), sn = trow<T>(Pn, 2);
+  const V3<T> s_in_c = vscale(s1, T(-1));
+  const V3<T> n1m = vscale(n1, T(-1));
+  Cx<T> Sc2, Sc1;
+  amplitudes<T>(sc.media[med_1], unit_angle(s_in_c, sn), Sc2, Sc1);
+  const V3<T> npp = safe_unit(vcross_unit(s_in_c, sn), n1m);
+  const V3<T> mpp_in = safe_unit(vcross_unit(npp, s_in_c), m1);
+  const V3<T> mpp_out = safe_unit(vcross_unit(npp, sn), mn);
+  T r00 = vdot(mpp_in, m1), r01 = vdot(mpp_in, n1m), r10 = vdot(npp, m1), r11 = vdot(npp, n1m);
+  const Cx<T> Fm = cadd(cmul(cscale(Sc2, r00), Em), cmul(cscale(Sc2, r01), En));
+  const Cx<T> Fn = cadd(cmul(cscale(Sc1, r10), Em), cmul(cscale(Sc1, r11), En));
   r00 = vdot(mn, mpp_out); r01 = vdot(mn, npp); r10 = vdot(nn, mpp_out); r11 = vdot(nn, npp);
-  Cx<double> gm = cadd(cscale(Fm, r00), cscale(Fn, r01));
-  Cx<double> gn = cadd(cscale(Fm, r10), cscale(Fn, r11));
-  const double nrm = sqrt(cnorm(gm) + cnorm(gn));
-  if (nrm > 1e-300) {
+  Cx<T> gm = cadd(cscale(Fm, r00), cscale(Fn, r01));
+  Cx<T> gn = cadd(cscale(Fm, r10), cscale(Fn, r11));
+  const T nrm = sqrt(cnorm(gm) + cnorm(gn));
+  if (nrm > tiny<T>()) {
     gm = {gm.re / nrm, gm.im / nrm};
     gn = {gn.re / nrm, gn.im / nrm};
   } else {
-    gm = {0.0, 0.0};
-    gn = {0.0, 0.0};
+    gm = {T(0), T(0)};
+    gn = {T(0), T(0)};
   }
   Om = gm;
   On = gn;
@@ -1337,6 +1344,158 @@ __device__ __noinline__ void estimate_vertex(const Scene &sc, const RunParams &r
 }
 
 // The vertex a photon is at, as the estimator reads it.
+// The same estimate in binary32 for binary32 transport (the CBS phase excepted): bin
+// directions from the binary32 copy of the bin table, the scattering angle as
+// atan2(|s_cur x s_out|, s_cur . s_out), binary32 amplitudes, transmittance, fields and
+// Stokes values, accumulated in binary64.  exp(i k L) multiplies the forward and the
+// reverse field alike and cancels in every Stokes value, so it is not formed; the CBS
+// phase q . (r_n - r_1) uses the table's q = k (s_out + s_in), formed in binary64.
+template <typename R>
+__device__ __noinline__ void estimate_vertex_f32(const Scene &sc, const RunParams &rp, const EstVertex v,
+                                                 unsigned long long *s_hits)
+{
+  const Laser &L = sc.laser;
+  float P[9], P1[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    P[j] = (float)v.P[j];
+    P1[j] = (float)v.P1[j];
+  }
+  const V3<float> m_cur = trow<float>(P, 0), n_cur = trow<float>(P, 1), s_cur = trow<float>(P, 2);
+  const Cx<float> Em = {(float)v.Em.re, (float)v.Em.im}, En = {(float)v.En.re, (float)v.En.im};
+  const float dr[3] = {(float)(v.pos[0] - v.r1[0]), (float)(v.pos[1] - v.r1[1]), (float)(v.pos[2] - v.r1[2])};
+  const Medium &med = sc.media[v.med];
+  const unsigned lane = threadIdx.x & 31u;
+  for (int si = 0; si < sc.n_sensors; ++si) {
+    const Sensor &s = sc.sensors[si];
+    if (s.kind != LMC_SENSOR_FARFIELD_CBS || !s.estimator)
+      continue;
+    if (s.f_events && (v.events < s.events_min || v.events > s.events_max))
+      continue;
+    if (med.I_norm < 1e-300)
+      continue;
+    const Layer &VL = sc.layers[v.layer];
+    const double w_scatter = v.w * (v.events == 0 ? VL.mu_s / VL.mu_t : med.mu_s / med.mu_t);
+    if (w_scatter < 1e-300)
+      continue;
+    const bool multi = v.events >= 1;
+    Cx<float> pre_m = {0.f, 0.f}, pre_n = {0.f, 0.f};
+    if (multi) {
+      const Cx<float> T[4] = {{(float)v.T[0].re, (float)v.T[0].im}, {(float)v.T[1].re, (float)v.T[1].im},
+                              {(float)v.T[2].re, (float)v.T[2].im}, {(float)v.T[3].re, (float)v.T[3].im}};
+      est_prefix<float>(sc, P, T, v.med, pre_m, pre_n);
+    }
+    const double t_launch = (s.dt > 0) ? emission_time<R>(L, rp, v.index) : 0.0;
+    // p(Omega) dOmega = F / (pi I_norm) x dOmega dphi; w_scatter folded in
+    const float pref = (float)(w_scatter / (3.141592653589793 * med.I_norm));
+    const float mu_t1 = sc.layers[v.layer].mu_t_f;
+    const float pz = (float)v.pos[2];
+    const float Emm = cnorm(Em), Enn = cnorm(En);
+    const float e12 = Em.re * En.re + Em.im * En.im;
+    double *base = rp.tallies + s.tally_off;
+    const unsigned long long PS = s.plane_stride;
+    const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
+    const int nb = s.est_n;
+    const float4 *bf = reinterpret_cast<const float4 *>(s.est_bins + nb);
+    for (int k = 0; k < nb; ++k) {
+      int b = k + (int)lane;
+      if (b >= nb)
+        b -= nb * (b / nb);
+      const float4 bin = bf[2 * b];
+      const V3<float> s_out = v3<float>(bin.x, bin.y, bin.z);
+      const float denom = s_out.z;                         // plane z = 0, normal +z
+      if (fabsf(denom) < 1e-14f)
+        continue;
+      const float Lp = -pz / denom;
+      if (!(Lp > 0.f))
+        continue;
+      const float tau = sc.n_layers == 1
+          ? mu_t1 * Lp
+          : (float)est_optical_depth(sc, v.pos, v3<double>(bin.x, bin.y, bin.z), (double)Lp);
+      const float Tr = expf(-tau);
+      if (Tr < 1e-20f)
+        continue;
+      // |s_cur x s_out| = sin(theta_scat) of the two unit vectors; its direction is the
+      // scattering plane's normal p_hat (vcross_unit, src/vec.cpp:14-26)
+      const V3<float> pv = {s_cur.y * s_out.z - s_cur.z * s_out.y, s_cur.z * s_out.x - s_cur.x * s_out.z,
+                            s_cur.x * s_out.y - s_cur.y * s_out.x};
+      const float pn = sqrtf(vdot(pv, pv));
+      if (!(pn > 0.f))
+        continue;
+      const V3<float> p_hat = vscale(pv, 1.f / pn);
+      const float sin_phi = -vdot(m_cur, p_hat);
+      const float cos_phi = vdot(n_cur, p_hat);
+      const float cdot = vdot(s_cur, s_out);
+      const float th_scat = atan2f(pn, cdot);
+      Cx<float> S2, S1;
+      amplitudes<float>(med, th_scat, S2, S1);
+      const float s22 = cnorm(S2), s11 = cnorm(S1);
+      const float c2 = cos_phi * cos_phi, sn2 = sin_phi * sin_phi;
+      const float F = Emm * (s22 * c2 + s11 * sn2) + Enn * (s22 * sn2 + s11 * c2) +
+                      2.f * e12 * (s22 - s11) * sin_phi * cos_phi;
+      if (!(F > 0.f))
+        continue;
+      const float w_bin = pref * Tr * F * bin.w;
+      if (!(w_bin > 0.f))
+        continue;
+      const int t_idx = time_bin(s, t_launch + (v.opath + (double)Lp));
+      if (t_idx < 0)
+        continue;
+      const float amp = sqrtf(w_bin);
+      // exit frame A(theta, phi) P (src/detector.cpp:1027-1045): cos, sin of th_scat
+      const float ih = rsqrtf(cdot * cdot + pn * pn);
+      const float ct = cdot * ih, st = pn * ih;
+      float Pe[9];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const float mj = P[j], nj = P[3 + j], sj = P[6 + j];
+        Pe[j] = ct * cos_phi * mj + ct * sin_phi * nj - st * sj;
+        Pe[3 + j] = -sin_phi * mj + cos_phi * nj;
+        Pe[6 + j] = st * cos_phi * mj + st * sin_phi * nj + ct * sj;
+      }
+      // forward field (S R(phi)) E / sqrt(F) (src/detector.cpp:121-160)
+      const float inv = amp * rsqrtf(F);
+      const Cx<float> T00 = cscale(S2, cos_phi), T01 = cscale(S2, sin_phi);
+      const Cx<float> T10 = cscale(S1, -sin_phi), T11 = cscale(S1, cos_phi);
+      const Cx<float> Efm = cscale(cadd(cmul(T00, Em), cmul(T01, En)), inv);
+      const Cx<float> Efn = cscale(cadd(cmul(T10, Em), cmul(T11, En)), inv);
+      const Cx<float> Efx = cadd(cscale(Efm, Pe[0]), cscale(Efn, Pe[3]));
+      const Cx<float> Efy = cadd(cscale(Efm, Pe[1]), cscale(Efn, Pe[4]));
+      Cx<float> Erx = {0.f, 0.f}, Ery = {0.f, 0.f};
+      if (multi) {
+        Cx<float> Rm, Rn;
+        est_suffix<float>(sc, P1, Pe, v.first_med, pre_m, pre_n, Rm, Rn);
+        const float4 q = bf[2 * b + 1];
+        const float arg = q.x * dr[0] + q.y * dr[1] + q.z * dr[2];
+        float sp_, cp_;
+        sincosf(arg, &sp_, &cp_);
+        const Cx<float> pp = {cp_ * amp, sp_ * amp};
+        const Cx<float> Rm2 = cmul(Rm, pp), Rn2 = cmul(Rn, pp);
+        Erx = cadd(cscale(Rm2, Pe[0]), cscale(Rn2, Pe[3]));
+        Ery = cadd(cscale(Rm2, Pe[1]), cscale(Rn2, Pe[4]));
+      }
+      // accumulate_stokes (src/detector.cpp:1194-1226)
+      const Cx<float> Ex = cadd(Efx, Erx), Ey = cadd(Efy, Ery);
+      const Cx<float> c_xy = cmul(Ex, Cx<float>{Ey.re, -Ey.im});
+      const Cx<float> f_xy = cmul(Efx, Cx<float>{Efy.re, -Efy.im});
+      const Cx<float> r_xy = cmul(Erx, Cx<float>{Ery.re, -Ery.im});
+      const double c0 = cnorm(Ex) + cnorm(Ey), c1 = cnorm(Ex) - cnorm(Ey);
+      const double c2s = 2.0 * c_xy.re, c3 = 2.0 * c_xy.im;
+      const double i0 = cnorm(Efx) + cnorm(Efy) + cnorm(Erx) + cnorm(Ery);
+      const double i1 = cnorm(Efx) - cnorm(Efy) + cnorm(Erx) - cnorm(Ery);
+      const double i2 = 2.0 * ((double)f_xy.re + r_xy.re), i3 = 2.0 * ((double)f_xy.im + r_xy.im);
+      const unsigned long long cell = (unsigned long long)(b / s.N_phi) * s.N_phi + (b % s.N_phi);
+      add4(base, PS, cell, c0, c1, c2s, c3);
+      add4(base + 4 * PS, PS, cell, i0, i1, i2, i3);
+      if (t_idx >= 1) {
+        add4(base, PS, t_idx * tstride + cell, c0, c1, c2s, c3);
+        add4(base + 4 * PS, PS, t_idx * tstride + cell, i0, i1, i2, i3);
+      }
+    }
+    atomicAdd(s_hits + si, 1ull);
+  }
+}
+
 template <typename R>
 __device__ __forceinline__ void estimate_at_vertex(const Scene &sc, const RunParams &rp, const Photon<R> &ph,
                                                    const Side<R> &side, int med_idx, unsigned long long *s_hits)
@@ -1377,7 +1536,10 @@ __device__ __forceinline__ void estimate_at_vertex(const Scene &sc, const RunPar
   } else {
     v.T[0] = T0; v.T[1] = T1; v.T[2] = T2; v.T[3] = T3;
   }
-  estimate_vertex<R>(sc, rp, v, s_hits);
+  if (sizeof(R) == 4)
+    estimate_vertex_f32<R>(sc, rp, v, s_hits);
+  else
+    estimate_vertex<R>(sc, rp, v, s_hits);
 }
 
 // Sensor::check_conditions (src/detector.cpp:374-417)

@@ -638,6 +638,18 @@ void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned cha
       }
     }
     d.est_n = (int)bins.size();
+    // binary32 copy for binary32 transport, after the binary64 table: per bin
+    // (s_out, dOmega dphi) and the CBS wave vector q = k (s_out + s_in), formed here in
+    // binary64 (s_out + s_in cancels near back-scatter)
+    const size_t nb = bins.size();
+    bins.resize(nb + nb);                                    // 2 float4 = 1 double4 per bin
+    float4 *bf = reinterpret_cast<float4 *>(bins.data() + nb);
+    for (size_t k = 0; k < nb; ++k) {
+      const double4 q = bins[k];
+      bf[2 * k] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
+      bf[2 * k + 1] = make_float4((float)((q.x + s_in[0]) * sc.laser.k), (float)((q.y + s_in[1]) * sc.laser.k),
+                                  (float)((q.z + s_in[2]) * sc.laser.k), 0.0f);
+    }
     b.est_off[i] = bins.empty() ? 0 : put(bins.data(), bins.size() * sizeof(double4));
     b.has_est = true;
   }
