@@ -59,7 +59,7 @@ def parse():
                     help="timed steps of the FP64 and FP32+adjoint variants (0: skip them)")
     ap.add_argument("--variants", default="fp64,differentiable,sweep,estimator",
                     help="comma-separated subset of the variant arms to measure")
-    ap.add_argument("--estimator-photons", type=int, default=200_000,
+    ap.add_argument("--estimator-photons", type=int, default=1_000_000,
                     help="photons of the estimator-mode variant")
     ap.add_argument("--precision-report", action="store_true",
                     help="instead of timing: FP32 tallies against FP64 on the same random "

@@ -190,6 +190,10 @@ struct RunParams {
   unsigned long long *sweep_hits;
   // sweep with likelihood-ratio outputs: per-scene layouts (adj_K above is the largest K)
   const AdjScene *adj_scenes;
+  // estimator-mode FarFieldCBS grids accumulated per block in shared memory: sensor i's
+  // copy at est_smem[i] doubles into the block's grid area (-1: global atomics)
+  int est_smem[LMC_MAX_SENSORS];
+  int est_smem_doubles;
 };
 
 }  // namespace dev

@@ -283,6 +283,14 @@ template <typename R> struct Side {
   int first_med[kBlock];
 };
 
+// Dynamic shared memory of a transport block: the Side arrays, then (kAdj) the
+// likelihood-ratio scores, adj_K * kBlock R, or (estimator kernels) the block's copies
+// of the estimated grids, RunParams::est_smem_doubles doubles.
+template <typename R> __host__ __device__ constexpr size_t side_bytes()
+{
+  return (sizeof(Side<R>) + 15) & ~size_t(15);
+}
+
 struct Counters {
   uint32_t events, steps, draws;
 };
@@ -1212,7 +1220,7 @@ __device__ __forceinline__ double est_optical_depth(const Scene &sc, const doubl
 
 template <typename R>
 __device__ __noinline__ void estimate_vertex(const Scene &sc, const RunParams &rp, const EstVertex v,
-                                             unsigned long long *s_hits)
+                                             unsigned long long *s_hits, double *s_est)
 {
   const Laser &L = sc.laser;
   const V3<double> s_in = v3<double>(L.dir[0], L.dir[1], L.dir[2]);
@@ -1238,7 +1246,8 @@ __device__ __noinline__ void estimate_vertex(const Scene &sc, const RunParams &r
     if (multi)
       est_prefix(sc, v.P, v.T, v.med, pre_m, pre_n);
     const double t_launch = (s.dt > 0) ? emission_time<R>(L, rp, v.index) : 0.0;
-    double *base = rp.tallies + s.tally_off;
+    // the block's shared copy of the grid when it has one, else the tallies
+    double *base = rp.est_smem[si] >= 0 ? s_est + rp.est_smem[si] : rp.tallies + s.tally_off;
     const unsigned long long P = s.plane_stride;
     const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
     const int nb = s.est_n;
@@ -1352,7 +1361,7 @@ __device__ __noinline__ void estimate_vertex(const Scene &sc, const RunParams &r
 // phase q . (r_n - r_1) uses the table's q = k (s_out + s_in), formed in binary64.
 template <typename R>
 __device__ __noinline__ void estimate_vertex_f32(const Scene &sc, const RunParams &rp, const EstVertex v,
-                                                 unsigned long long *s_hits)
+                                                 unsigned long long *s_hits, double *s_est)
 {
   const Laser &L = sc.laser;
   float P[9], P1[9];
@@ -1392,7 +1401,7 @@ __device__ __noinline__ void estimate_vertex_f32(const Scene &sc, const RunParam
     const float pz = (float)v.pos[2];
     const float Emm = cnorm(Em), Enn = cnorm(En);
     const float e12 = Em.re * En.re + Em.im * En.im;
-    double *base = rp.tallies + s.tally_off;
+    double *base = rp.est_smem[si] >= 0 ? s_est + rp.est_smem[si] : rp.tallies + s.tally_off;
     const unsigned long long PS = s.plane_stride;
     const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
     const int nb = s.est_n;
@@ -1500,6 +1509,8 @@ template <typename R>
 __device__ __forceinline__ void estimate_at_vertex(const Scene &sc, const RunParams &rp, const Photon<R> &ph,
                                                    const Side<R> &side, int med_idx, unsigned long long *s_hits)
 {
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  double *s_est = reinterpret_cast<double *>(s_dyn + side_bytes<R>());
   const int tid = threadIdx.x;
   EstVertex v;
   v.pos[0] = ph.px; v.pos[1] = ph.py; v.pos[2] = ph.pz;
@@ -1537,9 +1548,9 @@ __device__ __forceinline__ void estimate_at_vertex(const Scene &sc, const RunPar
     v.T[0] = T0; v.T[1] = T1; v.T[2] = T2; v.T[3] = T3;
   }
   if (sizeof(R) == 4)
-    estimate_vertex_f32<R>(sc, rp, v, s_hits);
+    estimate_vertex_f32<R>(sc, rp, v, s_hits, s_est);
   else
-    estimate_vertex<R>(sc, rp, v, s_hits);
+    estimate_vertex<R>(sc, rp, v, s_hits, s_est);
 }
 
 // Sensor::check_conditions (src/detector.cpp:374-417)
@@ -2062,12 +2073,6 @@ __device__ __forceinline__ void load_scene(unsigned char *s_raw, const Scene *g_
 
 // kMinBlocks > 1 asks the compiler to fit that many 256-thread blocks per SM
 // (register cap 65536 / (256 kMinBlocks)); lmc_run picks the variant.
-// Dynamic shared memory of a transport block: the Side arrays, then (kAdj) the
-// likelihood-ratio scores, adj_K * kBlock R.
-template <typename R> __host__ __device__ constexpr size_t side_bytes()
-{
-  return (sizeof(Side<R>) + 15) & ~size_t(15);
-}
 
 // Scene of global photon g in a sweep: the s with prefix[s] <= g < prefix[s + 1].
 __device__ __forceinline__ int sweep_scene(const RunParams &rp, unsigned long long g)
@@ -2104,6 +2109,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
     s_hits[threadIdx.x] = 0;
   if (threadIdx.x < 7)
     s_fate[threadIdx.x] = 0;
+  double *s_est = reinterpret_cast<double *>(s_dyn + side_bytes<R>());
+  if (kEst)
+    for (int j = threadIdx.x; j < rp.est_smem_doubles; j += blockDim.x)
+      s_est[j] = 0.0;
   __syncthreads();
   const Scene *scp = kSweep ? g_scene : reinterpret_cast<const Scene *>(s_raw);
   const unsigned lane = threadIdx.x & 31u;
@@ -2180,6 +2189,19 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
                                                          : &rp.scratch->cap;
     atomicAdd(dst, s_fate[threadIdx.x]);
     atomicAdd(&rp.scratch->photons, s_fate[threadIdx.x]);
+  }
+  if (kEst && rp.est_smem_doubles > 0) {      // the block's estimated grids into the tallies
+    const Scene &sc = *scp;
+    for (int si = 0; si < sc.n_sensors; ++si) {
+      const int o = rp.est_smem[si];
+      if (o < 0)
+        continue;
+      const Sensor &s = sc.sensors[si];
+      const int n = (int)(8 * s.plane_stride);
+      for (int j = threadIdx.x; j < n; j += blockDim.x)
+        if (s_est[o + j] != 0.0)
+          atomicAdd(rp.tallies + s.tally_off + j, s_est[o + j]);
+    }
   }
 }
 

@@ -1016,6 +1016,26 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   const size_t rbytes = fp32 ? sizeof(float) : sizeof(double);
   size_t dyn_transport = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
   size_t dyn_tally = 0;
+  // estimator-mode grids: each block accumulates its vertices' estimates in a shared
+  // copy of the grid (one flush of non-zero cells per block), as long as they fit
+  for (int i = 0; i < LMC_MAX_SENSORS; ++i)
+    rp.est_smem[i] = -1;
+  if (est) {
+    constexpr size_t kEstSmemDoubles = (40u << 10) / sizeof(double);
+    size_t used = 0;
+    for (int i = 0; i < h->scene.n_sensors; ++i) {
+      const dev::Sensor &S = h->scene.sensors[i];
+      if (S.kind != LMC_SENSOR_FARFIELD_CBS || !S.estimator || S.est_n == 0)
+        continue;
+      const size_t n = h->sensor_count[i];
+      if (used + n > kEstSmemDoubles)
+        continue;
+      rp.est_smem[i] = (int)used;
+      used += n;
+    }
+    rp.est_smem_doubles = (int)used;
+    dyn_transport += used * sizeof(double);
+  }
   if (adj && sw) {
     size_t total = 0;
     int kmax = 0;
