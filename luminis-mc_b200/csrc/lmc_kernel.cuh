@@ -1293,10 +1293,10 @@ __device__ __noinline__ void estimate_vertex(const Scene &sc, const RunParams &r
       const int t_idx = time_bin(s, t_launch + (v.opath + Lp));
       if (t_idx < 0)
         continue;
-      double sa, ca;
-      sincos(L.k * Lp, &sa, &ca);
-      const double sw = sqrt(w_bin);
-      const Cx<double> amp = {sw * ca, sw * sa};
+      // amp = sqrt(w_bin) exp(i k L) in the reference (src/detector.cpp:1425, :1533); the
+      // phase multiplies the forward and the reverse field alike and cancels in every
+      // Stokes value, so only the modulus is formed
+      const Cx<double> amp = {sqrt(w_bin), 0.0};
       // exit frame A(theta, phi) P (src/detector.cpp:1027-1045)
       double st, ct;
       sincos(th_scat, &st, &ct);
