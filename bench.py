@@ -151,6 +151,18 @@ def reference_module():
     return lm
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the baseline's record."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def reference_sample(spec, seconds, threads):
     """Time the reference's run_simulation_parallel on a bounded photon sample sized
     for about `seconds` of work; returns (photons/s, photons, wall)."""
@@ -324,7 +336,11 @@ def run_ours(args):
             rate, n, dt = reference_sample(spec, args.cpu_seconds, threads)
             cpu = {"value": rate, "unit": "photons/s", "cores": threads, "kind": "reference",
                    "sample": f"{n} photons of {spec['name']} in {dt:.1f} s, reference "
-                             f"run_simulation_parallel (oracle/_ref/perf) with n_threads={threads}"}
+                             f"run_simulation_parallel (oracle/_ref/perf) with n_threads={threads}",
+                   "cpu_model": cpu_model()}
+            rate1, n1, dt1 = reference_sample(spec, 3.0, 1)
+            cpu["single_thread"] = {"value": rate1, "unit": "photons/s",
+                                    "sample": f"{n1} photons in {dt1:.1f} s, n_threads=1"}
         except Exception as exc:          # the reference build is optional on a GPU box
             cpu = {"value": None, "unit": "photons/s", "cores": os.cpu_count(),
                    "kind": "reference", "sample": f"unavailable: {exc}"}
