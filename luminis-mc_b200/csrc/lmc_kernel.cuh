@@ -1992,21 +1992,25 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
     side.rn[0][tid] = ph.px; side.rn[1][tid] = ph.py; side.rn[2][tid] = ph.pz;
     ph.last_med = med_idx;
     if (evt >= 3) {
-      // T <- normalise(J_{n-1} T), J_{n-1} = diag(S2, S1) R(phi) of the previous event
+      // T <- J_{n-1} T, J_{n-1} = diag(S2, S1) R(phi) of the previous event: the real
+      // rotation first, then the rows scaled by S2 and S1.  The reference renormalises
+      // T (Frobenius) at every event only to stay in range; every use of T ends in a
+      // normalised field, so its scale is free, and every fourth event suffices for
+      // binary32's range (|S| products over three events stay far inside it).
       const Cx<R> pS2 = {side.last[0][tid], side.last[1][tid]};
       const Cx<R> pS1 = {side.last[2][tid], side.last[3][tid]};
       const R pc = side.last[4][tid], ps = side.last[5][tid];
-      const Cx<R> B00 = cscale(pS2, pc), B01 = cscale(pS2, ps), B10 = cscale(pS1, -ps), B11 = cscale(pS1, pc);
       const Cx<R> T0 = {side.T[0][tid], side.T[1][tid]}, T1 = {side.T[2][tid], side.T[3][tid]};
       const Cx<R> T2 = {side.T[4][tid], side.T[5][tid]}, T3 = {side.T[6][tid], side.T[7][tid]};
-      Cx<R> t0 = cadd(cmul(B00, T0), cmul(B01, T2));
-      Cx<R> t1 = cadd(cmul(B00, T1), cmul(B01, T3));
-      Cx<R> t2 = cadd(cmul(B10, T0), cmul(B11, T2));
-      Cx<R> t3 = cadd(cmul(B10, T1), cmul(B11, T3));
-      const R frob = m_sqrt(cnorm(t0) + cnorm(t1) + cnorm(t2) + cnorm(t3));
-      if (frob > tiny<R>()) {
-        const R inv = R(1) / frob;
-        t0 = cscale(t0, inv); t1 = cscale(t1, inv); t2 = cscale(t2, inv); t3 = cscale(t3, inv);
+      const Cx<R> u0 = cadd(cscale(T0, pc), cscale(T2, ps)), u1 = cadd(cscale(T1, pc), cscale(T3, ps));
+      const Cx<R> u2 = cadd(cscale(T2, pc), cscale(T0, -ps)), u3 = cadd(cscale(T3, pc), cscale(T1, -ps));
+      Cx<R> t0 = cmul(pS2, u0), t1 = cmul(pS2, u1), t2 = cmul(pS1, u2), t3 = cmul(pS1, u3);
+      if ((evt & 3u) == 0u) {
+        const R frob = m_sqrt(cnorm(t0) + cnorm(t1) + cnorm(t2) + cnorm(t3));
+        if (frob > tiny<R>()) {
+          const R inv = R(1) / frob;
+          t0 = cscale(t0, inv); t1 = cscale(t1, inv); t2 = cscale(t2, inv); t3 = cscale(t3, inv);
+        }
       }
       side.T[0][tid] = t0.re; side.T[1][tid] = t0.im; side.T[2][tid] = t1.re; side.T[3][tid] = t1.im;
       side.T[4][tid] = t2.re; side.T[5][tid] = t2.im; side.T[6][tid] = t3.re; side.T[7][tid] = t3.im;
