@@ -276,7 +276,8 @@ template <typename R> struct Photon {
 template <typename R> struct Side {
   R first[12][kBlock];         // r_1 (3), then P1 rows m_1, n_1, s_1 (9)
   R last[6][kBlock];           // S2, S1 (re, im) and cos, sin(phi) of the newest scatter
-  R pn1[9][kBlock];            // frame before the newest scatter (P_{n-1})
+  R ang[4][kBlock];            // cos, sin theta and cos, sin phi of the newest scatter:
+                               // P_{n-1} = A^T P_n when a hit needs it (prev_frame)
   R rn[3][kBlock];             // position of the newest scatter (r_n)
   R T[8][kBlock];              // matrix_T_raw: normalised interior Jones product (re, im)
   uint32_t ring[kRing][kBlock];  // the photon's generated Philox words (see RngT)
@@ -1581,6 +1582,29 @@ __device__ __forceinline__ bool check_conditions(const Sensor &s, double hx, dou
   return true;
 }
 
+// The frame before the newest scatter, P_{n-1} = A(theta_n, phi_n)^T P_n (A is a
+// rotation), from the newest scatter's angles; the launch frame before any scatter.
+template <typename R>
+__device__ __forceinline__ void prev_frame(const Photon<R> &ph, const Side<R> &side, R *out)
+{
+  const int tid = threadIdx.x;
+  if (ph.events == 0) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j)
+      out[j] = ph.P[j];
+    return;
+  }
+  const R ct = side.ang[0][tid], st = side.ang[1][tid];
+  const R cp = side.ang[2][tid], sp = side.ang[3][tid];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const R m = ph.P[j], n = ph.P[3 + j], s = ph.P[6 + j];
+    out[j] = ct * cp * m - sp * n + st * cp * s;
+    out[3 + j] = ct * sp * m + cp * n + st * sp * s;
+    out[6 + j] = -st * m + ct * s;
+  }
+}
+
 template <typename R>
 __device__ __forceinline__ void fill_hit(const Photon<R> &ph, const Side<R> &side, R hx, R hy, R hz,
                                          double opath, HitData<R> &h)
@@ -1599,8 +1623,8 @@ __device__ __forceinline__ void fill_hit(const Photon<R> &ph, const Side<R> &sid
   for (int j = 0; j < 9; ++j) {
     h.P[j] = ph.P[j];
     h.P1[j] = side.first[3 + j][tid];
-    h.Pn1[j] = side.pn1[j][tid];
   }
+  prev_frame<R>(ph, side, h.Pn1);
   h.Em = ph.Em;
   h.En = ph.En;
 #pragma unroll
@@ -1662,10 +1686,12 @@ __device__ __forceinline__ void enqueue_hit(const Scene &sc, const RunParams &rp
       r[(kQR1 + j) * C + slot] = side.first[j][tid];
       r[(kQRn + j) * C + slot] = side.rn[j][tid];
     }
+    R pn1[9];
+    prev_frame<R>(ph, side, pn1);
 #pragma unroll
     for (int j = 0; j < 9; ++j) {
       r[(kQP1 + j) * C + slot] = side.first[3 + j][tid];
-      r[(kQPn1 + j) * C + slot] = side.pn1[j][tid];
+      r[(kQPn1 + j) * C + slot] = pn1[j];
     }
 #pragma unroll
     for (int qd = 0; qd < 4; ++qd) {
@@ -1750,11 +1776,8 @@ __device__ void init_photon(const Scene &sc, const RunParams &rp, Photon<R> &ph,
   ph.scene = 0;
   ph.layer = layer_index_at<R>(sc, ph.pz);
   ph.last_med = 0;
-  const int tid = threadIdx.x;                              // r_1 = r_n = launch, P1 = Pn1 = P0
+  const int tid = threadIdx.x;                              // r_1 = r_n = launch, P1 = P0
   side.rn[0][tid] = ph.px; side.rn[1][tid] = ph.py; side.rn[2][tid] = ph.pz;
-#pragma unroll
-  for (int j = 0; j < 9; ++j)
-    side.pn1[j][tid] = ph.P[j];
 #pragma unroll
   for (int q = 0; q < 8; ++q)
     side.T[q][tid] = R(q == 0 || q == 6 ? 1 : 0);
@@ -1956,11 +1979,12 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   if (kAdj)
     flight_event<R>(sc, fl, med_idx, ct);
   // frame update P <- A(theta, phi) P (src/simulation.cpp:438-453); P_{n-1} <- old P
-  if (rp.track_reverse) {
+  if (rp.track_reverse) {              // the newest scatter's angles (P_{n-1} = A^T P_n)
     const int tid = threadIdx.x;
-#pragma unroll
-    for (int j = 0; j < 9; ++j)
-      side.pn1[j][tid] = ph.P[j];
+    side.ang[0][tid] = ct;
+    side.ang[1][tid] = st;
+    side.ang[2][tid] = cp;
+    side.ang[3][tid] = sp;
   }
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
