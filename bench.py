@@ -304,7 +304,7 @@ def run_ours(args):
     # end-to-end through the public API: host tally arrays, copies inside
     e2e = None
     if not args.no_e2e:
-        e2e_ms = []
+        e2e_ms, e2e_device_ms = [], []
         cfg2, h2, keep2 = W.build(lm, spec)
         tally_bytes = run.transport.tally_size * 8
         table_bytes = 0
@@ -315,19 +315,27 @@ def run_ours(args):
             if v is not None:
                 table_bytes += 2 * v.nbytes
         for k in range(2):
+            # every timed call uploads its scene's tables: the scene the public API keeps
+            # between calls is released first (outside the timed region)
+            lm.release_gpu_cache()
+            torch.cuda.synchronize()
             barrier()
             t0 = time.perf_counter()
             cfg2.seed = seed + 77 + k
             lm.run_simulation_parallel(cfg2, precision=args.precision)
             torch.cuda.synchronize()
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            e2e_device_ms.append(lm.last_run_stats()["kernel_ms"])
+        lm.release_gpu_cache()
         worst = torch.tensor([max(e2e_ms)], dtype=torch.float64, device=f"cuda:{local}")
         if dist is not None:
             dist.all_reduce(worst, op=dist.ReduceOp.MAX)
         e2e = {"value": P * world / (float(worst.item()) * 1e-3), "unit": "photons/s",
-               "h2d_bytes_per_step": int(tally_bytes + table_bytes),
+               "h2d_bytes_per_step": int(table_bytes),
                "d2h_bytes_per_step": int(tally_bytes + 256),
-               "path": "luminis_mc_b200.run_simulation_parallel(config) with numpy tallies"}
+               "path": "luminis_mc_b200.run_simulation_parallel(config) with numpy tallies",
+               "calls_ms": {"wall": [round(x, 2) for x in e2e_ms],
+                            "device": [round(x, 2) for x in e2e_device_ms]}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

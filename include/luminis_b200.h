@@ -209,7 +209,8 @@ typedef struct lmc_run_opts {
   uint64_t batch_photons;       /* photons per transport batch (hit-queue mode); 0: 8M */
   int stream_format;            /* 0: u24 for FP32, u53 for FP64; 1: u24 for both (an FP64
                                    run on the FP32 run's numbers: precision alone)      */
-  int pad;
+  int host_tallies_zero;        /* lmc_run_host only: the caller's host tallies are all zero,
+                                   so the device copy is cleared instead of uploaded     */
 } lmc_run_opts;
 
 /* Final state of one photon, written when opts.records is set (the same layout as

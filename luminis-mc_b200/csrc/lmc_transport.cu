@@ -1529,7 +1529,9 @@ lmc_status lmc_run_host(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uin
     h->host_tally_cap = bytes;
   }
   cudaStream_t stream = opts && opts->stream ? static_cast<cudaStream_t>(opts->stream) : h->stream;
-  if (bytes)
+  if (bytes && opts && opts->host_tallies_zero)
+    LMC_CUDA(cudaMemsetAsync(h->d_host_tally, 0, bytes, stream));
+  else if (bytes)
     LMC_CUDA(cudaMemcpyAsync(h->d_host_tally, h_tallies, bytes, cudaMemcpyHostToDevice, stream));
   lmc_stats local;
   const lmc_status st = lmc_run(h, seed, photon_begin, n_photons, opts, h->d_host_tally,

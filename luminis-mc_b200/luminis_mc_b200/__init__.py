@@ -20,7 +20,7 @@ from .simulation import (FarFieldCBSProcessed, PlanarFieldProcessed,  # noqa: F4
                          PlanarFluenceProcessed, SimConfig, StokesMatrixProcessed, Transport,
                          last_run_stats, postprocess_farfield_cbs, postprocess_farfield_fluence,
                          postprocess_planar_field, postprocess_planar_fluence,
-                         run_simulation_parallel, validate_sim_config)
+                         release_gpu_cache, run_simulation_parallel, validate_sim_config)
 
 # enum values exported at module level, as pybind's export_values() does
 Point, Uniform, Gaussian = LaserSource.Point, LaserSource.Uniform, LaserSource.Gaussian

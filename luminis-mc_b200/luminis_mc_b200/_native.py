@@ -101,7 +101,7 @@ class RunOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("max_events", C.c_int), ("track_reverse_paths", C.c_int),
                 ("block_size", C.c_int), ("blocks_per_sm", C.c_int), ("records", C.c_void_p),
                 ("stream", C.c_void_p), ("batch_photons", C.c_uint64),
-                ("stream_format", C.c_int), ("pad", C.c_int)]
+                ("stream_format", C.c_int), ("host_tallies_zero", C.c_int)]
 
 
 class Stats(C.Structure):

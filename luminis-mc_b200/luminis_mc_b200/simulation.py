@@ -9,9 +9,12 @@ through the C ABI (include/luminis_b200.h); there is no CPU fallback.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
+import hashlib
 import math
 import random
+import threading
 
 import numpy as np
 
@@ -223,9 +226,9 @@ class Transport:
     to run repeatedly (tallies stay on the device between ``run_device`` calls).
     """
 
-    def __init__(self, config: SimConfig):
+    def __init__(self, config: SimConfig, desc=None):
         self.config = config
-        self.scene, self._keep, self.sensors = scene_desc(config)
+        self.scene, self._keep, self.sensors = scene_desc(config) if desc is None else desc
         h = C.c_void_p()
         N.check(N.lib().lmc_create(C.byref(self.scene), C.byref(h)))
         self._h = h
@@ -259,7 +262,7 @@ class Transport:
 
     def opts(self, precision="fp32", max_events=None, track_reverse_paths=None, block_size=0,
              blocks_per_sm=0, records_ptr=None, stream=None, batch_photons=0,
-             stream_format=0) -> N.RunOpts:
+             stream_format=0, host_tallies_zero=False) -> N.RunOpts:
         if precision not in N.PRECISION:
             raise ValueError("precision must be 'fp32' or 'fp64'")
         c = self.config
@@ -274,6 +277,7 @@ class Transport:
         o.stream = stream
         o.batch_photons = int(batch_photons)
         o.stream_format = int(stream_format)
+        o.host_tallies_zero = int(bool(host_tallies_zero))
         return o
 
     def run_host(self, tallies: np.ndarray, n_photons: int, seed: int, begin: int = 0,
@@ -330,20 +334,58 @@ def run_simulation_parallel(config: SimConfig, *, precision: str = "fp32", block
     """
     global _last_stats
     validate_sim_config(config)
-    t = Transport(config)
-    try:
+    desc = scene_desc(config)
+    with _cache_lock:
+        t = _cached_transport(config, desc)
         flat = np.zeros(t.tally_size)
         stats = t.run_host(flat, int(config.n_photons), int(config.seed), 0,
                            precision=precision, block_size=block_size,
-                           blocks_per_sm=blocks_per_sm)
-        for i, (s, (off, cnt, _)) in enumerate(zip(t.sensors, t.layout)):
-            s._tally += flat[off:off + cnt]
-            s.hits += stats["hits"][i]
-        if config.absorption is not None:                 # src/simulation.cpp:237-242
-            config.absorption._add(t.absorption_grid(flat))
-        _last_stats = stats
-    finally:
-        t.close()
+                           blocks_per_sm=blocks_per_sm, host_tallies_zero=True,
+                           max_events=int(config.MAX_EVENTS),
+                           track_reverse_paths=bool(config.track_reverse_paths))
+    for i, (s, (off, cnt, _)) in enumerate(zip(desc[2], t.layout)):
+        s._tally += flat[off:off + cnt]
+        s.hits += stats["hits"][i]
+    if config.absorption is not None:                     # src/simulation.cpp:237-242
+        config.absorption._add(t.absorption_grid(flat))
+    _last_stats = stats
+
+
+# One created scene is kept between run_simulation_parallel calls: a call whose scene
+# (every parameter and table) equals the previous call's reuses its device tables, hit
+# queue and tally buffer instead of allocating and freeing them again.  It holds that
+# device memory until a call with another scene, release_gpu_cache() or exit.
+_cache_lock = threading.Lock()
+_cache: list = []                    # [digest, Transport] of the last scene
+
+
+def _scene_digest(desc) -> bytes:
+    sc, keep, _ = desc
+    h = hashlib.blake2b(bytes(sc), digest_size=32)
+    for a in keep:
+        if isinstance(a, np.ndarray):
+            h.update(np.ascontiguousarray(a).view(np.uint8).tobytes())
+    return h.digest()
+
+
+def _cached_transport(config: SimConfig, desc) -> "Transport":
+    digest = _scene_digest(desc)
+    if _cache and _cache[0] == digest:
+        return _cache[1]
+    release_gpu_cache()
+    t = Transport(config, desc)
+    _cache[:] = [digest, t]
+    return t
+
+
+def release_gpu_cache() -> None:
+    """Free the device memory run_simulation_parallel keeps for its last scene."""
+    if _cache:
+        _cache[1].close()
+        _cache.clear()
+
+
+atexit.register(release_gpu_cache)
 
 
 # --------------------------------------------------------------------- post-processing

@@ -188,6 +188,59 @@ def test_public_api_matches_oracle(cuda):
         assert h.hits == 2 * ref.hits[i]
 
 
+def test_public_api_scene_kept_between_calls(cuda):
+    """The scene run_simulation_parallel keeps between calls: alternating scenes, a
+    changed photon budget and MAX_EVENTS on an unchanged scene, and a changed laser
+    each give the tallies of a fresh call."""
+    def fresh(spec, **cfg_kw):
+        lm.release_gpu_cache()
+        cfg, hs, keep = W.build(lm, spec)
+        for k, v in cfg_kw.items():
+            setattr(cfg, k, v)
+        lm.run_simulation_parallel(cfg, precision="fp64")
+        return [W.tally_arrays(h, s["kind"]).copy() for h, s in zip(hs, spec["sensors"])]
+
+    a, b = W.bilayer_rgd_mie(1500, 31), W.mie_cbs_small(1500, 32)
+    want_a, want_b = fresh(a), fresh(b)
+    want_a_short = fresh(a, MAX_EVENTS=7)
+    cfg_a, hs_a, keep_a = W.build(lm, a)
+    cfg_b, hs_b, keep_b = W.build(lm, b)
+    lm.release_gpu_cache()
+    for cfg in (cfg_a, cfg_b, cfg_a):
+        lm.run_simulation_parallel(cfg, precision="fp64")
+    for h, s, w in zip(hs_a, a["sensors"], want_a):
+        np.testing.assert_allclose(W.tally_arrays(h, s["kind"]), 2 * w, rtol=1e-12,
+                                   atol=1e-12 * np.abs(w).max())
+    for h, s, w in zip(hs_b, b["sensors"], want_b):
+        np.testing.assert_allclose(W.tally_arrays(h, s["kind"]), w, rtol=1e-12,
+                                   atol=1e-12 * np.abs(w).max())
+    cfg_a, hs_a, keep_a = W.build(lm, a)
+    lm.run_simulation_parallel(cfg_a, precision="fp64")
+    cfg_a.MAX_EVENTS = 7
+    before = [W.tally_arrays(h, s["kind"]).copy() for h, s in zip(hs_a, a["sensors"])]
+    lm.run_simulation_parallel(cfg_a, precision="fp64")
+    for h, s, w, b0 in zip(hs_a, a["sensors"], want_a_short, before):
+        np.testing.assert_allclose(W.tally_arrays(h, s["kind"]) - b0, w, rtol=1e-9,
+                                   atol=1e-12 * max(np.abs(w).max(), 1.0))
+    cfg_a.MAX_EVENTS = a.get("max_events", cfg_a.MAX_EVENTS)
+    cfg_a.laser.position = lm.Vec3(0.3, -0.2, 1e-9)
+    lm.run_simulation_parallel(cfg_a, precision="fp64")
+    spec = dict(a)
+    got = [W.tally_arrays(h, s["kind"]).copy() for h, s in zip(hs_a, a["sensors"])]
+    lm.release_gpu_cache()
+    cfg_c, hs_c, keep_c = W.build(lm, spec)
+    cfg_c.laser.position = lm.Vec3(0.3, -0.2, 1e-9)
+    lm.run_simulation_parallel(cfg_c, precision="fp64")
+    moved = False
+    for g, h, s, b0, w, w0 in zip(got, hs_c, a["sensors"], before, want_a_short, want_a):
+        shifted = W.tally_arrays(h, s["kind"])
+        np.testing.assert_allclose(g - b0 - w, shifted, rtol=1e-9,
+                                   atol=1e-9 * max(np.abs(g).max(), 1.0))
+        moved |= not np.allclose(shifted, w0)
+    assert moved, "moving the source must change the tallies"
+    lm.release_gpu_cache()
+
+
 def test_device_then_host_run_on_one_handle(cuda):
     """lmc_run (grows the hit queue) followed by lmc_run_host on the same handle:
     the host path's staging buffer must not disturb the queue the next run reuses."""
