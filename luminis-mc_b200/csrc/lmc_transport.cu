@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "lmc_device.cuh"
@@ -1511,6 +1512,88 @@ lmc_status lmc_adjoint_contract(const double *d_adjoint, const double *d_grad_ou
   return LMC_OK;
 }
 
+}  // extern "C"
+
+namespace lmc {
+namespace {
+
+// lmc_run_host reads its tallies back through two pinned 16 MiB halves shared by every
+// handle of the process (allocated on first use, kept until exit): the copy engine fills
+// one half while host threads move the other into the caller's pageable buffer.
+constexpr size_t kStageBytes = size_t(16) << 20;
+std::mutex g_stage_mutex;
+unsigned char *g_stage = nullptr;
+
+struct StageEvents {
+  cudaEvent_t e[2] = {nullptr, nullptr};
+  cudaError_t create()
+  {
+    for (cudaEvent_t &x : e) {
+      const cudaError_t r = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+      if (r != cudaSuccess)
+        return r;
+    }
+    return cudaSuccess;
+  }
+  ~StageEvents()
+  {
+    for (cudaEvent_t x : e)
+      if (x)
+        cudaEventDestroy(x);
+  }
+};
+
+// memcpy split over up to 8 host threads (2 MiB or more each).
+void parallel_copy(unsigned char *dst, const unsigned char *src, size_t bytes)
+{
+  constexpr size_t kMinPart = size_t(2) << 20;
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t n = std::min<size_t>(std::min<size_t>(hw, 8), (bytes + kMinPart - 1) / kMinPart);
+  if (n <= 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t part = ((bytes + n - 1) / n + 63) & ~size_t(63);
+  std::vector<std::thread> pool;
+  for (size_t i = 1; i < n && i * part < bytes; ++i)
+    pool.emplace_back([=] { std::memcpy(dst + i * part, src + i * part, std::min(part, bytes - i * part)); });
+  std::memcpy(dst, src, std::min(part, bytes));
+  for (std::thread &t : pool)
+    t.join();
+}
+
+// Device tallies -> caller's host buffer, chunk by chunk through the pinned halves.
+lmc_status read_back(double *h_dst, const double *d_src, size_t bytes, cudaStream_t stream)
+{
+  std::lock_guard<std::mutex> lock(g_stage_mutex);
+  if (!g_stage)
+    LMC_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&g_stage), 2 * kStageBytes, cudaHostAllocPortable));
+  StageEvents ev;
+  LMC_CUDA(ev.create());
+  const unsigned char *src = reinterpret_cast<const unsigned char *>(d_src);
+  unsigned char *dst = reinterpret_cast<unsigned char *>(h_dst);
+  const size_t n_chunks = (bytes + kStageBytes - 1) / kStageBytes;
+  auto chunk_len = [&](size_t k) { return std::min(kStageBytes, bytes - k * kStageBytes); };
+  auto issue = [&](size_t k) {
+    cudaError_t e = cudaMemcpyAsync(g_stage + (k & 1) * kStageBytes, src + k * kStageBytes,
+                                    chunk_len(k), cudaMemcpyDeviceToHost, stream);
+    return e == cudaSuccess ? cudaEventRecord(ev.e[k & 1], stream) : e;
+  };
+  LMC_CUDA(issue(0));
+  for (size_t k = 0; k < n_chunks; ++k) {
+    LMC_CUDA(cudaEventSynchronize(ev.e[k & 1]));
+    if (k + 1 < n_chunks)           // the other half was emptied in the previous iteration
+      LMC_CUDA(issue(k + 1));
+    parallel_copy(dst + k * kStageBytes, g_stage + (k & 1) * kStageBytes, chunk_len(k));
+  }
+  return LMC_OK;
+}
+
+}  // namespace
+}  // namespace lmc
+
+extern "C" {
+
 lmc_status lmc_run_host(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
                         const lmc_run_opts *opts, double *h_tallies, lmc_stats *stats)
 {
@@ -1538,8 +1621,11 @@ lmc_status lmc_run_host(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uin
                                 stats ? stats : &local);
   if (st != LMC_OK)
     return st;
-  if (bytes)
-    LMC_CUDA(cudaMemcpyAsync(h_tallies, h->d_host_tally, bytes, cudaMemcpyDeviceToHost, stream));
+  if (bytes) {
+    const lmc_status rb = read_back(h_tallies, h->d_host_tally, bytes, stream);
+    if (rb != LMC_OK)
+      return rb;
+  }
   LMC_CUDA(cudaStreamSynchronize(stream));
   return LMC_OK;
 }

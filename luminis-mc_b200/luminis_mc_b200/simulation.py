@@ -337,7 +337,7 @@ def run_simulation_parallel(config: SimConfig, *, precision: str = "fp32", block
     desc = scene_desc(config)
     with _cache_lock:
         t = _cached_transport(config, desc)
-        flat = np.zeros(t.tally_size)
+        flat = np.empty(t.tally_size)       # overwritten: the device tallies start at zero
         stats = t.run_host(flat, int(config.n_photons), int(config.seed), 0,
                            precision=precision, block_size=block_size,
                            blocks_per_sm=blocks_per_sm, host_tallies_zero=True,
