@@ -436,6 +436,27 @@ typedef enum lmc_amp_kind { LMC_AMP_RGD = 0, LMC_AMP_MIE = 1 } lmc_amp_kind;
 LMC_API lmc_status lmc_amplitude_table(int kind, double radius, double n_particle, double n_medium,
                                double wavelength, int n, double *s1, double *s2);
 
+/* One Mie species of a batched table build: MiePhaseFunction(wavelength, radius,
+ * n_particle, n_medium, ...) with MieMedium(phase, radius, n_particle, n_medium, wavelength). */
+typedef struct lmc_mie_species {
+  double wavelength, radius, n_particle, n_medium;
+} lmc_mie_species;
+
+/* The set-up tables of n Mie species built together on the current CUDA device, bit for bit
+ * the numbers the per-species calls give:
+ *   values[n_div + 1]          sampling nodes min_val + i (max_val - min_val) / n_div (shared)
+ *   cdf[n][n_div + 1]          lmc_sampling_table(LMC_PDF_MIE, n_div, min_val, max_val)
+ *   sigma[n]                   lmc_phase_cross_section(LMC_PDF_MIE)
+ *   s1[n][2 n_amp], s2[...]    lmc_amplitude_table(LMC_AMP_MIE, n_amp), interleaved re/im
+ * All are host arrays.  values/cdf/sigma may be null together (n_div ignored), s1/s2 may be
+ * null together or n_amp 0 (no amplitude tables).  The Mie coefficient recurrence runs on
+ * the host; the angular sums, the PDF and the CDF on the GPU.  Replaces the per-species
+ * construction of MiePhaseFunction (src/phase.cpp:244-304, src/table.cpp:6-48) and
+ * MieMedium (src/medium.cpp:160-236) around MIEV0 (src/mie/MIEV0noP.f). */
+LMC_API lmc_status lmc_mie_tables(const lmc_mie_species *species, int n, int n_div,
+                                  double min_val, double max_val, int n_amp, double *values,
+                                  double *cdf, double *sigma, double *s1, double *s2);
+
 /* ---- measurement --------------------------------------------------------------------- */
 
 /* Measured FP32 FMA issue rate of the current GPU (TFLOP/s, 2 flops per FMA): the

@@ -1,7 +1,9 @@
 // lmc_internal.h -- shared host-side helpers of libluminis_b200 (not installed).
 #pragma once
+#include <complex>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "luminis_b200.h"
 
@@ -21,5 +23,20 @@ inline lmc_status fail(lmc_status code, const std::string &msg)
   last_error() = msg;
   return code;
 }
+
+// The Mie series of one size parameter in the form the angular sums consume:
+// ap[n-1] = (2n+1)/(n(n+1)) (a_n + b_n), bp[n-1] = (2n+1)/(n(n+1)) (a_n - b_n), or the
+// small-particle limit's three coefficients (ntrm == 0).  Same numbers as the per-angle
+// evaluation in lmc_mie / lmc_amplitude_table / lmc_sampling_table.
+struct MieSeries {
+  int ntrm = 0;
+  bool conj_out = false;
+  double small_rtmp = 0.0;
+  std::complex<double> small_a1, small_a2, small_b1;
+  std::vector<std::complex<double>> ap, bp;
+  double qsca = 0.0;
+};
+
+bool mie_series(double x, double m_re, double m_im, MieSeries &out);
 
 }  // namespace lmc

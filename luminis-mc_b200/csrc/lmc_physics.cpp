@@ -268,6 +268,33 @@ double rdemc_cross_section(const lmc_phase_params &p)
 
 }  // namespace
 
+bool lmc::mie_series(double x, double m_re, double m_im, MieSeries &out)
+{
+  MieCoefficients c;
+  if (!mie_coefficients(x, cd(m_re, m_im), true, c))
+    return false;
+  out.conj_out = c.conj_out;
+  out.qsca = c.qsca;
+  if (c.small) {
+    out.ntrm = 0;
+    out.small_rtmp = c.small_rtmp;
+    out.small_a1 = c.small_a1;
+    out.small_a2 = c.small_a2;
+    out.small_b1 = c.small_b1;
+    return true;
+  }
+  out.ntrm = c.ntrm;
+  out.ap.resize(c.ntrm);
+  out.bp.resize(c.ntrm);
+  for (int n = 1; n <= c.ntrm; ++n) {           // as in mie_amplitudes
+    const double fn = n;
+    const double coeff = (2 * n + 1) / (fn * (n + 1));
+    out.ap[n - 1] = coeff * (c.an[n] + c.bn[n]);
+    out.bp[n - 1] = coeff * (c.an[n] - c.bn[n]);
+  }
+  return true;
+}
+
 extern "C" {
 
 lmc_status lmc_mie(double x, double m_re, double m_im, int n, const double *mu, double *s1,

@@ -9,6 +9,7 @@ the reference does.
 from .core import (Absorption, CMatrix, CrossingDirection, CVec2, DrainePhaseFunction,  # noqa: F401
                    FarFieldCBSSensor, FarFieldFluenceSensor, HenyeyGreensteinPhaseFunction, Laser,
                    LaserSource, Layer, LogLevel, Matrix, MiePhaseFunction, MieMedium, MixtureLayer,
+                   mie_species,
                    PhaseFunction, PhotonRecordSensor, PlanarFieldSensor, PlanarFluenceSensor,
                    RayleighDebyeEMCPhaseFunction, RayleighDebyePhaseFunction,
                    RayleighPhaseFunction, RGDMedium, Rng, Sample, SampleLayer, ScatteringMedium,

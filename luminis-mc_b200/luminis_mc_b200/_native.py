@@ -133,6 +133,11 @@ class PhaseParams(C.Structure):
                 ("n_medium", C.c_double)]
 
 
+class MieSpecies(C.Structure):
+    _fields_ = [("wavelength", C.c_double), ("radius", C.c_double), ("n_particle", C.c_double),
+                ("n_medium", C.c_double)]
+
+
 # Per-photon record (same layout as lmc_record).
 RECORD_FIELDS = [("photon", "<u8"), ("events", "<u4"), ("draws", "<u4"), ("fate", "<i4"),
                  ("layer", "<i4"), ("weight", "<f8"), ("opticalpath", "<f8"),
@@ -148,7 +153,7 @@ EXPORTED = ["lmc_create", "lmc_destroy", "lmc_tally_layout", "lmc_run", "lmc_run
             "lmc_adjoint_layout", "lmc_run_adjoint", "lmc_adjoint_contract",
             "lmc_create_sweep", "lmc_sweep_layout", "lmc_sweep_set_photons", "lmc_run_sweep",
             "lmc_sweep_hits", "lmc_sweep_adjoint_layout", "lmc_run_sweep_adjoint",
-            "lmc_autotune"]
+            "lmc_autotune", "lmc_mie_tables"]
 
 _lib = None
 
@@ -193,6 +198,9 @@ def lib():
     L.lmc_amplitude_table.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                       C.c_int, dptr, dptr]
     L.lmc_amplitude_table.restype = C.c_int
+    L.lmc_mie_tables.argtypes = [C.POINTER(MieSpecies), C.c_int, C.c_int, C.c_double, C.c_double,
+                                 C.c_int, dptr, dptr, dptr, dptr, dptr]
+    L.lmc_mie_tables.restype = C.c_int
     L.lmc_probe_fp32_peak.argtypes = [C.c_int, dptr, dptr]
     L.lmc_probe_fp32_peak.restype = C.c_int
     L.lmc_run_noalloc.argtypes = [C.POINTER(SceneDesc), C.c_uint64, C.c_uint64, C.c_uint64,

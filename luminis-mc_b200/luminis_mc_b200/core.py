@@ -424,16 +424,19 @@ class MiePhaseFunction(_TablePhase):
     (src/phase.cpp:244-304)."""
 
     def __init__(self, wavelength, radius, n_particle, n_medium, nDiv, minVal, maxVal):
-        self.wavelength, self.radius = float(wavelength), float(radius)
-        self.n_particle, self.n_medium = float(n_particle), float(n_medium)
-        self.k = 2 * math.pi * self.n_medium / self.wavelength
-        self.m = complex(self.n_particle / self.n_medium, 0.0)
-        p = N.PhaseParams(kind=N.PDF_MIE, wavelength=wavelength, radius=radius,
-                          n_particle=n_particle, n_medium=n_medium)
+        p = self._set_particle(wavelength, radius, n_particle, n_medium)
         sig = np.zeros(1)
         N.check(N.lib().lmc_phase_cross_section(p, N.as_dptr(sig)))
         self._sigma = float(sig[0])
         self._build(p, nDiv, minVal, maxVal)
+
+    def _set_particle(self, wavelength, radius, n_particle, n_medium) -> N.PhaseParams:
+        self.wavelength, self.radius = float(wavelength), float(radius)
+        self.n_particle, self.n_medium = float(n_particle), float(n_medium)
+        self.k = 2 * math.pi * self.n_medium / self.wavelength
+        self.m = complex(self.n_particle / self.n_medium, 0.0)
+        return N.PhaseParams(kind=N.PDF_MIE, wavelength=wavelength, radius=radius,
+                             n_particle=n_particle, n_medium=n_medium)
 
     def scattering_cross_section(self):
         return self._sigma
@@ -513,6 +516,9 @@ class ScatteringMedium:
         s2 = np.zeros(2 * n)
         N.check(N.lib().lmc_amplitude_table(kind, self.radius, self.n_particle, self.n_medium,
                                             self.wavelength, n, N.as_dptr(s1), N.as_dptr(s2)))
+        self._set_amp(s1, s2, n)
+
+    def _set_amp(self, s1, s2, n):
         self._s1 = s1.view(np.complex128)
         self._s2 = s2.view(np.complex128)
         self._dtheta = math.pi / (n - 1)
@@ -533,13 +539,57 @@ class RGDMedium(ScatteringMedium):
 class MieMedium(ScatteringMedium):
     """Mie amplitudes on 1000 theta nodes at x = 2 pi r / lambda (src/medium.cpp:160-236)."""
 
+    N_AMP = 1000
+
     def __init__(self, phase_func, radius, n_particle, n_medium, wavelength):
-        super().__init__(phase_func)
+        self._set_particle(phase_func, radius, n_particle, n_medium, wavelength)
+        self._amp_table(N.AMP_MIE, self.N_AMP)
+
+    def _set_particle(self, phase_func, radius, n_particle, n_medium, wavelength):
+        ScatteringMedium.__init__(self, phase_func)
         self.radius, self.n_particle = float(radius), float(n_particle)
         self.n_medium, self.wavelength = float(n_medium), float(wavelength)
         self.m = complex(self.n_particle / self.n_medium, 0.0)
         self.k = 2 * math.pi * self.n_medium / self.wavelength
-        self._amp_table(N.AMP_MIE, 1000)
+
+
+def mie_species(species, nDiv=1000, minVal=0.0, maxVal=math.pi):
+    """Build many Mie species at once on the GPU (lmc_mie_tables).
+
+    ``species`` is a sequence of (wavelength, radius, n_particle, n_medium).  Returns one
+    (MiePhaseFunction(wavelength, radius, n_particle, n_medium, nDiv, minVal, maxVal),
+    MieMedium(phase, radius, n_particle, n_medium, wavelength)) pair per species, with
+    tables equal bit for bit to those the two constructors build one species at a time
+    (src/phase.cpp:244-304, src/medium.cpp:160-236).  Needs a CUDA device.
+    """
+    species = [tuple(float(v) for v in q) for q in species]
+    n = len(species)
+    if int(nDiv) <= 0:
+        raise ValueError("nDiv must be greater than 0")
+    if not float(minVal) < float(maxVal):
+        raise ValueError("minVal must be less than maxVal")
+    arr = (N.MieSpecies * max(n, 1))(*[N.MieSpecies(*q) for q in species])
+    n_amp = MieMedium.N_AMP
+    values = np.zeros(int(nDiv) + 1)
+    cdf = np.zeros((n, int(nDiv) + 1))
+    sigma = np.zeros(max(n, 1))
+    s1 = np.zeros((n, 2 * n_amp))
+    s2 = np.zeros((n, 2 * n_amp))
+    N.check(N.lib().lmc_mie_tables(arr, n, int(nDiv), float(minVal), float(maxVal), n_amp,
+                                   N.as_dptr(values), N.as_dptr(cdf), N.as_dptr(sigma),
+                                   N.as_dptr(s1), N.as_dptr(s2)))
+    out = []
+    for i, (wl, r, n_p, n_m) in enumerate(species):
+        ph = MiePhaseFunction.__new__(MiePhaseFunction)
+        ph._params = ph._set_particle(wl, r, n_p, n_m)
+        ph._sigma = float(sigma[i])
+        ph.nDiv, ph.minVal, ph.maxVal = int(nDiv), float(minVal), float(maxVal)
+        ph._values, ph._cdf = values.copy(), cdf[i]
+        med = MieMedium.__new__(MieMedium)
+        med._set_particle(ph, r, n_p, n_m, wl)
+        med._set_amp(s1[i], s2[i], n_amp)
+        out.append((ph, med))
+    return out
 
 
 # ------------------------------------------------------------------------------ sample

@@ -139,6 +139,27 @@ def mie_sweep(i, seed=12345, count=256):
     return spec
 
 
+def build_mie_sweep(lm, specs):
+    """Configs of single-medium Mie sweep specs (``mie_sweep``) whose phase functions and
+    media are built together by ``lm.mie_species`` (one GPU batch) instead of one by one."""
+    keys = []
+    for sp in specs:
+        p, m = sp["phases"][0], sp["media"][0]
+        if len(sp["phases"]) != 1 or len(sp["media"]) != 1 or p["kind"] != "mie" or m["kind"] != "mie":
+            raise ValueError("build_mie_sweep takes single-medium Mie specs")
+        if (p["wavelength"], p["radius"], p["n_particle"], p["n_medium"]) != (
+                m["wavelength"], m["radius"], m["n_particle"], m["n_medium"]):
+            raise ValueError("phase function and medium must describe the same particle")
+        keys.append((p["nDiv"], p["min"], p["max"]))
+    if len(set(keys)) > 1:
+        raise ValueError("all phase tables of a batch share nDiv, minVal, maxVal")
+    n_div, lo, hi = keys[0] if keys else (1000, 0.0, PI)
+    pairs = lm.mie_species([(sp["phases"][0]["wavelength"], sp["phases"][0]["radius"],
+                             sp["phases"][0]["n_particle"], sp["phases"][0]["n_medium"])
+                            for sp in specs], n_div, lo, hi)
+    return [build(lm, sp, prebuilt=([ph], [med]))[0] for sp, (ph, med) in zip(specs, pairs)]
+
+
 def mixture_bilayer(n_photons=10_000_000, seed=12345):
     """A MixtureLayer of three co-located species -- polystyrene spheres r = 0.5 um
     (n = 3e6 /mm^3, mu_s_i ~ 6.1/mm) and r = 0.25 um (1.5e7 /mm^3, ~2.3/mm) and RGD
@@ -193,18 +214,25 @@ _PHASE_CTORS = {
 }
 
 
-def build(lm, spec, n_photons=None, seed=None, n_threads=None):
+def build(lm, spec, n_photons=None, seed=None, n_threads=None, prebuilt=None):
     """Build (config, sensor handles, keep-alive list) with the luminis-mc API of ``lm``.
 
     Sensors whose class ``lm`` does not define are skipped and reported as None.
+    ``prebuilt`` = (phases, media objects) replaces the per-object constructors (the
+    media's coefficients are still set from the spec).
     """
     keep = []
-    phases = [_PHASE_CTORS[p["kind"]](lm, p) for p in spec["phases"]]
+    phases = (list(prebuilt[0]) if prebuilt else
+              [_PHASE_CTORS[p["kind"]](lm, p) for p in spec["phases"]])
     keep += phases
     media = []
-    for m in spec["media"]:
-        cls = lm.MieMedium if m["kind"] == "mie" else lm.RGDMedium
-        med = cls(phases[m["phase"]], m["radius"], m["n_particle"], m["n_medium"], m["wavelength"])
+    for j, m in enumerate(spec["media"]):
+        if prebuilt:
+            med = prebuilt[1][j]
+        else:
+            cls = lm.MieMedium if m["kind"] == "mie" else lm.RGDMedium
+            med = cls(phases[m["phase"]], m["radius"], m["n_particle"], m["n_medium"],
+                      m["wavelength"])
         med.set_scattering_coefficient(m["mu_s"])
         med.set_absorption_coefficient(m["mu_a"])
         med.set_mean_free_path(m["mfp"])

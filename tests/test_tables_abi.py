@@ -33,9 +33,10 @@ def test_struct_layouts_match_ctypes():
 #include <stddef.h>
 #include "luminis_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(lmc_scene), sizeof(lmc_medium_desc),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(lmc_scene), sizeof(lmc_medium_desc),
          sizeof(lmc_sensor_desc), sizeof(lmc_laser_desc), sizeof(lmc_run_opts), sizeof(lmc_stats),
-         sizeof(lmc_record), offsetof(lmc_scene, sensors), offsetof(lmc_run_opts, batch_photons));
+         sizeof(lmc_record), offsetof(lmc_scene, sensors), offsetof(lmc_run_opts, batch_photons),
+         sizeof(lmc_mie_species));
   return 0;
 }
 """
@@ -48,7 +49,7 @@ int main(void) {
     want = [C.sizeof(N.SceneDesc), C.sizeof(N.MediumDesc), C.sizeof(N.SensorDesc),
             C.sizeof(N.LaserDesc), C.sizeof(N.RunOpts), C.sizeof(N.Stats),
             np.dtype(N.RECORD_FIELDS).itemsize, N.SceneDesc.sensors.offset,
-            N.RunOpts.batch_photons.offset]
+            N.RunOpts.batch_photons.offset, C.sizeof(N.MieSpecies)]
     assert got == want
 
 
@@ -120,3 +121,25 @@ def test_hg_half_angle_form_matches_reference_inverse_cdf():
             omc = (1 - g) * (1 - u) * (1 - g + frac) / d
             opc = (1 + g) * u * (1 + g + frac) / d
             assert 2 * math.atan2(math.sqrt(omc), math.sqrt(opc)) == pytest.approx(ref, abs=1e-7)
+
+
+def test_mie_tables_rejects_bad_arguments_before_any_device_work():
+    """lmc_mie_tables validates its arguments on the host (no GPU needed to refuse)."""
+    sp = (N.MieSpecies * 1)(N.MieSpecies(0.633e-3, 0.5e-3, 1.59, 1.33))
+    v, c, s = np.zeros(11), np.zeros(11), np.zeros(1)
+    a, b = np.zeros(20), np.zeros(20)
+    L = N.lib()
+    assert L.lmc_mie_tables(sp, 1, 0, 0.0, 1.0, 10, N.as_dptr(v), N.as_dptr(c), N.as_dptr(s),
+                            N.as_dptr(a), N.as_dptr(b)) == N.LMC_ERR_INVALID
+    assert L.lmc_mie_tables(sp, 1, 10, 1.0, 1.0, 10, N.as_dptr(v), N.as_dptr(c), N.as_dptr(s),
+                            N.as_dptr(a), N.as_dptr(b)) == N.LMC_ERR_INVALID
+    assert L.lmc_mie_tables(sp, 1, 10, 0.0, 1.0, 1, None, None, None,
+                            N.as_dptr(a), N.as_dptr(b)) == N.LMC_ERR_INVALID
+    assert L.lmc_mie_tables(sp, 1, 10, 0.0, 1.0, 10, N.as_dptr(v), None, N.as_dptr(s),
+                            None, None) == N.LMC_ERR_INVALID
+    bad = (N.MieSpecies * 1)(N.MieSpecies(0.0, 0.5e-3, 1.59, 1.33))
+    assert L.lmc_mie_tables(bad, 1, 10, 0.0, 1.0, 10, N.as_dptr(v), N.as_dptr(c), N.as_dptr(s),
+                            N.as_dptr(a), N.as_dptr(b)) == N.LMC_ERR_INVALID
+    assert "wavelength" in N.last_error()
+    with pytest.raises(ValueError):
+        lm.mie_species([(0.633e-3, 0.5e-3, 1.59, 1.33)], 0)
