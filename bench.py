@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--batch-photons", type=int, default=0)
     ap.add_argument("--variant-steps", type=int, default=2,
                     help="timed steps of the FP64 and FP32+adjoint variants (0: skip them)")
-    ap.add_argument("--variants", default="fp64,differentiable,sweep,estimator",
+    ap.add_argument("--variants", default="fp64,differentiable,sweep,estimator,f2",
                     help="comma-separated subset of the variant arms to measure")
     ap.add_argument("--estimator-photons", type=int, default=1_000_000,
                     help="photons of the estimator-mode variant")
@@ -408,6 +408,56 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
         out.update(measure_sweep(args, local, stream, flush, world, rank, max_ms))
     if "estimator" in sel:
         out.update(measure_estimator(args, local, stream, flush, world, rank, max_ms))
+    if "f2" in sel:
+        out.update(measure_f2(args, local, stream, flush, world, rank, max_ms))
+    return out
+
+
+def f2_specs(n_photons):
+    """The transport's optional parts on the headline geometry: a three-species
+    MixtureLayer slab, the Absorption recorder on a 100 x 100 (r, z) grid, and a
+    StatisticsSensor with event, theta, phi and depth histograms beside the sensors."""
+    from luminis_mc_b200 import workloads as W
+    mix = W.mixture_bilayer(n_photons, 12345)
+    absorb = W.bilayer_rgd_mie(n_photons, 12345)
+    absorb["name"] = "bilayer_rgd_mie_absorption"
+    absorb["absorption"] = {"radius": 5.0, "depth": 2.0, "d_r": 0.05, "d_z": 0.02}
+    stats = W.bilayer_rgd_mie(n_photons, 12345)
+    stats["name"] = "bilayer_rgd_mie_statistics"
+    stats["sensors"].append({"kind": "statistics", "z": 0.0, "absorb": False, "events": 200,
+                             "theta": [0.0, 3.1416, 90], "phi": [0.0, 6.2832, 36],
+                             "depth": [2.0, 100]})
+    return {"mixture_bilayer": mix, "absorption": absorb, "statistics": stats}
+
+
+def measure_f2(args, local, stream, flush, world, rank, max_ms):
+    """MixtureLayer, Absorption recorder and StatisticsSensor workloads (FP32, device time),
+    each beside the reference's own run_simulation_parallel on this host's cores."""
+    import luminis_mc_b200 as lm
+    from luminis_mc_b200 import workloads as W
+    from luminis_mc_b200.device import DeviceRun
+
+    out = {}
+    P = 10_000_000
+    for key, spec in f2_specs(P).items():
+        cfg, _, keep = W.build(lm, spec)
+        run = DeviceRun(cfg, device=f"cuda:{local}")
+        run.run(P // 10, 99, precision="fp32", stream=stream.cuda_stream)
+        flush.zero_()
+        st, _ = run.run(P, 12345, begin=(1 + rank) * P, precision="fp32", stream=stream.cuda_stream)
+        run.close()
+        ms = max_ms(st["kernel_ms"])
+        rec = {"value": P * world / (ms * 1e-3), "unit": "photons/s", "workload": spec["name"],
+               "photons": P, "events_per_photon": st["events"] / P}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            try:
+                rate, n, dt = reference_sample(spec, 3.0, os.cpu_count() or 1)
+                rec["cpu_reference"] = {"value": rate, "unit": "photons/s", "cores": os.cpu_count(),
+                                        "sample": f"{n} photons in {dt:.1f} s, reference "
+                                                  f"run_simulation_parallel (oracle/_ref/perf)"}
+            except Exception as exc:
+                rec["cpu_reference"] = {"value": None, "sample": f"unavailable: {exc}"}
+        out[f"f2_{key}"] = rec
     return out
 
 

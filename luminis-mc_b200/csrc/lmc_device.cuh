@@ -50,6 +50,7 @@ struct AbsorbGrid {
   int on, n_t, n_r, n_z;
   double radius, depth, d_r, d_z, d_t;
   unsigned long long off;
+  float radius_f, depth_f, inv_dr_f, inv_dz_f;   // binary32 transport's cell lookup
 };
 
 // StatisticsSensor histograms (src/detector.cpp:1720-1888): bin parameters and the

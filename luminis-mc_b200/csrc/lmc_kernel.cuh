@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "lmc_device.cuh"
 #include "luminis_b200.h"
@@ -1821,6 +1822,31 @@ __device__ __noinline__ void record_absorption(const AbsorbGrid &g, double *tall
   }
 }
 
+// The same deposit for the binary32 transport: the cell from the binary32 position by
+// reciprocal multiplies instead of binary64 divisions.  The position itself carries
+// binary32 rounding (~1e-7 relative), so the bin edges are no blurrier than the position.
+// Short enough to inline without spills (80 registers, 3 blocks per SM kept).
+__device__ __forceinline__ void record_absorption_f32(const AbsorbGrid &g, double *tallies, float x,
+                                                   float y, float z, double t, double d_weight)
+{
+  const float r = sqrtf(x * x + y * y);
+  if (!(r <= g.radius_f) || !(z >= 0.0f) || !(z <= g.depth_f))
+    return;
+  const float fr = floorf(r * g.inv_dr_f), fz = floorf(z * g.inv_dz_f);
+  if (!(fr < (float)g.n_r) || !(fz < (float)g.n_z))
+    return;
+  const unsigned long long cell = (unsigned long long)fr * (unsigned long long)g.n_z +
+                                  (unsigned long long)fz;
+  double *grid = tallies + g.off;
+  atomicAdd(grid + cell, d_weight);
+  if (g.d_t > 0.0) {
+    const double fk = floor(t / g.d_t) + 1.0;
+    if (fk >= 1.0 && fk < (double)g.n_t)
+      atomicAdd(grid + (unsigned long long)fk * (unsigned long long)g.n_r * (unsigned long long)g.n_z + cell,
+                d_weight);
+  }
+}
+
 // One loop iteration of run_photon (src/simulation.cpp:297-614).  Returns the
 // photon's fate (kAlive if it continues).
 // kExtras: the MixtureLayer species draw and the Absorption recorder are compiled in
@@ -2049,8 +2075,11 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   cnt.events++;
   if (kExtras && (lflags & kLayerAbsorb)) {                   // :589-592
     const double t = sc.absorb.d_t > 0.0 ? launch_time<R>(sc, rp, ph) + ph.opath : 0.0;  // velocity 1
-    record_absorption(sc.absorb, rp.tallies, (double)ph.px, (double)ph.py, (double)ph.pz, t,
-                      SL.mu_t > 0 ? ph.w * SL.absorb_prob : 1.0);
+    const double dw = SL.mu_t > 0 ? ph.w * SL.absorb_prob : 1.0;
+    if constexpr (std::is_same<R, float>::value)
+      record_absorption_f32(sc.absorb, rp.tallies, ph.px, ph.py, ph.pz, t, dw);
+    else
+      record_absorption(sc.absorb, rp.tallies, (double)ph.px, (double)ph.py, (double)ph.pz, t, dw);
   }
   ph.w *= SL.albedo;                                          // the layer's aggregate albedo
   if (ph.w < 1e-4) {                                          // :596-607

@@ -470,6 +470,10 @@ void fill_absorption(const lmc_scene *s, dev::Scene &sc, size_t tally_base, size
   g.d_r = A.d_r;
   g.d_z = A.d_z;
   g.d_t = A.d_t;
+  g.radius_f = (float)A.radius;
+  g.depth_f = (float)A.depth;
+  g.inv_dr_f = (float)(1.0 / A.d_r);
+  g.inv_dz_f = (float)(1.0 / A.d_z);
   g.off = tally_base + off;
   count = (size_t)g.n_t * (size_t)g.n_r * (size_t)g.n_z;
   dims[0] = g.n_t; dims[1] = g.n_r; dims[2] = g.n_z; dims[3] = 1;
