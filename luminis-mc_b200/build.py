@@ -22,8 +22,13 @@ OBJ_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libluminis_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
-              "-fvisibility=hidden", "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}"]
+# Binary32 division and square root by the fast approximations, binary32 denormals
+# flushed: the FP32 transport's results stay within its parity tolerances and the sweep,
+# mixture and absorption kernels run 6-12 % faster.  Binary64 arithmetic is unaffected
+# (the Mie tables in lmc_tables.cu use explicitly rounded binary64 operations).
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-prec-div=false", "-prec-sqrt=false", "-ftz=true",
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+              "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", f"-I{INCLUDE}", f"-I{CSRC}"]
 
 
