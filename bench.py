@@ -36,7 +36,7 @@ METRIC = "photons/s"
 # DRAM bytes (read + write) per photon of one transport launch on bilayer_rgd_mie in
 # FP32: 89.8 MB read + 763.0 MB written for an 8 M-photon launch in one ncu capture
 # (profiles/transport_kernel_bilayer_rgd_mie.md); traffic grows with photons.
-TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": (89.845e6 + 763.017e6) / 8e6}
+TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": (92.413e6 + 762.985e6) / 8e6}
 
 
 def parse():
