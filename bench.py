@@ -36,6 +36,17 @@ METRIC = "photons/s"
 # DRAM bytes (read + write) per photon of one transport launch on bilayer_rgd_mie in
 # FP32: 89.8 MB read + 763.0 MB written for an 8 M-photon launch in one ncu capture
 # (profiles/transport_kernel_bilayer_rgd_mie.md); traffic grows with photons.
+def _hbm_peak():
+    """Measured HBM copy bandwidth of the B200 (MEASURED_PEAKS.json beside this file),
+    else 6.65 TB/s, an earlier STREAM-style copy measurement on B200."""
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
+    except (OSError, KeyError, ValueError, TypeError):
+        return 6650.0, "fallback: 6.65 TB/s, an earlier B200 copy measurement (MEASURED_PEAKS.json absent)"
+
+
+HBM_PEAK_GBS = _hbm_peak()
 TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": (92.413e6 + 762.985e6) / 8e6}
 
 
@@ -373,7 +384,13 @@ def run_ours(args):
                              "ms_per_launch": transport_ms / max(1, transport_launches),
                              "traffic": traffic,
                              "traffic_source": "ncu dram bytes per photon x photons per launch"
-                                               if traffic else None},
+                                               if traffic else None,
+                             # the same launches against HBM: the hit queue is all they move
+                             "hbm_view": ({"achieved": traffic / (transport_ms / max(1, transport_launches)) / 1e6,
+                                           "peak": HBM_PEAK_GBS[0], "unit": "GB/s",
+                                           "frac": traffic / (transport_ms / max(1, transport_launches)) / 1e6
+                                           / HBM_PEAK_GBS[0], "peak_source": HBM_PEAK_GBS[1]}
+                                          if traffic else None)},
                 "variants": variants,
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches}
         print(json.dumps(line), flush=True)
