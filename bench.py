@@ -360,7 +360,7 @@ def run_ours(args):
             rate1, n1, dt1 = reference_sample(spec, 3.0, 1)
             cpu["single_thread"] = {"value": rate1, "unit": "photons/s",
                                     "sample": f"{n1} photons in {dt1:.1f} s, n_threads=1"}
-        except Exception as exc:          # the reference build is optional on a GPU box
+        except Exception as exc:          # the reference build is optional where the bench runs
             cpu = {"value": None, "unit": "photons/s", "cores": os.cpu_count(),
                    "kind": "reference", "sample": f"unavailable: {exc}"}
 
