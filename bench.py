@@ -93,7 +93,7 @@ def config_block(spec, args, n_gpus):
             "l2": "flushed between steps (256 MiB write)", "parallelism": f"photon-range x{n_gpus}",
             "seed": spec["seed"], "block_size": args.block_size or 256,
             "blocks_per_sm": args.blocks_per_sm or "auto",
-            "batch_photons": args.batch_photons or (8 << 20)}
+            "batch_photons": args.batch_photons or (32 << 20)}
 
 
 # ------------------------------------------------------------------------- clocks

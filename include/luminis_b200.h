@@ -206,7 +206,7 @@ typedef struct lmc_run_opts {
   int blocks_per_sm;            /* 0: as many as fit                                   */
   void *records;                /* optional device array of n_photons lmc_record       */
   void *stream;                 /* cudaStream_t to launch on; NULL: the handle's own   */
-  uint64_t batch_photons;       /* photons per transport batch (hit-queue mode); 0: 8M */
+  uint64_t batch_photons;       /* photons per transport batch (hit-queue mode); 0: 32 Mi */
   int stream_format;            /* 0: u24 for FP32, u53 for FP64; 1: u24 for both (an FP64
                                    run on the FP32 run's numbers: precision alone)      */
   int host_tallies_zero;        /* lmc_run_host only: the caller's host tallies are all zero,
@@ -337,7 +337,7 @@ typedef struct lmc_tune_result {
 
 /* Times candidate launch shapes -- threads per block (256, 128), resident blocks per SM
  * (as many as fit, 2, 1: the persistent grid, hence photons per thread) and photons per
- * hit-queue batch (8 Mi, 2 Mi) -- on a sample of about sample_photons photons (a
+ * hit-queue batch (32 Mi, 8 Mi) -- on a sample of about sample_photons photons (a
  * sweep: every scene's count scaled down, restored afterwards) with the rest of `opts`,
  * and returns the fastest; copy its fields into lmc_run_opts for the real runs.  Runs
  * into a scratch tally buffer (allocates it); synchronous. */

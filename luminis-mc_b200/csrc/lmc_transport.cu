@@ -1114,7 +1114,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   // batches: the whole range at once inline; queue-sized batches when queued
   unsigned long long batch = n_photons;
   if (h->queued && n_photons > 0) {
-    batch = opts->batch_photons ? opts->batch_photons : (8ull << 20);
+    batch = opts->batch_photons ? opts->batch_photons : (32ull << 20);   // ~110 B of queue per photon
     batch = std::min<unsigned long long>(batch, n_photons);
     const unsigned long long planes = std::max(1, h->max_planes);
     const unsigned long long cap = batch * planes + batch / 16 + 1024;
@@ -1379,7 +1379,7 @@ lmc_status lmc_autotune(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts, 
   // thread of the persistent kernel) x photons per hit-queue batch
   const int blocks[] = {256, 128};
   const int per_sm[] = {0, 2, 1};
-  const unsigned long long batches[] = {8ull << 20, 2ull << 20};
+  const unsigned long long batches[] = {32ull << 20, 8ull << 20};
   lmc_tune_result best;
   std::memset(&best, 0, sizeof(best));
   lmc_status result = LMC_OK;
