@@ -569,14 +569,15 @@ def measure_sweep(args, local, stream, flush, world, rank, max_ms):
     # against one lmc_mie_tables batch on the GPU (same numbers bit for bit)
     particles = [(sp["phases"][0]["wavelength"], sp["phases"][0]["radius"],
                   sp["phases"][0]["n_particle"], sp["phases"][0]["n_medium"]) for sp in sspecs]
-    host_s, gpu_s = [], []
+    host_s, gpu_s, split = [], [], []
     for _ in range(3):
         t0 = time.perf_counter()
         for q in particles:
             lm.MieMedium(lm.MiePhaseFunction(*q, 1000, 0.0, math.pi), q[1], q[2], q[3], q[0])
         host_s.append(time.perf_counter() - t0)
         t0 = time.perf_counter()
-        lm.mie_species(particles, 1000, 0.0, math.pi)
+        split.append({})
+        lm.mie_species(particles, 1000, 0.0, math.pi, timing=split[-1])
         gpu_s.append(time.perf_counter() - t0)
     scfgs = W.build_mie_sweep(lm, sspecs)
     sw = SweepRun(scfgs, device=f"cuda:{local}")
@@ -641,6 +642,7 @@ def measure_sweep(args, local, stream, flush, world, rank, max_ms):
                     "(numpy default_rng(2026))",
         "tables": {"species": len(particles), "host_s": round(sorted(host_s)[1], 4),
                    "gpu_s": round(sorted(gpu_s)[1], 4),
+                   "gpu_split_ms": {k: round(sorted(t[k] for t in split)[1], 3) for k in split[0]},
                    "what": "MiePhaseFunction (1001-node CDF) + MieMedium (1000-node S1/S2) "
                            "per species; host: the constructors one species at a time on one "
                            "thread; gpu: lmc_mie_tables, host coefficients + device sums, "

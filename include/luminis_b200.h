@@ -450,12 +450,15 @@ typedef struct lmc_mie_species {
  *   s1[n][2 n_amp], s2[...]    lmc_amplitude_table(LMC_AMP_MIE, n_amp), interleaved re/im
  * All are host arrays.  values/cdf/sigma may be null together (n_div ignored), s1/s2 may be
  * null together or n_amp 0 (no amplitude tables).  The Mie coefficient recurrence runs on
- * the host; the angular sums, the PDF and the CDF on the GPU.  Replaces the per-species
+ * the host; the angular sums, the PDF and the CDF on the GPU.  timing_ms (4 doubles, may
+ * be null) receives the host series, upload, device-kernel and read-back times in ms.
+ * Replaces the per-species
  * construction of MiePhaseFunction (src/phase.cpp:244-304, src/table.cpp:6-48) and
  * MieMedium (src/medium.cpp:160-236) around MIEV0 (src/mie/MIEV0noP.f). */
 LMC_API lmc_status lmc_mie_tables(const lmc_mie_species *species, int n, int n_div,
                                   double min_val, double max_val, int n_amp, double *values,
-                                  double *cdf, double *sigma, double *s1, double *s2);
+                                  double *cdf, double *sigma, double *s1, double *s2,
+                                  double *timing_ms);
 
 /* ---- measurement --------------------------------------------------------------------- */
 

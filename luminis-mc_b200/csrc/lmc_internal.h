@@ -39,4 +39,9 @@ struct MieSeries {
 
 bool mie_series(double x, double m_re, double m_im, MieSeries &out);
 
+// Device buffer -> pageable host buffer through two pinned 16 MiB halves shared by the
+// process, host-thread copies overlapping the DMA; `stream` is a cudaStream_t.  Blocks
+// until the copy is done.
+lmc_status read_back(double *h_dst, const double *d_src, size_t bytes, void *stream);
+
 }  // namespace lmc

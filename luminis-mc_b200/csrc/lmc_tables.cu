@@ -11,10 +11,14 @@
 // for bit.
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstdint>
+#include <mutex>
 #include <string>
+#include <tuple>
+#include <utility>
 #include <vector>
 
 #include "lmc_internal.h"
@@ -134,10 +138,32 @@ __global__ void cdf_kernel(double *__restrict__ rows, int n_species, int n_pdf, 
     atomicExch(nonfinite, 1);
 }
 
-struct DeviceBuffer {
-  void *p = nullptr;
-  ~DeviceBuffer() { cudaFree(p); }
-};
+// One work buffer per device, kept between calls (a sweep's 256 species need ~12 MB);
+// allocating and freeing it per call cost more than the whole computation.
+std::mutex g_arena_mutex;
+std::vector<std::pair<void *, size_t>> g_arena;        // per device ordinal
+
+lmc_status arena(size_t bytes, unsigned char **out)
+{
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess)
+    return fail(LMC_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (g_arena.size() <= size_t(dev))
+    g_arena.resize(size_t(dev) + 1, {nullptr, 0});
+  auto &a = g_arena[dev];
+  if (a.second < bytes) {
+    cudaFree(a.first);
+    a = {nullptr, 0};
+    e = cudaMalloc(&a.first, bytes);
+    if (e != cudaSuccess)
+      return fail(e == cudaErrorMemoryAllocation ? LMC_ERR_NOMEM : LMC_ERR_CUDA,
+                  std::string("lmc_mie_tables work buffer: ") + cudaGetErrorString(e));
+    a.second = bytes;
+  }
+  *out = static_cast<unsigned char *>(a.first);
+  return LMC_OK;
+}
 
 }  // namespace tables
 }  // namespace lmc
@@ -153,11 +179,11 @@ extern "C" {
 
 LMC_API lmc_status lmc_mie_tables(const lmc_mie_species *species, int n, int n_div,
                                   double min_val, double max_val, int n_amp, double *values,
-                                  double *cdf, double *sigma, double *s1, double *s2)
+                                  double *cdf, double *sigma, double *s1, double *s2,
+                                  double *timing_ms)
 {
   using namespace lmc;
   using namespace lmc::tables;
-  using cd = std::complex<double>;
   const bool want_pdf = values || cdf || sigma;
   const bool want_amp = (s1 || s2) && n_amp != 0;
   if (n < 0 || (n > 0 && !species))
@@ -172,6 +198,17 @@ LMC_API lmc_status lmc_mie_tables(const lmc_mie_species *species, int n, int n_d
     return fail(LMC_ERR_INVALID, "lmc_mie_tables: s1 and s2 go together, n_amp >= 2");
   const int n_pdf = want_pdf ? n_div + 1 : 0;
   const int n_nodes_amp = want_amp ? n_amp : 0;
+  using clock = std::chrono::steady_clock;
+  auto ms_since = [](clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(clock::now() - t).count();
+  };
+  double timing[4] = {0.0, 0.0, 0.0, 0.0};      // series, upload, kernels, read-back
+  auto report = [&] {
+    if (timing_ms)
+      for (int i = 0; i < 4; ++i)
+        timing_ms[i] = timing[i];
+  };
+  clock::time_point t0 = clock::now();
 
   // host side: node tables shared by all species (as lmc_sampling_table and
   // lmc_amplitude_table compute them), then each species' two coefficient series
@@ -223,8 +260,12 @@ LMC_API lmc_status lmc_mie_tables(const lmc_mie_species *species, int n, int n_d
       desc[2 * size_t(i) + 1].fac = M_PI / (k * k * sigma[i]);
     }
   }
-  if (n == 0 || (!want_pdf && !want_amp))
+  timing[0] = ms_since(t0);
+  if (n == 0 || (!want_pdf && !want_amp)) {
+    report();
     return LMC_OK;
+  }
+  t0 = clock::now();
 
   // device side: one allocation for every input and output
   const size_t b_desc = desc.size() * sizeof(SeriesDesc);
@@ -236,9 +277,11 @@ LMC_API lmc_status lmc_mie_tables(const lmc_mie_species *species, int n, int n_d
   const size_t o_coef = up(b_desc), o_bp = o_coef + up(b_coef), o_nodes = o_bp + up(b_coef);
   const size_t o_s1 = o_nodes + up(b_nodes), o_s2 = o_s1 + up(b_amp), o_pdf = o_s2 + up(b_amp);
   const size_t o_flag = o_pdf + up(b_pdf), total = o_flag + 256;
-  DeviceBuffer buf;
-  LMC_TCUDA(cudaMalloc(&buf.p, total));
-  unsigned char *base = static_cast<unsigned char *>(buf.p);
+  std::lock_guard<std::mutex> lock(g_arena_mutex);
+  unsigned char *base = nullptr;
+  const lmc_status ar = arena(total, &base);
+  if (ar != LMC_OK)
+    return ar;
   auto at = [&](size_t off) { return base + off; };
   double *d_nodes = reinterpret_cast<double *>(at(o_nodes));
   LMC_TCUDA(cudaMemcpy(at(0), desc.data(), b_desc, cudaMemcpyHostToDevice));
@@ -255,6 +298,15 @@ LMC_API lmc_status lmc_mie_tables(const lmc_mie_species *species, int n, int n_d
                          cudaMemcpyHostToDevice));
   }
   LMC_TCUDA(cudaMemset(at(o_flag), 0, sizeof(int)));
+  timing[1] = ms_since(t0);
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  struct EventPair {
+    cudaEvent_t *e;
+    ~EventPair() { for (int i = 0; i < 2; ++i) if (e[i]) cudaEventDestroy(e[i]); }
+  } ev_guard{ev};
+  LMC_TCUDA(cudaEventCreate(&ev[0]));
+  LMC_TCUDA(cudaEventCreate(&ev[1]));
+  LMC_TCUDA(cudaEventRecord(ev[0]));
   constexpr int kThreads = 128;
   const dim3 grid((n_nodes_amp + n_pdf + kThreads - 1) / kThreads, std::min(n, 65535));
   sums_kernel<<<grid, kThreads>>>(
@@ -268,17 +320,27 @@ LMC_API lmc_status lmc_mie_tables(const lmc_mie_species *species, int n, int n_d
         reinterpret_cast<double *>(at(o_pdf)), n, n_pdf, step, reinterpret_cast<int *>(at(o_flag)));
     LMC_TCUDA(cudaGetLastError());
   }
+  LMC_TCUDA(cudaEventRecord(ev[1]));
+  LMC_TCUDA(cudaEventSynchronize(ev[1]));
+  float kernel_ms = 0.f;
+  LMC_TCUDA(cudaEventElapsedTime(&kernel_ms, ev[0], ev[1]));
+  timing[2] = kernel_ms;
+  t0 = clock::now();
   int nonfinite = 0;
   if (n_pdf)
     LMC_TCUDA(cudaMemcpy(&nonfinite, at(o_flag), sizeof(int), cudaMemcpyDeviceToHost));
   if (nonfinite)
     return fail(LMC_ERR_INVALID, "phase-function CDF is not finite");
-  if (n_pdf)
-    LMC_TCUDA(cudaMemcpy(cdf, at(o_pdf), b_pdf, cudaMemcpyDeviceToHost));
-  if (n_nodes_amp) {
-    LMC_TCUDA(cudaMemcpy(s1, at(o_s1), b_amp, cudaMemcpyDeviceToHost));
-    LMC_TCUDA(cudaMemcpy(s2, at(o_s2), b_amp, cudaMemcpyDeviceToHost));
+  for (auto [dst, off, bytes] : {std::make_tuple(cdf, o_pdf, b_pdf), std::make_tuple(s1, o_s1, b_amp),
+                                  std::make_tuple(s2, o_s2, b_amp)}) {
+    if (!bytes)
+      continue;
+    const lmc_status rb = read_back(dst, reinterpret_cast<const double *>(at(off)), bytes, nullptr);
+    if (rb != LMC_OK)
+      return rb;
   }
+  timing[3] = ms_since(t0);
+  report();
   return LMC_OK;
 }
 

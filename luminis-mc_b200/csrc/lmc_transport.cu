@@ -1566,9 +1566,12 @@ void parallel_copy(unsigned char *dst, const unsigned char *src, size_t bytes)
     t.join();
 }
 
+}  // namespace
+
 // Device tallies -> caller's host buffer, chunk by chunk through the pinned halves.
-lmc_status read_back(double *h_dst, const double *d_src, size_t bytes, cudaStream_t stream)
+lmc_status read_back(double *h_dst, const double *d_src, size_t bytes, void *stream_ptr)
 {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
   std::lock_guard<std::mutex> lock(g_stage_mutex);
   if (!g_stage)
     LMC_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&g_stage), 2 * kStageBytes, cudaHostAllocPortable));
@@ -1593,7 +1596,6 @@ lmc_status read_back(double *h_dst, const double *d_src, size_t bytes, cudaStrea
   return LMC_OK;
 }
 
-}  // namespace
 }  // namespace lmc
 
 extern "C" {
@@ -1626,7 +1628,7 @@ lmc_status lmc_run_host(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uin
   if (st != LMC_OK)
     return st;
   if (bytes) {
-    const lmc_status rb = read_back(h_tallies, h->d_host_tally, bytes, stream);
+    const lmc_status rb = read_back(h_tallies, h->d_host_tally, bytes, static_cast<void *>(stream));
     if (rb != LMC_OK)
       return rb;
   }

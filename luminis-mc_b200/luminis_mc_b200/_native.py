@@ -199,7 +199,7 @@ def lib():
                                       C.c_int, dptr, dptr]
     L.lmc_amplitude_table.restype = C.c_int
     L.lmc_mie_tables.argtypes = [C.POINTER(MieSpecies), C.c_int, C.c_int, C.c_double, C.c_double,
-                                 C.c_int, dptr, dptr, dptr, dptr, dptr]
+                                 C.c_int, dptr, dptr, dptr, dptr, dptr, dptr]
     L.lmc_mie_tables.restype = C.c_int
     L.lmc_probe_fp32_peak.argtypes = [C.c_int, dptr, dptr]
     L.lmc_probe_fp32_peak.restype = C.c_int

@@ -553,14 +553,16 @@ class MieMedium(ScatteringMedium):
         self.k = 2 * math.pi * self.n_medium / self.wavelength
 
 
-def mie_species(species, nDiv=1000, minVal=0.0, maxVal=math.pi):
+def mie_species(species, nDiv=1000, minVal=0.0, maxVal=math.pi, timing=None):
     """Build many Mie species at once on the GPU (lmc_mie_tables).
 
     ``species`` is a sequence of (wavelength, radius, n_particle, n_medium).  Returns one
     (MiePhaseFunction(wavelength, radius, n_particle, n_medium, nDiv, minVal, maxVal),
     MieMedium(phase, radius, n_particle, n_medium, wavelength)) pair per species, with
     tables equal bit for bit to those the two constructors build one species at a time
-    (src/phase.cpp:244-304, src/medium.cpp:160-236).  Needs a CUDA device.
+    (src/phase.cpp:244-304, src/medium.cpp:160-236).  Needs a CUDA device.  ``timing``, a
+    dict, receives the milliseconds of the host series, the uploads, the device kernels
+    and the read-back.
     """
     species = [tuple(float(v) for v in q) for q in species]
     n = len(species)
@@ -575,9 +577,12 @@ def mie_species(species, nDiv=1000, minVal=0.0, maxVal=math.pi):
     sigma = np.zeros(max(n, 1))
     s1 = np.zeros((n, 2 * n_amp))
     s2 = np.zeros((n, 2 * n_amp))
+    t_ms = np.zeros(4)
     N.check(N.lib().lmc_mie_tables(arr, n, int(nDiv), float(minVal), float(maxVal), n_amp,
                                    N.as_dptr(values), N.as_dptr(cdf), N.as_dptr(sigma),
-                                   N.as_dptr(s1), N.as_dptr(s2)))
+                                   N.as_dptr(s1), N.as_dptr(s2), N.as_dptr(t_ms)))
+    if timing is not None:
+        timing.update(zip(("series_ms", "upload_ms", "kernels_ms", "readback_ms"), t_ms.tolist()))
     out = []
     for i, (wl, r, n_p, n_m) in enumerate(species):
         ph = MiePhaseFunction.__new__(MiePhaseFunction)

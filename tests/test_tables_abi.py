@@ -130,16 +130,16 @@ def test_mie_tables_rejects_bad_arguments_before_any_device_work():
     a, b = np.zeros(20), np.zeros(20)
     L = N.lib()
     assert L.lmc_mie_tables(sp, 1, 0, 0.0, 1.0, 10, N.as_dptr(v), N.as_dptr(c), N.as_dptr(s),
-                            N.as_dptr(a), N.as_dptr(b)) == N.LMC_ERR_INVALID
+                            N.as_dptr(a), N.as_dptr(b), None) == N.LMC_ERR_INVALID
     assert L.lmc_mie_tables(sp, 1, 10, 1.0, 1.0, 10, N.as_dptr(v), N.as_dptr(c), N.as_dptr(s),
-                            N.as_dptr(a), N.as_dptr(b)) == N.LMC_ERR_INVALID
+                            N.as_dptr(a), N.as_dptr(b), None) == N.LMC_ERR_INVALID
     assert L.lmc_mie_tables(sp, 1, 10, 0.0, 1.0, 1, None, None, None,
-                            N.as_dptr(a), N.as_dptr(b)) == N.LMC_ERR_INVALID
+                            N.as_dptr(a), N.as_dptr(b), None) == N.LMC_ERR_INVALID
     assert L.lmc_mie_tables(sp, 1, 10, 0.0, 1.0, 10, N.as_dptr(v), None, N.as_dptr(s),
-                            None, None) == N.LMC_ERR_INVALID
+                            None, None, None) == N.LMC_ERR_INVALID
     bad = (N.MieSpecies * 1)(N.MieSpecies(0.0, 0.5e-3, 1.59, 1.33))
     assert L.lmc_mie_tables(bad, 1, 10, 0.0, 1.0, 10, N.as_dptr(v), N.as_dptr(c), N.as_dptr(s),
-                            N.as_dptr(a), N.as_dptr(b)) == N.LMC_ERR_INVALID
+                            N.as_dptr(a), N.as_dptr(b), None) == N.LMC_ERR_INVALID
     assert "wavelength" in N.last_error()
     with pytest.raises(ValueError):
         lm.mie_species([(0.633e-3, 0.5e-3, 1.59, 1.33)], 0)
