@@ -921,7 +921,7 @@ static KernelFn pick_transport_e(bool fp32, bool queued, bool three, bool adj, b
     return fp32 ? transport_kernel<float, true, 2, false, false, true, E>
                 : transport_kernel<double, true, 1, false, false, true, E>;
   if (sw && adj)
-    return fp32 ? transport_kernel<float, true, 2, true, true> : transport_kernel<double, true, 1, true, true>;
+    return fp32 ? transport_kernel<float, true, 3, true, true> : transport_kernel<double, true, 1, true, true>;
   if (sw)
     return fp32 ? transport_kernel<float, true, 3, false, true, false, E>
                 : transport_kernel<double, true, 2, false, true, false, E>;
