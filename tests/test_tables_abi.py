@@ -143,3 +143,19 @@ def test_mie_tables_rejects_bad_arguments_before_any_device_work():
     assert "wavelength" in N.last_error()
     with pytest.raises(ValueError):
         lm.mie_species([(0.633e-3, 0.5e-3, 1.59, 1.33)], 0)
+
+
+def test_build_mie_sweep_refuses_other_specs():
+    """workloads.build_mie_sweep batches single-medium Mie specs only, on one node grid."""
+    spec = W.mie_sweep(0)
+    other = W.bilayer_rgd_mie(10, 1)
+    with pytest.raises(ValueError, match="single-medium Mie"):
+        W.build_mie_sweep(lm, [spec, other])
+    grid = W.mie_sweep(1)
+    grid["phases"][0]["nDiv"] = 500
+    with pytest.raises(ValueError, match="nDiv"):
+        W.build_mie_sweep(lm, [spec, grid])
+    mismatch = W.mie_sweep(2)
+    mismatch["media"][0]["radius"] *= 2
+    with pytest.raises(ValueError, match="same particle"):
+        W.build_mie_sweep(lm, [mismatch])
