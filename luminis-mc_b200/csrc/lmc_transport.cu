@@ -919,7 +919,7 @@ static KernelFn pick_transport_e(bool fp32, bool queued, bool three, bool adj, b
   using namespace lmc::dev;
   if (est)
     return fp32 ? transport_kernel<float, true, 2, false, false, true, E>
-                : transport_kernel<double, true, 1, false, false, true, E>;
+                : transport_kernel<double, true, 2, false, false, true, E>;
   if (sw && adj)
     return fp32 ? transport_kernel<float, true, 3, true, true> : transport_kernel<double, true, 1, true, true>;
   if (sw)
