@@ -33,9 +33,8 @@ sys.path.insert(0, REPO)
 
 FLOP_PER_EVENT = 300        # FP32 flops per scattering event (add/mul = 1, FMA = 2)
 METRIC = "photons/s"
-# DRAM bytes (read + write) per photon of one transport launch on bilayer_rgd_mie in
-# FP32: 89.8 MB read + 763.0 MB written for an 8 M-photon launch in one ncu capture
-# (profiles/transport_kernel_bilayer_rgd_mie.md); traffic grows with photons.
+
+
 def _hbm_peak():
     """Measured HBM copy bandwidth of the B200 (MEASURED_PEAKS.json beside this file),
     else 6.65 TB/s, an earlier STREAM-style copy measurement on B200."""
@@ -47,6 +46,9 @@ def _hbm_peak():
 
 
 HBM_PEAK_GBS = _hbm_peak()
+# DRAM bytes (read + write) per photon of one FP32 transport launch on bilayer_rgd_mie:
+# 92.4 MB read + 763.0 MB written for an 8 M-photon launch in one ncu capture of the
+# transport kernel; the traffic is the hit queue, so it grows with the photons.
 TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": (92.413e6 + 762.985e6) / 8e6}
 
 

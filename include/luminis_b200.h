@@ -287,12 +287,15 @@ LMC_API size_t lmc_last_error(char *buf, size_t len);
  * 64 MiB device array that the CUDA runtime reserves per GPU when this library is
  * loaded.  Limits: the scene's tables must fit in 8 MiB (a larger scene returns
  * LMC_ERR_INVALID with the size it needs); photons are processed in batches that
- * fit the remaining ~56 MiB hit queue.  The first call on each device looks up the
+ * fit the remaining ~56 MiB hit queue, or of opts->batch_photons when that is
+ * smaller.  opts->block_size and opts->blocks_per_sm pick the launch shape and the
+ * kernel variant as they do for lmc_run.  The first call on each device looks up the
  * array's device address (cudaGetSymbolAddress), so make that first call before
  * any stream capture.  All calls on one device share the array: calls that
  * overlap in time -- from two threads, or on two streams -- race and corrupt each
  * other's results; serialise them.  Runs on opts->stream (NULL = legacy default
- * stream) and returns after the stream has finished the run.  stats->kernel_ms is
+ * stream) and is synchronous: it copies the run counters back and returns only
+ * after the stream has finished the run.  stats->kernel_ms is
  * always 0 (timing events would be allocations).
  * No counterpart in the reference. */
 LMC_API lmc_status lmc_run_noalloc(const lmc_scene *scene, uint64_t seed, uint64_t photon_begin,

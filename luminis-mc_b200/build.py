@@ -77,12 +77,13 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if force or _stale(obj, [src] + headers):
             extra = ["-Xptxas", "-v"] if ptxas_info else []
             run([nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", src, "-o", obj])
+    cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc())), "include")   # NVTX headers
     for f in cpp:
         src = os.path.join(CSRC, f)
         obj = os.path.join(OBJ_DIR, f + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
-            run(["g++", *CXX_FLAGS, "-c", src, "-o", obj])
+            run(["g++", *CXX_FLAGS, f"-I{cuda_inc}", "-c", src, "-o", obj])
     if force or _stale(LIB, objs):
         run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lpthread"])
     return LIB

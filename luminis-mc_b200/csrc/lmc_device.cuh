@@ -171,7 +171,7 @@ struct RunParams {
   uint32_t key0, key1;
   int max_events, track_reverse;
   double *tallies;
-  lmc_record *records;
+  lmc_record *records;                   // this launch's photons: photon_begin + i at records[i]
   Scratch *scratch;
   Queue queue;                           // used by the queued kernel pair
   unsigned int cbs_mask;                 // sensors whose hits need the CBS fields

@@ -5,9 +5,21 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "luminis_b200.h"
 
 namespace lmc {
+
+// An NVTX range named `name` for the object's lifetime (scene set-up, launches, tally
+// read-back), so a profiler that traces NVTX shows the host phases of a run beside its
+// kernels.  Without a profiler attached each push/pop is a branch on a null callback.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Thread-local last-error message behind lmc_last_error().
 std::string &last_error();

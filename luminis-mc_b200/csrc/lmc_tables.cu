@@ -184,6 +184,7 @@ LMC_API lmc_status lmc_mie_tables(const lmc_mie_species *species, int n, int n_d
 {
   using namespace lmc;
   using namespace lmc::tables;
+  NvtxRange range("lmc_mie_tables: batched Mie set-up tables");
   const bool want_pdf = values || cdf || sigma;
   const bool want_amp = (s1 || s2) && n_amp != 0;
   if (n < 0 || (n > 0 && !species))

@@ -480,10 +480,15 @@ void fill_absorption(const lmc_scene *s, dev::Scene &sc, size_t tally_base, size
   off += count;
 }
 
-// tally_base: offset (doubles) of this scene's first sensor in the tally buffer.
-void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned char> &arena, SceneBuild &b)
+// The parts of a device scene that need no table memory, shared by lmc_create and
+// lmc_run_noalloc: counts, layers, laser, sensors with their planes and tally offsets,
+// the Absorption grid, the sensor masks and every medium's scalar fields (the table
+// pointers stay null).  Sensor i's tallies start at tally_base + sensor_off[i]; returns
+// the scene's tally doubles (sensors, then the Absorption grid at *abs_off).
+size_t fill_scene_head(const lmc_scene *s, size_t tally_base, dev::Scene &sc, size_t *sensor_off,
+                       size_t *sensor_count, int (*sensor_dims)[4], size_t *abs_off,
+                       size_t *abs_count, int *abs_dims)
 {
-  dev::Scene &sc = b.sc;
   std::memset(&sc, 0, sizeof(sc));
   sc.n_layers = s->n_layers;
   sc.n_media = s->n_media;
@@ -511,67 +516,53 @@ void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned cha
   sc.laser.time_offset = L.time_offset;
 
   // sensor planes: one key per z within 1e-9 (DoubleComparator, detector.hpp:46-48)
-  std::vector<double> planes;
+  double planes[LMC_MAX_SENSORS];
+  int n_planes = 0;
   size_t off = 0;
   for (int i = 0; i < s->n_sensors; ++i) {
     const lmc_sensor_desc &S = s->sensors[i];
     dev::Sensor &d = sc.sensors[i];
     size_t count = 0;
-    fill_sensor(S, d, count, b.sensor_dims[i]);
+    fill_sensor(S, d, count, sensor_dims[i]);
     const double z = (S.kind == LMC_SENSOR_FARFIELD_CBS || S.kind == LMC_SENSOR_FARFIELD_FLUENCE) ? 0.0 : S.z;
     if (S.kind == LMC_SENSOR_PLANAR_FIELD && !d.estimator)
       sc.need_phase = 1;
     int g = -1;
-    for (size_t k = 0; k < planes.size(); ++k)
+    for (int k = 0; k < n_planes; ++k)
       if (!(planes[k] < z - 1e-9) && !(z < planes[k] - 1e-9))
-        g = (int)k;
+        g = k;
     if (g < 0) {
-      planes.push_back(z);
-      g = (int)planes.size() - 1;
+      planes[n_planes] = z;
+      g = n_planes++;
     }
     d.plane = g;
     d.tally_off = tally_base + off;
-    b.sensor_off[i] = off;
-    b.sensor_count[i] = count;
+    sensor_off[i] = off;
+    sensor_count[i] = count;
     off += count;
   }
-  // sort planes ascending and remap (record_hit walks the map in key order)
-  std::vector<int> order(planes.size());
-  for (size_t k = 0; k < planes.size(); ++k)
-    order[k] = (int)k;
-  std::sort(order.begin(), order.end(), [&](int a, int c) { return planes[a] < planes[c]; });
-  std::vector<int> rank(planes.size());
-  for (size_t k = 0; k < order.size(); ++k) {
-    rank[order[k]] = (int)k;
-    sc.plane_z[k] = planes[order[k]];
-    sc.plane_z_f[k] = (float)planes[order[k]];
+  // planes in ascending z, ties in insertion order (record_hit walks the map in key
+  // order)
+  int rank[LMC_MAX_SENSORS];
+  for (int k = 0; k < n_planes; ++k) {
+    int r = 0;
+    for (int q = 0; q < n_planes; ++q)
+      r += (planes[q] < planes[k] || (planes[q] == planes[k] && q < k)) ? 1 : 0;
+    rank[k] = r;
+    sc.plane_z[r] = planes[k];
+    sc.plane_z_f[r] = (float)planes[k];
   }
   for (int i = 0; i < s->n_sensors; ++i)
     sc.sensors[i].plane = rank[sc.sensors[i].plane];
-  sc.n_planes = (int)planes.size();
-  b.abs_off = off;
-  fill_absorption(s, sc, tally_base, off, b.abs_count, b.abs_dims);
-  b.tally_doubles = off;
-  // A photon below z = 0 has left the sample, so a plane at z <= 0 is crossed at
-  // most once per photon: hits fit a queue of (photons x planes) entries and are
-  // tallied by a second kernel.  Planes inside the sample may be crossed any
-  // number of times; such scenes tally inside the transport kernel.
-  b.queued = sc.n_planes == 0 || sc.plane_z[sc.n_planes - 1] <= 0.0;
-  for (int i = 0; i < s->n_sensors; ++i)
+  sc.n_planes = n_planes;
+  *abs_off = off;
+  fill_absorption(s, sc, tally_base, off, *abs_count, abs_dims);
+  for (int i = 0; i < s->n_sensors; ++i) {
     if (s->sensors[i].kind == LMC_SENSOR_FARFIELD_CBS)
-      b.cbs_mask |= 1u << i;
-  sc.cbs_mask = b.cbs_mask;
-  for (int i = 0; i < s->n_sensors; ++i)
+      sc.cbs_mask |= 1u << i;
     if (s->sensors[i].kind == LMC_SENSOR_STATISTICS)
       sc.stat_mask |= 1u << i;
-
-  // table arena: per medium double/float theta tables, guide tables, amplitudes
-  auto put = [&](const void *src, size_t bytes) -> size_t {
-    const size_t o = (arena.size() + 255) & ~size_t(255);
-    arena.resize(o + bytes);
-    std::memcpy(arena.data() + o, src, bytes);
-    return o;
-  };
+  }
   for (int i = 0; i < s->n_media; ++i) {
     const lmc_medium_desc &M = s->media[i];
     dev::Medium &d = sc.media[i];
@@ -587,11 +578,45 @@ void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned cha
     d.amp_inv_dx_f = (float)d.amp_inv_dx;
     d.mu_s = M.mu_s;
     d.mu_s_f = (float)M.mu_s;
+    d.I_norm = medium_I_norm(M);
+    if (M.theta_kind == LMC_THETA_TABLE || M.theta_kind == LMC_THETA_TABLE_COS)
+      d.theta_n = M.theta_n;
+  }
+  return off;
+}
+
+// A photon below z = 0 has left the sample, so a plane at z <= 0 is crossed at most
+// once per photon: hits fit a queue of (photons x planes) entries and are tallied by a
+// second kernel.  Planes inside the sample may be crossed any number of times; such
+// scenes tally inside the transport kernel.
+bool scene_queued(const dev::Scene &sc)
+{
+  return sc.n_planes == 0 || sc.plane_z[sc.n_planes - 1] <= 0.0;
+}
+
+// tally_base: offset (doubles) of this scene's first sensor in the tally buffer.
+void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned char> &arena, SceneBuild &b)
+{
+  dev::Scene &sc = b.sc;
+  b.tally_doubles = fill_scene_head(s, tally_base, sc, b.sensor_off, b.sensor_count, b.sensor_dims,
+                                    &b.abs_off, &b.abs_count, b.abs_dims);
+  b.queued = scene_queued(sc);
+  b.cbs_mask = sc.cbs_mask;
+  const lmc_laser_desc &L = s->laser;
+
+  // table arena: per medium double/float theta tables, guide tables, amplitudes
+  auto put = [&](const void *src, size_t bytes) -> size_t {
+    const size_t o = (arena.size() + 255) & ~size_t(255);
+    arena.resize(o + bytes);
+    std::memcpy(arena.data() + o, src, bytes);
+    return o;
+  };
+  for (int i = 0; i < s->n_media; ++i) {
+    const lmc_medium_desc &M = s->media[i];
     MedOff &o = b.mo[i];
     o = MedOff{0, 0, 0, 0, 0, 0};
     if (M.theta_kind == LMC_THETA_TABLE || M.theta_kind == LMC_THETA_TABLE_COS) {
       const int n = M.theta_n;
-      d.theta_n = n;
       std::vector<double> vd(M.theta_values, M.theta_values + n), cd(M.theta_cdf, M.theta_cdf + n);
       std::vector<double2> cs(n);
       for (int k = 0; k < n; ++k) {
@@ -614,7 +639,6 @@ void build_scene(const lmc_scene *s, size_t tally_base, std::vector<unsigned cha
     }
     o.ad = put(ad.data(), ad.size() * sizeof(double4));
     o.af = put(af.data(), af.size() * sizeof(float4));
-    d.I_norm = medium_I_norm(M);
   }
   // Estimator-mode FarFieldCBS: the bin directions of the estimated grid around the
   // backscatter axis -s_in of the launch frame, with their solid angles
@@ -728,6 +752,7 @@ size_t lmc_last_error(char *buf, size_t len)
 lmc_status lmc_create(const lmc_scene *s, lmc_handle **out)
 {
   using namespace lmc;
+  NvtxRange range("lmc_create: scene set-up and upload");
   if (!out)
     return fail(LMC_ERR_INVALID, "out must not be null");
   *out = nullptr;
@@ -972,6 +997,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   using namespace lmc;
   if (!h || !opts)
     return fail(LMC_ERR_INVALID, "handle and options must not be null");
+  NvtxRange range("lmc_run: transport and tally launches");
   if (h->tally_doubles && !d_tallies)
     return fail(LMC_ERR_INVALID, "device tally buffer must not be null");
   if (opts->precision != LMC_PRECISION_FP32 && opts->precision != LMC_PRECISION_FP64)
@@ -1148,10 +1174,12 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     }
   }
   LMC_CUDA(cudaEventRecord(h->ev0, stream));
+  lmc_record *const records = static_cast<lmc_record *>(opts->records);
   for (unsigned long long done = 0; done < n_photons; done += batch) {
     const unsigned long long nb = std::min(batch, n_photons - done);
     rp.photon_begin = photon_begin + done;
     rp.n_photons = nb;
+    rp.records = records ? records + done : nullptr;   // the kernels index from photon_begin
     // reset the work counter and the queue fill of this batch
     LMC_CUDA(cudaMemsetAsync(h->d_scratch, 0, 2 * sizeof(unsigned long long), stream));
     const int grid = (int)std::max<unsigned long long>(
@@ -1213,6 +1241,7 @@ lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t
 lmc_status lmc_create_sweep(const lmc_scene *scenes, int n_scenes, lmc_handle **out)
 {
   using namespace lmc;
+  NvtxRange range("lmc_create_sweep: scene set-up and upload");
   if (!out || !scenes)
     return fail(LMC_ERR_INVALID, "scenes and out must not be null");
   *out = nullptr;
@@ -1571,6 +1600,7 @@ void parallel_copy(unsigned char *dst, const unsigned char *src, size_t bytes)
 // Device tallies -> caller's host buffer, chunk by chunk through the pinned halves.
 lmc_status read_back(double *h_dst, const double *d_src, size_t bytes, void *stream_ptr)
 {
+  NvtxRange range("lmc tallies: device to host read-back");
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
   std::lock_guard<std::mutex> lock(g_stage_mutex);
   if (!g_stage)
@@ -1604,6 +1634,7 @@ lmc_status lmc_run_host(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uin
                         const lmc_run_opts *opts, double *h_tallies, lmc_stats *stats)
 {
   using namespace lmc;
+  NvtxRange range("lmc_run_host");
   if (!h)
     return fail(LMC_ERR_INVALID, "handle must not be null");
   if (h->tally_doubles && !h_tallies)
@@ -1730,6 +1761,7 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
   using namespace lmc;
   if (!opts)
     return fail(LMC_ERR_INVALID, "options must not be null");
+  NvtxRange range("lmc_run_noalloc");
   const lmc_status v = validate(s);
   if (v != LMC_OK)
     return v;
@@ -1753,81 +1785,16 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     return b;
   cudaStream_t stream = static_cast<cudaStream_t>(opts->stream);
 
-  // ---- device scene, built on the stack (no host or device allocation)
+  // ---- device scene, built on the stack (no device allocation): the same fields as
+  // lmc_create's, tables patched in below
   dev::Scene sc;
-  std::memset(&sc, 0, sizeof(sc));
-  sc.n_layers = s->n_layers;
-  sc.n_media = s->n_media;
-  sc.n_sensors = s->n_sensors;
-  sc.top = s->layers[s->n_layers - 1].z_max;
-  sc.top_is_inf = std::isinf(sc.top) ? 1 : 0;
-  sc.top_f = (float)sc.top;
-  sc.n_step = 1.0 / (1.0 / s->n_host);
-  fill_layers(s, sc);
-  const lmc_laser_desc &L = s->laser;
-  for (int j = 0; j < 3; ++j) {
-    sc.laser.pos[j] = L.position[j];
-    sc.laser.dir[j] = L.direction[j];
-    sc.laser.m[j] = L.local_m[j];
-    sc.laser.n[j] = L.local_n[j];
-  }
-  for (int j = 0; j < 4; ++j)
-    sc.laser.E[j] = L.jones[j];
-  sc.laser.k = 2.0 * M_PI / L.wavelength;
-  sc.laser.sigma = L.sigma;
-  sc.laser.source = L.source;
-  sc.laser.temporal = L.temporal;
-  sc.laser.pulse_duration = L.pulse_duration;
-  sc.laser.repetition_rate = L.repetition_rate;
-  sc.laser.time_offset = L.time_offset;
-  double planes[LMC_MAX_SENSORS];
-  int n_planes = 0;
-  size_t tally_doubles = 0;
-  unsigned cbs_mask = 0;
-  for (int i = 0; i < s->n_sensors; ++i) {
-    const lmc_sensor_desc &S = s->sensors[i];
-    dev::Sensor &d = sc.sensors[i];
-    size_t count = 0;
-    int dims[4];
-    fill_sensor(S, d, count, dims);
-    const double z = (S.kind == LMC_SENSOR_FARFIELD_CBS || S.kind == LMC_SENSOR_FARFIELD_FLUENCE) ? 0.0 : S.z;
-    if (S.kind == LMC_SENSOR_PLANAR_FIELD && !d.estimator)
-      sc.need_phase = 1;
-    if (S.kind == LMC_SENSOR_FARFIELD_CBS)
-      cbs_mask |= 1u << i;
-    if (S.kind == LMC_SENSOR_STATISTICS)
-      sc.stat_mask |= 1u << i;
-    int g = -1;
-    for (int k = 0; k < n_planes; ++k)
-      if (!(planes[k] < z - 1e-9) && !(z < planes[k] - 1e-9))
-        g = k;
-    if (g < 0) {
-      planes[n_planes] = z;
-      g = n_planes++;
-    }
-    d.plane = g;
-    d.tally_off = tally_doubles;
-    tally_doubles += count;
-  }
-  int rank[LMC_MAX_SENSORS];                                 // planes in ascending z
-  for (int k = 0; k < n_planes; ++k) {
-    int r = 0;
-    for (int q = 0; q < n_planes; ++q)
-      r += (planes[q] < planes[k] || (planes[q] == planes[k] && q < k)) ? 1 : 0;
-    rank[k] = r;
-    sc.plane_z[r] = planes[k];
-    sc.plane_z_f[r] = (float)planes[k];
-  }
-  for (int i = 0; i < s->n_sensors; ++i)
-    sc.sensors[i].plane = rank[sc.sensors[i].plane];
-  sc.n_planes = n_planes;
-  {
-    size_t abs_count = 0;
-    int abs_dims[4];
-    fill_absorption(s, sc, 0, tally_doubles, abs_count, abs_dims);
-  }
-  const bool queued = n_planes == 0 || sc.plane_z[n_planes - 1] <= 0.0;
-  sc.cbs_mask = cbs_mask;
+  size_t sensor_off[LMC_MAX_SENSORS], sensor_count[LMC_MAX_SENSORS], abs_off = 0, abs_count = 0;
+  int sensor_dims[LMC_MAX_SENSORS][4], abs_dims[4];
+  const size_t tally_doubles = fill_scene_head(s, 0, sc, sensor_off, sensor_count, sensor_dims,
+                                               &abs_off, &abs_count, abs_dims);
+  const bool queued = scene_queued(sc);
+  const int n_planes = sc.n_planes;
+  const unsigned cbs_mask = sc.cbs_mask;
   if (tally_doubles && !d_tallies)
     return fail(LMC_ERR_INVALID, "device tally buffer must not be null");
 
@@ -1867,23 +1834,10 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     const lmc_medium_desc &M = s->media[i];
     const MediumSpan &p = span[i];
     dev::Medium &d = sc.media[i];
-    d.theta_kind = M.theta_kind;
-    d.hg_g = M.hg_g;
-    d.hg_g_f = (float)M.hg_g;
-    d.mu_t = M.mu_a + M.mu_s;
-    d.mfp = M.mean_free_path;
-    d.mu_t_f = (float)d.mu_t;
-    d.mfp_f = (float)d.mfp;
-    d.amp_n = M.amp_n;
-    d.amp_inv_dx = 1.0 / M.amp_dtheta;
-    d.amp_inv_dx_f = (float)d.amp_inv_dx;
-    d.mu_s = M.mu_s;
-    d.mu_s_f = (float)M.mu_s;
-    const int nt = (M.theta_kind == LMC_THETA_TABLE || M.theta_kind == LMC_THETA_TABLE_COS) ? M.theta_n : 0;
+    const int nt = d.theta_n;
     DeriveArgs a;
     std::memset(&a, 0, sizeof(a));
     if (nt) {
-      d.theta_n = nt;
       d.th_val_d = reinterpret_cast<const double *>(tb + p.vals);
       d.th_cdf_d = reinterpret_cast<const double *>(tb + p.cdf);
       d.th_cs = reinterpret_cast<const double2 *>(tb + p.cs);
@@ -1939,19 +1893,20 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
   if (opts->stream_format != 0 && opts->stream_format != 1)
     return fail(LMC_ERR_INVALID, "stream_format must be 0 or 1");
   rp.stream_u24 = (!fp32 && opts->stream_format == 1) ? 1 : 0;
-  const int block = dev::kBlock;
-  const bool extras = scene_extras(sc);
-  const KernelFn tk =
-      extras ? (fp32 ? (queued ? dev::transport_kernel<float, true, 2, false, false, false, true>
-                               : dev::transport_kernel<float, false, 1, false, false, false, true>)
-                     : (queued ? dev::transport_kernel<double, true, 1, false, false, false, true>
-                               : dev::transport_kernel<double, false, 1, false, false, false, true>))
-             : (fp32 ? (queued ? dev::transport_kernel<float, true, 2> : dev::transport_kernel<float, false, 1>)
-                     : (queued ? dev::transport_kernel<double, true, 1> : dev::transport_kernel<double, false, 1>));
+  const int block = opts->block_size > 0 ? opts->block_size : dev::kBlock;
+  if (block % 32 != 0 || block > dev::kBlock)
+    return fail(LMC_ERR_INVALID, "block_size must be a multiple of 32 and at most 256");
+  // the kernels lmc_run picks for the same scene and options
+  const bool three = fp32 && queued && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
+  const KernelFn tk = pick_transport(fp32, queued, three, false, false, false, scene_extras(sc));
+  const KernelFn tl = pick_tally(fp32, false, false);
   const size_t dyn_transport = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
-  LMC_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_transport));
+  LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)dyn_transport));
   int per_sm = 0;
-  LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tk, block, dyn_transport));
+  LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)tk, block, dyn_transport));
+  if (opts->blocks_per_sm > 0)
+    per_sm = std::min(per_sm, opts->blocks_per_sm);
   per_sm = std::max(per_sm, 1);
   unsigned long long batch = n_photons;
   if (queued && n_photons > 0) {
@@ -1959,8 +1914,11 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
                          dev::kQRFields * (fp32 ? sizeof(float) : sizeof(double));
     const unsigned long long cap = (kNoAllocBytes - kNaQueueOff - 3 * 256) / entry;
     const unsigned long long planes_n = std::max(1, n_planes);
-    // cap = batch * planes + batch / 16 + 1024, as in lmc_run
+    // cap = batch * planes + batch / 16 + 1024, as in lmc_run; a smaller batch_photons
+    // of the options is honoured
     batch = std::min<unsigned long long>(n_photons, ((cap - 1024) * 16) / (16 * planes_n + 1));
+    if (opts->batch_photons)
+      batch = std::min<unsigned long long>(batch, opts->batch_photons);
     if (batch == 0)
       return fail(LMC_ERR_INVALID, "lmc_run_noalloc: too many sensor planes for the hit queue");
     unsigned char *q = base + kNaQueueOff;
@@ -1971,10 +1929,12 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     o += align((size_t)cap * dev::kQF64Fields * 8);
     rp.queue.r = q + o;
   }
+  lmc_record *const records = static_cast<lmc_record *>(opts->records);
   for (unsigned long long done = 0; done < n_photons; done += batch) {
     const unsigned long long nb = std::min(batch, n_photons - done);
     rp.photon_begin = photon_begin + done;
     rp.n_photons = nb;
+    rp.records = records ? records + done : nullptr;   // the kernels index from photon_begin
     LMC_CUDA(cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned long long), stream));
     const int grid = (int)std::max<unsigned long long>(
         1ull, std::min<unsigned long long>((unsigned long long)sm_count * per_sm, (nb + block - 1) / block));
@@ -1984,10 +1944,7 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
       const int tgrid = (int)std::max<unsigned long long>(
           1ull, std::min<unsigned long long>((unsigned long long)sm_count * 8,
                                              (rp.queue.cap + dev::kBlock - 1) / dev::kBlock));
-      if (fp32)
-        dev::tally_kernel<float><<<tgrid, dev::kBlock, 0, stream>>>(d_scene, rp);
-      else
-        dev::tally_kernel<double><<<tgrid, dev::kBlock, 0, stream>>>(d_scene, rp);
+      tl<<<tgrid, dev::kBlock, 0, stream>>>(d_scene, rp);
       LMC_CUDA(cudaGetLastError());
     }
   }

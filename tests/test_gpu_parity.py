@@ -147,6 +147,24 @@ def test_launch_shape_independence(cuda):
     b.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_records_over_several_batches(precision, cuda):
+    """A run split into hit-queue batches writes every photon's record at its own slot
+    (photon begin + i at records[i]), exactly as a one-batch run does."""
+    spec = W.bilayer_rgd_mie(2000, 37)
+    cfg, _, keep = W.build(lm, spec)
+    a = DeviceRun(cfg)
+    _, ra = a.run(2000, 37, 500, precision=precision, records=True)
+    b = DeviceRun(cfg)
+    _, rb = b.run(2000, 37, 500, precision=precision, records=True, batch_photons=300)
+    assert np.array_equal(rb["photon"], np.arange(500, 2500, dtype=rb["photon"].dtype))
+    assert ra.tobytes() == rb.tobytes()
+    for ga, gb in zip(a.host_tallies(), b.host_tallies()):
+        np.testing.assert_allclose(gb, ga, rtol=1e-12, atol=1e-12 * max(np.abs(ga).max(), 1e-300))
+    a.close()
+    b.close()
+
+
 def test_photon_ranges_compose(cuda):
     """Two runs over [0, n/2) and [n/2, n) tally the same as one run over [0, n)."""
     spec = W.mie_cbs_small(4000, 99)

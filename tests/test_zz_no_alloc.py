@@ -114,6 +114,27 @@ def test_noalloc_several_queue_batches(cuda):
     run.close()
 
 
+def test_noalloc_records_over_several_batches(cuda):
+    """Per-photon records of a run split into batches (a batch_photons below the
+    queue's own limit is honoured) equal lmc_run's one-batch records."""
+    import torch
+    spec = W.bilayer_rgd_mie(1500, 41)
+    cfg, _, keep = W.build(lm, spec)
+    run = DeviceRun(cfg)
+    _, want = run.run(1500, 41, 200, precision="fp64", records=True)
+    from luminis_mc_b200.device import RECORD_DTYPE
+    rec = torch.zeros(1500 * RECORD_DTYPE.itemsize, dtype=torch.uint8, device=run.device)
+    d = torch.zeros(max(run.transport.tally_size, 1), dtype=torch.float64, device=run.device)
+    torch.cuda.synchronize()
+    o = run.transport.opts(precision="fp64", records_ptr=rec.data_ptr(), batch_photons=400)
+    st = N.Stats()
+    N.check(N.lib().lmc_run_noalloc(C.byref(run.transport.scene), 41, 200, 1500, C.byref(o),
+                                    C.c_void_p(d.data_ptr()), C.byref(st)))
+    got = rec.cpu().numpy().view(RECORD_DTYPE)
+    assert got.tobytes() == want.tobytes()
+    run.close()
+
+
 def test_noalloc_rejects_tables_beyond_its_limit(cuda):
     """A scene whose tables exceed the static array's table region is refused with
     a message naming the size, and the next call still works."""
