@@ -13,9 +13,12 @@ tallies and hit counts:
   stat_ref_<scene>.npz     R independent-seed replicas of the unmodified reference
                            (its own RNG): per-bin mean and variance of tally / N,
                            the statistical oracle for other random streams
+  cone_ref_<scene>.npz     the same for the FarFieldCBS grids of the workloads, plus
+                           every replica's theta profiles of S0 coherent / incoherent
 
     python tests/golden/make_golden.py        (needs oracle/_ref; run `make -C oracle ref`)
     python tests/golden/make_golden.py stat   (the replica fixtures only)
+    python tests/golden/make_golden.py cone   (CBS cone replicas at the workloads' resolution)
     python tests/golden/make_golden.py farfield  (far-field fluence from reference records)
     python tests/golden/make_golden.py estimator (estimator-mode FarFieldCBS, Philox stream)
     python tests/golden/make_golden.py mixture   (MixtureLayer scenes, both streams)
@@ -128,6 +131,70 @@ np.savez_compressed(sys.argv[1], **out)
 def stat_main():
     for spec in stat_scenes():
         print("wrote", run_stat_reference(spec["name"]))
+
+
+CONE_REPLICAS = 16
+CONE_PHOTONS = 1_000_000
+
+
+def cone_scenes():
+    """The CBS cone at the resolution the workloads use: the mie_cbs_small detector as
+    written (100 theta bins of 1 mrad to 0.1 rad, one phi bin, mu_a = 0.01/mm) and the
+    bilayer_rgd_mie FarFieldCBS grid (200 x 8 bins to 0.1 rad) alone on that geometry.
+    1e6 photons per replica put tens of photons into the innermost 10 mrad, where the
+    enhancement eta = S0_coh / S0_incoh peaks."""
+    a = W.mie_cbs_small(CONE_PHOTONS, 1)
+    a["name"] = "cone_mie"
+    b = W.bilayer_rgd_mie(CONE_PHOTONS, 1)
+    b["name"] = "cone_bilayer"
+    b["sensors"] = [b["sensors"][0]]
+    return [a, b]
+
+
+def cone_profiles(tally):
+    """S0 coherent and incoherent of a FarFieldCBS tally [8][N_t][N_theta][N_phi],
+    time bin 0, summed over phi: two profiles over theta."""
+    t = np.asarray(tally)
+    return t[0, 0].sum(axis=-1), t[4, 0].sum(axis=-1)
+
+
+def run_cone_reference(scene_name, seed0=1000, path=None):
+    """R replicas of one cone scene with the reference's own RNG (pin build), in a fresh
+    interpreter: per-bin moments of the full grid and every replica's theta profiles of
+    S0 coherent / incoherent (for the enhancement near theta = 0)."""
+    code = f"""
+import os, sys, numpy as np
+sys.path.insert(0, {REPO!r}); sys.path.insert(0, {os.path.join(REPO, 'luminis-mc_b200')!r})
+from tests.golden.make_golden import (cone_scenes, cone_profiles, replica_moments,
+                                      CONE_REPLICAS, CONE_PHOTONS)
+from luminis_mc_b200 import workloads as W
+from oracle import pyoracle as O
+lm = O.reference_module("pin"); lm.set_log_level(lm.LogLevel.off)
+spec = [s for s in cone_scenes() if s["name"] == {scene_name!r}][0]
+reps, coh, inc = [], [], []
+for r in range(CONE_REPLICAS):
+    cfg, hs, keep = W.build(lm, spec, seed={seed0} + r, n_threads=os.cpu_count())
+    lm.run_simulation_parallel(cfg)
+    t = [W.tally_arrays(h, s["kind"]) for h, s in zip(hs, spec["sensors"])]
+    reps.append(t)
+    c, i = cone_profiles(t[0])
+    coh.append(c)
+    inc.append(i)
+out = {{"R": np.int64(CONE_REPLICAS), "N": np.int64(CONE_PHOTONS),
+       "coh_theta": np.stack(coh), "incoh_theta": np.stack(inc)}}
+for i, (m, v) in enumerate(replica_moments(reps, CONE_PHOTONS)):
+    out[f"sensor{{i}}_mean"] = m
+    out[f"sensor{{i}}_var"] = v
+np.savez_compressed(sys.argv[1], **out)
+"""
+    path = path or os.path.join(HERE, f"cone_ref_{scene_name}.npz")
+    subprocess.run([sys.executable, "-c", code, path], check=True)
+    return path
+
+
+def cone_main():
+    for spec in cone_scenes():
+        print("wrote", run_cone_reference(spec["name"]))
 
 
 def estimator_scenes():
@@ -401,6 +468,8 @@ def main():
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "stat":
         stat_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "cone":
+        cone_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "farfield":
         farfield_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "estimator":
