@@ -193,8 +193,11 @@ struct RunParams {
   const AdjScene *adj_scenes;
   // estimator-mode FarFieldCBS grids accumulated per block in shared memory: sensor i's
   // copy at est_smem[i] doubles into the block's grid area (-1: global atomics)
+  // est_per_warp: each warp of the block has its own copy of those grids, est_warp_doubles
+  // apart (the block's est_smem_doubles = warps x est_warp_doubles)
   int est_smem[LMC_MAX_SENSORS];
   int est_smem_doubles;
+  int est_per_warp, est_warp_doubles;
 };
 
 }  // namespace dev

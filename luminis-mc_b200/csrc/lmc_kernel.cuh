@@ -1094,18 +1094,7 @@ __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData
 // centre of every angular bin of an estimator-mode FarFieldCBS grid.  The bin gets the
 // weight w mu_s / mu_t x transmittance to the plane x p(Omega) dOmega, with
 // p = F / (pi I_norm), and the forward field.  From the second vertex on it also gets
-// the reverse (CBS) field with its geometric phase.  Computed in binary64 whatever the
-// transport precision.  One thread runs all bins of its own vertex, starting at a
-// lane-dependent bin so that the lanes of a warp update different tally cells at
-// each step.
-struct EstVertex {
-  double pos[3], P[9], P1[9], r1[3];
-  Cx<double> Em, En, T[4];      // Jones vector; interior product including the newest event
-  double w, opath;
-  unsigned long long index;
-  int events, med, first_med, layer;
-};
-
+// the reverse (CBS) field with its geometric phase.
 __device__ __forceinline__ V3<double> drow(const double *P, int r)
 {
   return v3<double>(P[3 * r], P[3 * r + 1], P[3 * r + 2]);
@@ -1220,339 +1209,419 @@ __device__ __forceinline__ double est_optical_depth(const Scene &sc, const doubl
   return tau;
 }
 
-template <typename R>
-__device__ __noinline__ void estimate_vertex(const Scene &sc, const RunParams &rp, const EstVertex v,
-                                             unsigned long long *s_hits, double *s_est)
-{
-  const Laser &L = sc.laser;
-  const V3<double> s_in = v3<double>(L.dir[0], L.dir[1], L.dir[2]);
-  const V3<double> m_cur = drow(v.P, 0), n_cur = drow(v.P, 1), s_cur = drow(v.P, 2);
-  const Medium &med = sc.media[v.med];
-  const unsigned lane = threadIdx.x & 31u;
-  for (int si = 0; si < sc.n_sensors; ++si) {
-    const Sensor &s = sc.sensors[si];
-    if (s.kind != LMC_SENSOR_FARFIELD_CBS || !s.estimator)
-      continue;
-    if (s.f_events && (v.events < s.events_min || v.events > s.events_max))
-      continue;
-    if (med.I_norm < 1e-300)
-      continue;
-    // the layer's aggregate albedo at the first vertex (src/detector.cpp:1378), the
-    // selected species' own later (:1472); the same for a HomogeneousLayer
-    const Layer &VL = sc.layers[v.layer];
-    const double w_scatter = v.w * (v.events == 0 ? VL.mu_s / VL.mu_t : med.mu_s / med.mu_t);
-    if (w_scatter < 1e-300)
-      continue;
-    const bool multi = v.events >= 1;
-    Cx<double> pre_m = {0.0, 0.0}, pre_n = {0.0, 0.0};
-    if (multi)
-      est_prefix(sc, v.P, v.T, v.med, pre_m, pre_n);
-    const double t_launch = (s.dt > 0) ? emission_time<R>(L, rp, v.index) : 0.0;
-    // the block's shared copy of the grid when it has one, else the tallies
-    double *base = rp.est_smem[si] >= 0 ? s_est + rp.est_smem[si] : rp.tallies + s.tally_off;
-    const unsigned long long P = s.plane_stride;
-    const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
-    const int nb = s.est_n;
-    for (int k = 0; k < nb; ++k) {
-      int b = k + (int)lane;
-      if (b >= nb)
-        b -= nb * (b / nb);
-      const double4 bin = s.est_bins[b];
-      const V3<double> s_out = v3<double>(bin.x, bin.y, bin.z);
-      const double denom = s_out.z;                        // plane z = 0, normal +z
-      if (fabs(denom) < 1e-14)
-        continue;
-      const double Lp = (-v.pos[2]) / denom;
-      if (Lp <= 0.0)
-        continue;
-      const double Tr = exp(-est_optical_depth(sc, v.pos, s_out, Lp));
-      if (Tr < 1e-20)
-        continue;
-      const V3<double> pv = vcross_unit(s_cur, s_out);
-      const double pn = sqrt(vdot(pv, pv));
-      if (pn < 1e-12)
-        continue;
-      const V3<double> p_hat = vscale(pv, 1.0 / pn);
-      const double sin_phi = -vdot(m_cur, p_hat);
-      const double cos_phi = vdot(n_cur, p_hat);
-      double cdot = vdot(s_cur, s_out);
-      cdot = cdot > 1.0 ? 1.0 : (cdot < -1.0 ? -1.0 : cdot);
-      const double th_scat = acos(cdot);
-      Cx<double> S2, S1;
-      amplitudes<double>(med, th_scat, S2, S1);
-      const double s22 = cnorm(S2), s11 = cnorm(S1);
-      const double Emm = cnorm(v.Em), Enn = cnorm(v.En);
-      const double c2 = cos_phi * cos_phi, sn2 = sin_phi * sin_phi;
-      const double e12 = v.Em.re * v.En.re + v.Em.im * v.En.im;
-      const double F = Emm * (s22 * c2 + s11 * sn2) + Enn * (s22 * sn2 + s11 * c2) +
-                       2.0 * e12 * (s22 - s11) * sin_phi * cos_phi;
-      if (F < 1e-300)
-        continue;
-      const double prob_bin = (F / (3.141592653589793 * med.I_norm)) * bin.w;
-      const double w_bin = w_scatter * Tr * prob_bin;
-      if (w_bin < 1e-300)
-        continue;
-      const int t_idx = time_bin(s, t_launch + (v.opath + Lp));
-      if (t_idx < 0)
-        continue;
-      // amp = sqrt(w_bin) exp(i k L) in the reference (src/detector.cpp:1425, :1533); the
-      // phase multiplies the forward and the reverse field alike and cancels in every
-      // Stokes value, so only the modulus is formed
-      const Cx<double> amp = {sqrt(w_bin), 0.0};
-      // exit frame A(theta, phi) P (src/detector.cpp:1027-1045)
-      double st, ct;
-      sincos(th_scat, &st, &ct);
-      double Pe[9];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const double mj = v.P[j], nj = v.P[3 + j], sj = v.P[6 + j];
-        Pe[j] = ct * cos_phi * mj + ct * sin_phi * nj + (-st) * sj;
-        Pe[3 + j] = -sin_phi * mj + cos_phi * nj + 0.0 * sj;
-        Pe[6 + j] = st * cos_phi * mj + st * sin_phi * nj + ct * sj;
-      }
-      // forward field (S R(phi)) E / sqrt(F) (src/detector.cpp:121-160)
-      const double inv = 1.0 / sqrt(F);
-      const Cx<double> T00 = cscale(S2, cos_phi), T01 = cscale(S2, sin_phi);
-      const Cx<double> T10 = cscale(S1, -sin_phi), T11 = cscale(S1, cos_phi);
-      const Cx<double> Efm = cmul(cscale(cadd(cmul(T00, v.Em), cmul(T01, v.En)), inv), amp);
-      const Cx<double> Efn = cmul(cscale(cadd(cmul(T10, v.Em), cmul(T11, v.En)), inv), amp);
-      const Cx<double> Efx = cadd(cscale(Efm, Pe[0]), cscale(Efn, Pe[3]));
-      const Cx<double> Efy = cadd(cscale(Efm, Pe[1]), cscale(Efn, Pe[4]));
-      Cx<double> Erx = {0.0, 0.0}, Ery = {0.0, 0.0};
-      if (multi) {
-        Cx<double> Rm, Rn;
-        est_suffix(sc, v.P1, Pe, v.first_med, pre_m, pre_n, Rm, Rn);
-        const double qx = (s_out.x + s_in.x) * L.k, qy = (s_out.y + s_in.y) * L.k,
-                     qz = (s_out.z + s_in.z) * L.k;
-        const double arg = qx * (v.pos[0] - v.r1[0]) + qy * (v.pos[1] - v.r1[1]) + qz * (v.pos[2] - v.r1[2]);
-        double sp_, cp_;
-        sincos(arg, &sp_, &cp_);
-        const Cx<double> pp = {cp_, sp_};
-        const Cx<double> Rm2 = cmul(cmul(Rm, amp), pp), Rn2 = cmul(cmul(Rn, amp), pp);
-        Erx = cadd(cscale(Rm2, Pe[0]), cscale(Rn2, Pe[3]));
-        Ery = cadd(cscale(Rm2, Pe[1]), cscale(Rn2, Pe[4]));
-      }
-      // accumulate_stokes (src/detector.cpp:1194-1226)
-      const Cx<double> Ex = cadd(Efx, Erx), Ey = cadd(Efy, Ery);
-      const Cx<double> c_xy = cmul(Ex, Cx<double>{Ey.re, -Ey.im});
-      const Cx<double> f_xy = cmul(Efx, Cx<double>{Efy.re, -Efy.im});
-      const Cx<double> r_xy = cmul(Erx, Cx<double>{Ery.re, -Ery.im});
-      const double c0 = cnorm(Ex) + cnorm(Ey), c1 = cnorm(Ex) - cnorm(Ey);
-      const double c2s = 2.0 * c_xy.re, c3 = 2.0 * c_xy.im;
-      const double i0 = cnorm(Efx) + cnorm(Efy) + cnorm(Erx) + cnorm(Ery);
-      const double i1 = cnorm(Efx) - cnorm(Efy) + cnorm(Erx) - cnorm(Ery);
-      const double i2 = 2.0 * (f_xy.re + r_xy.re), i3 = 2.0 * (f_xy.im + r_xy.im);
-      const unsigned long long cell = (unsigned long long)(b / s.N_phi) * s.N_phi + (b % s.N_phi);
-      add4(base, P, cell, c0, c1, c2s, c3);
-      add4(base + 4 * P, P, cell, i0, i1, i2, i3);
-      if (t_idx >= 1) {
-        add4(base, P, t_idx * tstride + cell, c0, c1, c2s, c3);
-        add4(base + 4 * P, P, t_idx * tstride + cell, i0, i1, i2, i3);
-      }
-    }
-    atomicAdd(s_hits + si, 1ull);
+// ------------------------------------------------ warp-cooperative estimation
+// The 32 lanes of a warp estimate together.  Every lane whose photon is at a vertex
+// prepares it (filters, weight, the reverse-path prefix, launch time); the warp then
+// takes the prepared vertices one at a time, broadcast by shuffles, and lane j
+// evaluates bins j, j + 32, ... of the grid.  A vertex so deep that the
+// transmittance to the plane is below the reference's cut (1e-20) for every bin is
+// skipped by the whole warp instead of by each bin.  The 32 lanes of one step write
+// 32 different cells, so a warp can accumulate into a private copy of the grid
+// with plain adds.
+
+// Where a sensor's estimate accumulates: the warp's private copy of the grid in
+// shared memory (plain adds), the block's shared copy (shared atomics: several warps
+// write it), or the tallies (global atomics).
+struct EstTarget {
+  double *base;
+  bool atomic;
+  __device__ __forceinline__ void add(unsigned long long off, double v) const
+  {
+    if (atomic)
+      atomicAdd(base + off, v);
+    else
+      base[off] += v;
   }
+  __device__ __forceinline__ void add4(unsigned long long stride, unsigned long long off, double a,
+                                       double b, double c, double d) const
+  {
+    add(off, a);
+    add(stride + off, b);
+    add(2 * stride + off, c);
+    add(3 * stride + off, d);
+  }
+};
+
+__device__ __forceinline__ EstTarget est_target(const RunParams &rp, const Sensor &s, int si, double *s_est)
+{
+  if (rp.est_smem[si] < 0)
+    return {rp.tallies + s.tally_off, true};
+  if (rp.est_per_warp)
+    return {s_est + (threadIdx.x >> 5) * rp.est_warp_doubles + rp.est_smem[si], false};
+  return {s_est + rp.est_smem[si], true};
 }
 
-// The vertex a photon is at, as the estimator reads it.
-// The same estimate in binary32 for binary32 transport (the CBS phase excepted): bin
-// directions from the binary32 copy of the bin table, the scattering angle as
-// atan2(|s_cur x s_out|, s_cur . s_out), binary32 amplitudes, transmittance, fields and
-// Stokes values, accumulated in binary64.  exp(i k L) multiplies the forward and the
-// reverse field alike and cancels in every Stokes value, so it is not formed; the CBS
-// phase q . (r_n - r_1) uses the table's q = k (s_out + s_in), formed in binary64.
-template <typename R>
-__device__ __noinline__ void estimate_vertex_f32(const Scene &sc, const RunParams &rp, const EstVertex v,
-                                                 unsigned long long *s_hits, double *s_est)
+// A vertex as the estimate reads it, in the estimate's precision T (binary64 for
+// binary64 transport, binary32 for binary32 transport, whose positions are binary32
+// already).  Small, because every lane holds its own vertex and the one broadcast.
+template <typename T> struct EstV {
+  T P[9], P1[9];                // frame at the vertex; frame after the first scatter
+  Cx<T> Em, En;                 // Jones vector
+  Cx<T> pre_m, pre_n;           // reverse path through stages A + B (from the 2nd vertex)
+  T pos[3];                     // vertex
+  T dr[3];                      // r_n - r_1 (CBS phase), formed in binary64
+  T wgt;                        // binary64: w mu_s / mu_t; binary32: that / (pi I_norm)
+  double opath, t_launch;       // broadcast only for a time-resolved grid
+  int ids;                      // medium | first medium << 8 | layer << 16 | multi << 24
+  __device__ __forceinline__ int med() const { return ids & 0xff; }
+  __device__ __forceinline__ int first_med() const { return (ids >> 8) & 0xff; }
+  __device__ __forceinline__ int layer() const { return (ids >> 16) & 0xff; }
+  __device__ __forceinline__ bool multi() const { return (ids >> 24) & 1; }
+};
+
+template <typename T> __device__ __forceinline__ void est_bcast(EstV<T> &v, int src, bool timed)
 {
-  const Laser &L = sc.laser;
-  float P[9], P1[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) {
-    P[j] = (float)v.P[j];
-    P1[j] = (float)v.P1[j];
+    v.P[j] = __shfl_sync(kFull, v.P[j], src);
+    v.P1[j] = __shfl_sync(kFull, v.P1[j], src);
   }
-  const V3<float> m_cur = trow<float>(P, 0), n_cur = trow<float>(P, 1), s_cur = trow<float>(P, 2);
-  const Cx<float> Em = {(float)v.Em.re, (float)v.Em.im}, En = {(float)v.En.re, (float)v.En.im};
-  const float dr[3] = {(float)(v.pos[0] - v.r1[0]), (float)(v.pos[1] - v.r1[1]), (float)(v.pos[2] - v.r1[2])};
-  const Medium &med = sc.media[v.med];
-  const unsigned lane = threadIdx.x & 31u;
-  for (int si = 0; si < sc.n_sensors; ++si) {
-    const Sensor &s = sc.sensors[si];
-    if (s.kind != LMC_SENSOR_FARFIELD_CBS || !s.estimator)
-      continue;
-    if (s.f_events && (v.events < s.events_min || v.events > s.events_max))
-      continue;
-    if (med.I_norm < 1e-300)
-      continue;
-    const Layer &VL = sc.layers[v.layer];
-    const double w_scatter = v.w * (v.events == 0 ? VL.mu_s / VL.mu_t : med.mu_s / med.mu_t);
-    if (w_scatter < 1e-300)
-      continue;
-    const bool multi = v.events >= 1;
-    Cx<float> pre_m = {0.f, 0.f}, pre_n = {0.f, 0.f};
-    if (multi) {
-      const Cx<float> T[4] = {{(float)v.T[0].re, (float)v.T[0].im}, {(float)v.T[1].re, (float)v.T[1].im},
-                              {(float)v.T[2].re, (float)v.T[2].im}, {(float)v.T[3].re, (float)v.T[3].im}};
-      est_prefix<float>(sc, P, T, v.med, pre_m, pre_n);
-    }
-    const double t_launch = (s.dt > 0) ? emission_time<R>(L, rp, v.index) : 0.0;
-    // p(Omega) dOmega = F / (pi I_norm) x dOmega dphi; w_scatter folded in
-    const float pref = (float)(w_scatter / (3.141592653589793 * med.I_norm));
-    const float mu_t1 = sc.layers[v.layer].mu_t_f;
-    const float pz = (float)v.pos[2];
-    const float Emm = cnorm(Em), Enn = cnorm(En);
-    const float e12 = Em.re * En.re + Em.im * En.im;
-    double *base = rp.est_smem[si] >= 0 ? s_est + rp.est_smem[si] : rp.tallies + s.tally_off;
-    const unsigned long long PS = s.plane_stride;
-    const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
-    const int nb = s.est_n;
-    const float4 *bf = reinterpret_cast<const float4 *>(s.est_bins + nb);
-    for (int k = 0; k < nb; ++k) {
-      int b = k + (int)lane;
-      if (b >= nb)
-        b -= nb * (b / nb);
-      const float4 bin = bf[2 * b];
-      const V3<float> s_out = v3<float>(bin.x, bin.y, bin.z);
-      const float denom = s_out.z;                         // plane z = 0, normal +z
-      if (fabsf(denom) < 1e-14f)
-        continue;
-      const float Lp = -pz / denom;
-      if (!(Lp > 0.f))
-        continue;
-      const float tau = sc.n_layers == 1
-          ? mu_t1 * Lp
-          : (float)est_optical_depth(sc, v.pos, v3<double>(bin.x, bin.y, bin.z), (double)Lp);
-      const float Tr = expf(-tau);
-      if (Tr < 1e-20f)
-        continue;
-      // |s_cur x s_out| = sin(theta_scat) of the two unit vectors; its direction is the
-      // scattering plane's normal p_hat (vcross_unit, src/vec.cpp:14-26)
-      const V3<float> pv = {s_cur.y * s_out.z - s_cur.z * s_out.y, s_cur.z * s_out.x - s_cur.x * s_out.z,
-                            s_cur.x * s_out.y - s_cur.y * s_out.x};
-      const float pn = sqrtf(vdot(pv, pv));
-      if (!(pn > 0.f))
-        continue;
-      const V3<float> p_hat = vscale(pv, 1.f / pn);
-      const float sin_phi = -vdot(m_cur, p_hat);
-      const float cos_phi = vdot(n_cur, p_hat);
-      const float cdot = vdot(s_cur, s_out);
-      const float th_scat = atan2f(pn, cdot);
-      Cx<float> S2, S1;
-      amplitudes<float>(med, th_scat, S2, S1);
-      const float s22 = cnorm(S2), s11 = cnorm(S1);
-      const float c2 = cos_phi * cos_phi, sn2 = sin_phi * sin_phi;
-      const float F = Emm * (s22 * c2 + s11 * sn2) + Enn * (s22 * sn2 + s11 * c2) +
-                      2.f * e12 * (s22 - s11) * sin_phi * cos_phi;
-      if (!(F > 0.f))
-        continue;
-      const float w_bin = pref * Tr * F * bin.w;
-      if (!(w_bin > 0.f))
-        continue;
-      const int t_idx = time_bin(s, t_launch + (v.opath + (double)Lp));
-      if (t_idx < 0)
-        continue;
-      const float amp = sqrtf(w_bin);
-      // exit frame A(theta, phi) P (src/detector.cpp:1027-1045): cos, sin of th_scat
-      const float ih = rsqrtf(cdot * cdot + pn * pn);
-      const float ct = cdot * ih, st = pn * ih;
-      float Pe[9];
+  v.Em.re = __shfl_sync(kFull, v.Em.re, src);
+  v.Em.im = __shfl_sync(kFull, v.Em.im, src);
+  v.En.re = __shfl_sync(kFull, v.En.re, src);
+  v.En.im = __shfl_sync(kFull, v.En.im, src);
+  v.pre_m.re = __shfl_sync(kFull, v.pre_m.re, src);
+  v.pre_m.im = __shfl_sync(kFull, v.pre_m.im, src);
+  v.pre_n.re = __shfl_sync(kFull, v.pre_n.re, src);
+  v.pre_n.im = __shfl_sync(kFull, v.pre_n.im, src);
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const float mj = P[j], nj = P[3 + j], sj = P[6 + j];
-        Pe[j] = ct * cos_phi * mj + ct * sin_phi * nj - st * sj;
-        Pe[3 + j] = -sin_phi * mj + cos_phi * nj;
-        Pe[6 + j] = st * cos_phi * mj + st * sin_phi * nj + ct * sj;
-      }
-      // forward field (S R(phi)) E / sqrt(F) (src/detector.cpp:121-160)
-      const float inv = amp * rsqrtf(F);
-      const Cx<float> T00 = cscale(S2, cos_phi), T01 = cscale(S2, sin_phi);
-      const Cx<float> T10 = cscale(S1, -sin_phi), T11 = cscale(S1, cos_phi);
-      const Cx<float> Efm = cscale(cadd(cmul(T00, Em), cmul(T01, En)), inv);
-      const Cx<float> Efn = cscale(cadd(cmul(T10, Em), cmul(T11, En)), inv);
-      const Cx<float> Efx = cadd(cscale(Efm, Pe[0]), cscale(Efn, Pe[3]));
-      const Cx<float> Efy = cadd(cscale(Efm, Pe[1]), cscale(Efn, Pe[4]));
-      Cx<float> Erx = {0.f, 0.f}, Ery = {0.f, 0.f};
-      if (multi) {
-        Cx<float> Rm, Rn;
-        est_suffix<float>(sc, P1, Pe, v.first_med, pre_m, pre_n, Rm, Rn);
-        const float4 q = bf[2 * b + 1];
-        const float arg = q.x * dr[0] + q.y * dr[1] + q.z * dr[2];
-        float sp_, cp_;
-        sincosf(arg, &sp_, &cp_);
-        const Cx<float> pp = {cp_ * amp, sp_ * amp};
-        const Cx<float> Rm2 = cmul(Rm, pp), Rn2 = cmul(Rn, pp);
-        Erx = cadd(cscale(Rm2, Pe[0]), cscale(Rn2, Pe[3]));
-        Ery = cadd(cscale(Rm2, Pe[1]), cscale(Rn2, Pe[4]));
-      }
-      // accumulate_stokes (src/detector.cpp:1194-1226)
-      const Cx<float> Ex = cadd(Efx, Erx), Ey = cadd(Efy, Ery);
-      const Cx<float> c_xy = cmul(Ex, Cx<float>{Ey.re, -Ey.im});
-      const Cx<float> f_xy = cmul(Efx, Cx<float>{Efy.re, -Efy.im});
-      const Cx<float> r_xy = cmul(Erx, Cx<float>{Ery.re, -Ery.im});
-      const double c0 = cnorm(Ex) + cnorm(Ey), c1 = cnorm(Ex) - cnorm(Ey);
-      const double c2s = 2.0 * c_xy.re, c3 = 2.0 * c_xy.im;
-      const double i0 = cnorm(Efx) + cnorm(Efy) + cnorm(Erx) + cnorm(Ery);
-      const double i1 = cnorm(Efx) - cnorm(Efy) + cnorm(Erx) - cnorm(Ery);
-      const double i2 = 2.0 * ((double)f_xy.re + r_xy.re), i3 = 2.0 * ((double)f_xy.im + r_xy.im);
-      const unsigned long long cell = (unsigned long long)(b / s.N_phi) * s.N_phi + (b % s.N_phi);
-      add4(base, PS, cell, c0, c1, c2s, c3);
-      add4(base + 4 * PS, PS, cell, i0, i1, i2, i3);
-      if (t_idx >= 1) {
-        add4(base, PS, t_idx * tstride + cell, c0, c1, c2s, c3);
-        add4(base + 4 * PS, PS, t_idx * tstride + cell, i0, i1, i2, i3);
-      }
-    }
-    atomicAdd(s_hits + si, 1ull);
+  for (int j = 0; j < 3; ++j) {
+    v.pos[j] = __shfl_sync(kFull, v.pos[j], src);
+    v.dr[j] = __shfl_sync(kFull, v.dr[j], src);
+  }
+  v.wgt = __shfl_sync(kFull, v.wgt, src);
+  v.ids = __shfl_sync(kFull, v.ids, src);
+  if (timed) {
+    v.opath = __shfl_sync(kFull, v.opath, src);
+    v.t_launch = __shfl_sync(kFull, v.t_launch, src);
   }
 }
 
-template <typename R>
-__device__ __forceinline__ void estimate_at_vertex(const Scene &sc, const RunParams &rp, const Photon<R> &ph,
-                                                   const Side<R> &side, int med_idx, unsigned long long *s_hits)
+// This lane's vertex for sensor s: false when process_estimation would return before
+// the bin loop (events filter, I_norm, weight; src/detector.cpp:1356-1380).  The
+// interior product folds the newest event's raw factor into the committed one from
+// two events on (src/detector.cpp:1462-1469), in binary64.
+template <typename T, typename R>
+__device__ __forceinline__ bool est_prepare(const Scene &sc, const RunParams &rp, const Photon<R> &ph,
+                                            const Side<R> &side, int med_idx, const Sensor &s, EstV<T> &v)
 {
-  extern __shared__ __align__(16) unsigned char s_dyn[];
-  double *s_est = reinterpret_cast<double *>(s_dyn + side_bytes<R>());
+  if (s.f_events && ((int)ph.events < s.events_min || (int)ph.events > s.events_max))
+    return false;
+  const Medium &med = sc.media[med_idx];
+  if (med.I_norm < 1e-300)
+    return false;
+  // the layer's aggregate albedo at the first vertex (src/detector.cpp:1378), the
+  // selected species' own later (:1472); the same for a HomogeneousLayer
+  const Layer &VL = sc.layers[ph.layer];
+  const double w_scatter = ph.w * (ph.events == 0 ? VL.mu_s / VL.mu_t : med.mu_s / med.mu_t);
+  if (w_scatter < 1e-300)
+    return false;
+  v.wgt = sizeof(T) == 8 ? (T)w_scatter : (T)(w_scatter / (3.141592653589793 * med.I_norm));
   const int tid = threadIdx.x;
-  EstVertex v;
-  v.pos[0] = ph.px; v.pos[1] = ph.py; v.pos[2] = ph.pz;
+  const double px = ph.px, py = ph.py, pz = ph.pz;
+  v.pos[0] = (T)px; v.pos[1] = (T)py; v.pos[2] = (T)pz;
+  v.dr[0] = (T)(px - (double)side.first[0][tid]);
+  v.dr[1] = (T)(py - (double)side.first[1][tid]);
+  v.dr[2] = (T)(pz - (double)side.first[2][tid]);
 #pragma unroll
   for (int j = 0; j < 9; ++j) {
-    v.P[j] = ph.P[j];
-    v.P1[j] = side.first[3 + j][tid];
+    v.P[j] = (T)ph.P[j];
+    v.P1[j] = (T)side.first[3 + j][tid];
   }
-#pragma unroll
-  for (int j = 0; j < 3; ++j)
-    v.r1[j] = side.first[j][tid];
-  v.Em = {ph.Em.re, ph.Em.im};
-  v.En = {ph.En.re, ph.En.im};
-  v.w = ph.w;
+  v.Em = {(T)ph.Em.re, (T)ph.Em.im};
+  v.En = {(T)ph.En.re, (T)ph.En.im};
   v.opath = ph.opath;
-  v.index = ph.index();
-  v.events = (int)ph.events;
-  v.med = med_idx;
-  v.layer = ph.layer;
-  v.first_med = side.first_med[tid];
-  // interior product for the estimated path (src/detector.cpp:1462-1469): the
-  // newest event's raw factor folded into the committed product (from 2 events on)
-  const Cx<double> T0 = {side.T[0][tid], side.T[1][tid]}, T1 = {side.T[2][tid], side.T[3][tid]};
-  const Cx<double> T2 = {side.T[4][tid], side.T[5][tid]}, T3 = {side.T[6][tid], side.T[7][tid]};
-  if (ph.events >= 2) {
-    const Cx<double> pS2 = {side.last[0][tid], side.last[1][tid]};
-    const Cx<double> pS1 = {side.last[2][tid], side.last[3][tid]};
-    const double pc = side.last[4][tid], ps = side.last[5][tid];
-    const Cx<double> B00 = cscale(pS2, pc), B01 = cscale(pS2, ps), B10 = cscale(pS1, -ps), B11 = cscale(pS1, pc);
-    v.T[0] = cadd(cmul(B00, T0), cmul(B01, T2));
-    v.T[1] = cadd(cmul(B00, T1), cmul(B01, T3));
-    v.T[2] = cadd(cmul(B10, T0), cmul(B11, T2));
-    v.T[3] = cadd(cmul(B10, T1), cmul(B11, T3));
-  } else {
-    v.T[0] = T0; v.T[1] = T1; v.T[2] = T2; v.T[3] = T3;
+  const bool multi = ph.events >= 1;
+  v.ids = med_idx | (side.first_med[tid] << 8) | (ph.layer << 16) | ((multi ? 1 : 0) << 24);
+  v.pre_m = {T(0), T(0)};
+  v.pre_n = {T(0), T(0)};
+  if (multi) {
+    const Cx<double> T0 = {side.T[0][tid], side.T[1][tid]}, T1 = {side.T[2][tid], side.T[3][tid]};
+    const Cx<double> T2 = {side.T[4][tid], side.T[5][tid]}, T3 = {side.T[6][tid], side.T[7][tid]};
+    Cx<double> Td[4] = {T0, T1, T2, T3};
+    if (ph.events >= 2) {
+      const Cx<double> pS2 = {side.last[0][tid], side.last[1][tid]};
+      const Cx<double> pS1 = {side.last[2][tid], side.last[3][tid]};
+      const double pc = side.last[4][tid], ps = side.last[5][tid];
+      const Cx<double> B00 = cscale(pS2, pc), B01 = cscale(pS2, ps), B10 = cscale(pS1, -ps),
+                       B11 = cscale(pS1, pc);
+      Td[0] = cadd(cmul(B00, T0), cmul(B01, T2));
+      Td[1] = cadd(cmul(B00, T1), cmul(B01, T3));
+      Td[2] = cadd(cmul(B10, T0), cmul(B11, T2));
+      Td[3] = cadd(cmul(B10, T1), cmul(B11, T3));
+    }
+    const Cx<T> Tt[4] = {{(T)Td[0].re, (T)Td[0].im}, {(T)Td[1].re, (T)Td[1].im},
+                         {(T)Td[2].re, (T)Td[2].im}, {(T)Td[3].re, (T)Td[3].im}};
+    est_prefix<T>(sc, v.P, Tt, med_idx, v.pre_m, v.pre_n);
   }
-  if (sizeof(R) == 4)
-    estimate_vertex_f32<R>(sc, rp, v, s_hits, s_est);
-  else
-    estimate_vertex<R>(sc, rp, v, s_hits, s_est);
+  v.t_launch = (s.dt > 0) ? emission_time<R>(sc.laser, rp, ph.index()) : 0.0;
+  return true;
+}
+
+// Whether a vertex at depth z > 0 in `layer` can reach the plane z = 0 with a
+// transmittance of 1e-20 or more for some bin: the path to the plane is at least z
+// and crosses only the layers from 0 to `layer`, so its optical depth is at least
+// z times the smallest mu_t among them; e^-47 < 1e-20 leaves a margin over the
+// per-bin test's rounding.
+__device__ __forceinline__ bool est_reachable(const Scene &sc, double z, int layer)
+{
+  double mu = sc.layers[0].mu_t;
+  for (int i = 1; i <= layer && i < sc.n_layers; ++i)
+    mu = fmin(mu, sc.layers[i].mu_t);
+  return !(mu * z > 47.0);
+}
+
+// One bin of one vertex, binary64 (FarFieldCBSSensor::process_estimation,
+// src/detector.cpp:1384-1560, per bin).
+__device__ __forceinline__ void est_bin(const Scene &sc, const Sensor &s, const EstV<double> &v, int b,
+                                        const EstTarget &tg)
+{
+  const Laser &L = sc.laser;
+  const Medium &med = sc.media[v.med()];
+  const double4 bin = s.est_bins[b];
+  const V3<double> s_out = v3<double>(bin.x, bin.y, bin.z);
+  const double denom = s_out.z;                            // plane z = 0, normal +z
+  if (fabs(denom) < 1e-14)
+    return;
+  const double Lp = (-v.pos[2]) / denom;
+  if (Lp <= 0.0)
+    return;
+  const double Tr = exp(-est_optical_depth(sc, v.pos, s_out, Lp));
+  if (Tr < 1e-20)
+    return;
+  const V3<double> m_cur = drow(v.P, 0), n_cur = drow(v.P, 1), s_cur = drow(v.P, 2);
+  const V3<double> pv = vcross_unit(s_cur, s_out);
+  const double pn = sqrt(vdot(pv, pv));
+  if (pn < 1e-12)
+    return;
+  const V3<double> p_hat = vscale(pv, 1.0 / pn);
+  const double sin_phi = -vdot(m_cur, p_hat);
+  const double cos_phi = vdot(n_cur, p_hat);
+  double cdot = vdot(s_cur, s_out);
+  cdot = cdot > 1.0 ? 1.0 : (cdot < -1.0 ? -1.0 : cdot);
+  const double th_scat = acos(cdot);
+  Cx<double> S2, S1;
+  amplitudes<double>(med, th_scat, S2, S1);
+  const double s22 = cnorm(S2), s11 = cnorm(S1);
+  const double Emm = cnorm(v.Em), Enn = cnorm(v.En);
+  const double c2 = cos_phi * cos_phi, sn2 = sin_phi * sin_phi;
+  const double e12 = v.Em.re * v.En.re + v.Em.im * v.En.im;
+  const double F = Emm * (s22 * c2 + s11 * sn2) + Enn * (s22 * sn2 + s11 * c2) +
+                   2.0 * e12 * (s22 - s11) * sin_phi * cos_phi;
+  if (F < 1e-300)
+    return;
+  const double prob_bin = (F / (3.141592653589793 * med.I_norm)) * bin.w;
+  const double w_bin = v.wgt * Tr * prob_bin;
+  if (w_bin < 1e-300)
+    return;
+  const int t_idx = time_bin(s, v.t_launch + (v.opath + Lp));
+  if (t_idx < 0)
+    return;
+  // amp = sqrt(w_bin) exp(i k L) in the reference (src/detector.cpp:1425, :1533); the
+  // phase multiplies the forward and the reverse field alike and cancels in every
+  // Stokes value, so only the modulus is formed
+  const Cx<double> amp = {sqrt(w_bin), 0.0};
+  // exit frame A(theta, phi) P (src/detector.cpp:1027-1045)
+  double st, ct;
+  sincos(th_scat, &st, &ct);
+  double Pe[9];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const double mj = v.P[j], nj = v.P[3 + j], sj = v.P[6 + j];
+    Pe[j] = ct * cos_phi * mj + ct * sin_phi * nj + (-st) * sj;
+    Pe[3 + j] = -sin_phi * mj + cos_phi * nj + 0.0 * sj;
+    Pe[6 + j] = st * cos_phi * mj + st * sin_phi * nj + ct * sj;
+  }
+  // forward field (S R(phi)) E / sqrt(F) (src/detector.cpp:121-160)
+  const double inv = 1.0 / sqrt(F);
+  const Cx<double> T00 = cscale(S2, cos_phi), T01 = cscale(S2, sin_phi);
+  const Cx<double> T10 = cscale(S1, -sin_phi), T11 = cscale(S1, cos_phi);
+  const Cx<double> Efm = cmul(cscale(cadd(cmul(T00, v.Em), cmul(T01, v.En)), inv), amp);
+  const Cx<double> Efn = cmul(cscale(cadd(cmul(T10, v.Em), cmul(T11, v.En)), inv), amp);
+  const Cx<double> Efx = cadd(cscale(Efm, Pe[0]), cscale(Efn, Pe[3]));
+  const Cx<double> Efy = cadd(cscale(Efm, Pe[1]), cscale(Efn, Pe[4]));
+  Cx<double> Erx = {0.0, 0.0}, Ery = {0.0, 0.0};
+  if (v.multi()) {
+    const V3<double> s_in = v3<double>(L.dir[0], L.dir[1], L.dir[2]);
+    Cx<double> Rm, Rn;
+    est_suffix(sc, v.P1, Pe, v.first_med(), v.pre_m, v.pre_n, Rm, Rn);
+    const double qx = (s_out.x + s_in.x) * L.k, qy = (s_out.y + s_in.y) * L.k,
+                 qz = (s_out.z + s_in.z) * L.k;
+    const double arg = qx * v.dr[0] + qy * v.dr[1] + qz * v.dr[2];
+    double sp_, cp_;
+    sincos(arg, &sp_, &cp_);
+    const Cx<double> pp = {cp_, sp_};
+    const Cx<double> Rm2 = cmul(cmul(Rm, amp), pp), Rn2 = cmul(cmul(Rn, amp), pp);
+    Erx = cadd(cscale(Rm2, Pe[0]), cscale(Rn2, Pe[3]));
+    Ery = cadd(cscale(Rm2, Pe[1]), cscale(Rn2, Pe[4]));
+  }
+  // accumulate_stokes (src/detector.cpp:1194-1226)
+  const Cx<double> Ex = cadd(Efx, Erx), Ey = cadd(Efy, Ery);
+  const Cx<double> c_xy = cmul(Ex, Cx<double>{Ey.re, -Ey.im});
+  const Cx<double> f_xy = cmul(Efx, Cx<double>{Efy.re, -Efy.im});
+  const Cx<double> r_xy = cmul(Erx, Cx<double>{Ery.re, -Ery.im});
+  const double c0 = cnorm(Ex) + cnorm(Ey), c1 = cnorm(Ex) - cnorm(Ey);
+  const double c2s = 2.0 * c_xy.re, c3 = 2.0 * c_xy.im;
+  const double i0 = cnorm(Efx) + cnorm(Efy) + cnorm(Erx) + cnorm(Ery);
+  const double i1 = cnorm(Efx) - cnorm(Efy) + cnorm(Erx) - cnorm(Ery);
+  const double i2 = 2.0 * (f_xy.re + r_xy.re), i3 = 2.0 * (f_xy.im + r_xy.im);
+  const unsigned long long P = s.plane_stride;
+  const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
+  const unsigned long long cell = (unsigned long long)b;   // bins enumerate (theta, phi) row-major
+  tg.add4(P, cell, c0, c1, c2s, c3);
+  tg.add4(P, 4 * P + cell, i0, i1, i2, i3);
+  if (t_idx >= 1) {
+    tg.add4(P, t_idx * tstride + cell, c0, c1, c2s, c3);
+    tg.add4(P, 4 * P + t_idx * tstride + cell, i0, i1, i2, i3);
+  }
+}
+
+// The same bin in binary32 for binary32 transport (the CBS phase excepted): bin
+// directions from the binary32 copy of the bin table, the scattering angle as
+// atan2(|s_cur x s_out|, s_cur . s_out), binary32 amplitudes, transmittance, fields
+// and Stokes values, accumulated in binary64.  The CBS phase q . (r_n - r_1) uses the
+// table's q = k (s_out + s_in), formed in binary64, and r_n - r_1 formed in binary64.
+__device__ __forceinline__ void est_bin_f32(const Scene &sc, const Sensor &s, const EstV<float> &v, int b,
+                                            const EstTarget &tg)
+{
+  const Medium &med = sc.media[v.med()];
+  const float4 *bf = reinterpret_cast<const float4 *>(s.est_bins + s.est_n);
+  const float4 bin = bf[2 * b];
+  const V3<float> s_out = v3<float>(bin.x, bin.y, bin.z);
+  const float denom = s_out.z;                             // plane z = 0, normal +z
+  if (fabsf(denom) < 1e-14f)
+    return;
+  const float pz = v.pos[2];
+  const float Lp = -pz / denom;
+  if (!(Lp > 0.f))
+    return;
+  const double posd[3] = {(double)v.pos[0], (double)v.pos[1], (double)v.pos[2]};
+  const float tau = sc.n_layers == 1
+      ? sc.layers[v.layer()].mu_t_f * Lp
+      : (float)est_optical_depth(sc, posd, v3<double>(bin.x, bin.y, bin.z), (double)Lp);
+  const float Tr = expf(-tau);
+  if (Tr < 1e-20f)
+    return;
+  const V3<float> m_cur = trow<float>(v.P, 0), n_cur = trow<float>(v.P, 1), s_cur = trow<float>(v.P, 2);
+  // |s_cur x s_out| = sin(theta_scat) of the two unit vectors; its direction is the
+  // scattering plane's normal p_hat (vcross_unit, src/vec.cpp:14-26)
+  const V3<float> pv = {s_cur.y * s_out.z - s_cur.z * s_out.y, s_cur.z * s_out.x - s_cur.x * s_out.z,
+                        s_cur.x * s_out.y - s_cur.y * s_out.x};
+  const float pn = sqrtf(vdot(pv, pv));
+  if (!(pn > 0.f))
+    return;
+  const V3<float> p_hat = vscale(pv, 1.f / pn);
+  const float sin_phi = -vdot(m_cur, p_hat);
+  const float cos_phi = vdot(n_cur, p_hat);
+  const float cdot = vdot(s_cur, s_out);
+  const float th_scat = atan2f(pn, cdot);
+  Cx<float> S2, S1;
+  amplitudes<float>(med, th_scat, S2, S1);
+  const float s22 = cnorm(S2), s11 = cnorm(S1);
+  const float Emm = cnorm(v.Em), Enn = cnorm(v.En);
+  const float e12 = v.Em.re * v.En.re + v.Em.im * v.En.im;
+  const float c2 = cos_phi * cos_phi, sn2 = sin_phi * sin_phi;
+  const float F = Emm * (s22 * c2 + s11 * sn2) + Enn * (s22 * sn2 + s11 * c2) +
+                  2.f * e12 * (s22 - s11) * sin_phi * cos_phi;
+  if (!(F > 0.f))
+    return;
+  // p(Omega) dOmega = F / (pi I_norm) x dOmega dphi; w mu_s / mu_t / (pi I_norm) in wgt
+  const float w_bin = v.wgt * Tr * F * bin.w;
+  if (!(w_bin > 0.f))
+    return;
+  const int t_idx = time_bin(s, v.t_launch + (v.opath + (double)Lp));
+  if (t_idx < 0)
+    return;
+  const float amp = sqrtf(w_bin);
+  // exit frame A(theta, phi) P (src/detector.cpp:1027-1045): cos, sin of th_scat
+  const float ih = rsqrtf(cdot * cdot + pn * pn);
+  const float ct = cdot * ih, st = pn * ih;
+  float Pe[9];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const float mj = v.P[j], nj = v.P[3 + j], sj = v.P[6 + j];
+    Pe[j] = ct * cos_phi * mj + ct * sin_phi * nj - st * sj;
+    Pe[3 + j] = -sin_phi * mj + cos_phi * nj;
+    Pe[6 + j] = st * cos_phi * mj + st * sin_phi * nj + ct * sj;
+  }
+  // forward field (S R(phi)) E / sqrt(F) (src/detector.cpp:121-160)
+  const float inv = amp * rsqrtf(F);
+  const Cx<float> T00 = cscale(S2, cos_phi), T01 = cscale(S2, sin_phi);
+  const Cx<float> T10 = cscale(S1, -sin_phi), T11 = cscale(S1, cos_phi);
+  const Cx<float> Efm = cscale(cadd(cmul(T00, v.Em), cmul(T01, v.En)), inv);
+  const Cx<float> Efn = cscale(cadd(cmul(T10, v.Em), cmul(T11, v.En)), inv);
+  const Cx<float> Efx = cadd(cscale(Efm, Pe[0]), cscale(Efn, Pe[3]));
+  const Cx<float> Efy = cadd(cscale(Efm, Pe[1]), cscale(Efn, Pe[4]));
+  Cx<float> Erx = {0.f, 0.f}, Ery = {0.f, 0.f};
+  if (v.multi()) {
+    Cx<float> Rm, Rn;
+    est_suffix<float>(sc, v.P1, Pe, v.first_med(), v.pre_m, v.pre_n, Rm, Rn);
+    const float4 q = bf[2 * b + 1];
+    const float arg = q.x * v.dr[0] + q.y * v.dr[1] + q.z * v.dr[2];
+    float sp_, cp_;
+    sincosf(arg, &sp_, &cp_);
+    const Cx<float> pp = {cp_ * amp, sp_ * amp};
+    const Cx<float> Rm2 = cmul(Rm, pp), Rn2 = cmul(Rn, pp);
+    Erx = cadd(cscale(Rm2, Pe[0]), cscale(Rn2, Pe[3]));
+    Ery = cadd(cscale(Rm2, Pe[1]), cscale(Rn2, Pe[4]));
+  }
+  // accumulate_stokes (src/detector.cpp:1194-1226)
+  const Cx<float> Ex = cadd(Efx, Erx), Ey = cadd(Efy, Ery);
+  const Cx<float> c_xy = cmul(Ex, Cx<float>{Ey.re, -Ey.im});
+  const Cx<float> f_xy = cmul(Efx, Cx<float>{Efy.re, -Efy.im});
+  const Cx<float> r_xy = cmul(Erx, Cx<float>{Ery.re, -Ery.im});
+  const double c0 = cnorm(Ex) + cnorm(Ey), c1 = cnorm(Ex) - cnorm(Ey);
+  const double c2s = 2.0 * c_xy.re, c3 = 2.0 * c_xy.im;
+  const double i0 = cnorm(Efx) + cnorm(Efy) + cnorm(Erx) + cnorm(Ery);
+  const double i1 = cnorm(Efx) - cnorm(Efy) + cnorm(Erx) - cnorm(Ery);
+  const double i2 = 2.0 * ((double)f_xy.re + r_xy.re), i3 = 2.0 * ((double)f_xy.im + r_xy.im);
+  const unsigned long long PS = s.plane_stride;
+  const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
+  const unsigned long long cell = (unsigned long long)b;
+  tg.add4(PS, cell, c0, c1, c2s, c3);
+  tg.add4(PS, 4 * PS + cell, i0, i1, i2, i3);
+  if (t_idx >= 1) {
+    tg.add4(PS, t_idx * tstride + cell, c0, c1, c2s, c3);
+    tg.add4(PS, 4 * PS + t_idx * tstride + cell, i0, i1, i2, i3);
+  }
+}
+
+// run_estimators (src/detector.cpp:274-281, called at src/simulation.cpp:419-426) for
+// the whole warp: `at` marks the lanes whose photon is at a vertex in medium med_idx.
+// Every lane of the warp calls it (converged).  Vertices are estimated in binary64 by
+// binary64 transport and in binary32 (CBS phase and tallies binary64) by binary32
+// transport.
+template <typename R>
+__device__ __noinline__ void estimate_warp(const Scene &sc, const RunParams &rp, const Photon<R> &ph,
+                                           const Side<R> &side, int med_idx, bool at,
+                                           unsigned long long *s_hits, double *s_est)
+{
+  using T = R;
+  const unsigned lane = threadIdx.x & 31u;
+  for (int si = 0; si < sc.n_sensors; ++si) {
+    const Sensor &s = sc.sensors[si];
+    if (s.kind != LMC_SENSOR_FARFIELD_CBS || !s.estimator)
+      continue;
+    EstV<T> v;
+    const bool want = at && est_prepare<T, R>(sc, rp, ph, side, med_idx, s, v);
+    const unsigned counted = __ballot_sync(kFull, want);
+    if (lane == 0 && counted)
+      atomicAdd(s_hits + si, (unsigned long long)__popc(counted));
+    const bool reach = want && est_reachable(sc, (double)v.pos[2], v.layer());
+    const EstTarget tg = est_target(rp, s, si, s_est);
+    const int nb = s.est_n;
+    const bool timed = s.dt > 0;
+    for (unsigned pend = __ballot_sync(kFull, reach); pend; pend &= pend - 1u) {
+      EstV<T> w = v;
+      est_bcast(w, __ffs(pend) - 1, timed);
+      for (int b = (int)lane; b < nb; b += 32) {
+        if constexpr (sizeof(T) == 4)
+          est_bin_f32(sc, s, w, b, tg);
+        else
+          est_bin(sc, s, w, b, tg);
+      }
+    }
+  }
 }
 
 // Sensor::check_conditions (src/detector.cpp:374-417)
@@ -1847,14 +1916,18 @@ __device__ __forceinline__ void record_absorption_f32(const AbsorbGrid &g, doubl
   }
 }
 
-// One loop iteration of run_photon (src/simulation.cpp:297-614).  Returns the
-// photon's fate (kAlive if it continues).
+// First half of one loop iteration of run_photon (src/simulation.cpp:297-426): the
+// free flight with its interface crossings and sensor planes, the inside test and the
+// scattering species.  Returns the photon's fate; kAlive leaves the photon at its next
+// scattering vertex, in medium med_out.
 // kExtras: the MixtureLayer species draw and the Absorption recorder are compiled in
-// (scenes without either run the variant without their code).
-template <typename R, bool kQueue, bool kAdj, bool kEst = false, bool kExtras = false>
-__device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, Photon<R> &ph,
+// (scenes without either run the variant without their code).  kHits = false (the CBS
+// replay) leaves the sensor planes out: a replayed event never reaches one, because
+// crossing a plane at z <= 0 ends a photon.
+template <typename R, bool kQueue, bool kAdj, bool kExtras = false, bool kHits = true>
+__device__ __forceinline__ int event_move(const Scene &sc, const RunParams &rp, Photon<R> &ph,
                                           Side<R> &side, Flight<R> &fl, Counters &cnt,
-                                          unsigned long long *s_hits)
+                                          unsigned long long *s_hits, int &med_out)
 {
   rng_prefetch<R>(ph.rng, rp);
   {
@@ -1898,7 +1971,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
         fl.seg_med = sc.layers[ph.layer].medium;
         fl.seg_len = s_move;
       }
-      if (sc.n_planes > 0 && fabs(ph.pz - z0) >= R(1e-12)) {
+      if (kHits && sc.n_planes > 0 && fabs(ph.pz - z0) >= R(1e-12)) {
         const R zlo = z0 < ph.pz ? z0 : ph.pz, zhi = z0 < ph.pz ? ph.pz : z0;
         if (sc_plane<R>(sc, 0) <= zhi && sc_plane<R>(sc, sc.n_planes - 1) >= zlo &&
             record_hit<R, kQueue, kAdj>(sc, rp, ph, side, fl, x0, y0, z0, s_hits))
@@ -1934,12 +2007,23 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
       ++i;
     med_idx = sc.mix_species[SL.mix_begin + i];
   }
-  const Medium &m = sc.media[med_idx];
   if (kAdj)
     flight_scatter<R>(sc, fl, fl.seg_med, fl.seg_len);
-  if (kEst)                                                   // :419-426 run_estimators
-    estimate_at_vertex<R>(sc, rp, ph, side, med_idx, s_hits);
+  med_out = med_idx;
+  return kAlive;
+}
 
+// Second half (src/simulation.cpp:429-613): the scatter at the vertex in medium med_idx
+// (theta, S(theta), the conditional azimuth, frame, Jones vector, CBS bookkeeping), the
+// absorption weight, roulette and the event cap.  kDeposit = false (the CBS replay)
+// leaves the Absorption recorder out: the transport recorded those deposits already.
+template <typename R, bool kAdj, bool kExtras = false, bool kDeposit = true>
+__device__ __forceinline__ int event_scatter(const Scene &sc, const RunParams &rp, Photon<R> &ph,
+                                             Side<R> &side, Flight<R> &fl, Counters &cnt, int med_idx)
+{
+  const Layer &SL = sc.layers[ph.layer];
+  const int lflags = SL.flags;
+  const Medium &m = sc.media[med_idx];
   const R theta = sample_theta<R>(m, uniform<R>(ph.rng, rp));  // :429
   Cx<R> S2, S1;
   amplitudes<R>(m, theta, S2, S1);                            // :430
@@ -2073,7 +2157,7 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   }
   ph.events++;                                                // :578-587
   cnt.events++;
-  if (kExtras && (lflags & kLayerAbsorb)) {                   // :589-592
+  if (kExtras && kDeposit && (lflags & kLayerAbsorb)) {       // :589-592
     const double t = sc.absorb.d_t > 0.0 ? launch_time<R>(sc, rp, ph) + ph.opath : 0.0;  // velocity 1
     const double dw = SL.mu_t > 0 ? ph.w * SL.absorb_prob : 1.0;
     if constexpr (std::is_same<R, float>::value)
@@ -2091,6 +2175,20 @@ __device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, 
   if ((int)ph.events > rp.max_events)                         // :609-613
     return kCap;
   return kAlive;
+}
+
+// One loop iteration of run_photon (src/simulation.cpp:297-614).  Returns the photon's
+// fate (kAlive if it continues).
+template <typename R, bool kQueue, bool kAdj, bool kExtras = false>
+__device__ __forceinline__ int event_step(const Scene &sc, const RunParams &rp, Photon<R> &ph,
+                                          Side<R> &side, Flight<R> &fl, Counters &cnt,
+                                          unsigned long long *s_hits)
+{
+  int med_idx = 0;
+  const int fate = event_move<R, kQueue, kAdj, kExtras>(sc, rp, ph, side, fl, cnt, s_hits, med_idx);
+  if (fate != kAlive)
+    return fate;
+  return event_scatter<R, kAdj, kExtras>(sc, rp, ph, side, fl, cnt, med_idx);
 }
 
 template <typename R>
@@ -2145,7 +2243,7 @@ __device__ __forceinline__ int sweep_scene(const RunParams &rp, unsigned long lo
   return lo;
 }
 
-// kEst: the scene has an estimator-mode FarFieldCBS sensor (estimate_vertex at every
+// kEst: the scene has an estimator-mode FarFieldCBS sensor (estimate_warp at every
 // vertex).  kAdj: likelihood-ratio run (queued mode only).  kSweep: g_scene is an array of
 // rp.n_scenes scenes read from global memory (L1-cached), photon g belongs to scene
 // sweep_scene(g), and each lane follows its own photon's scene.
@@ -2206,8 +2304,20 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
     }
     if (__all_sync(kFull, done))
       break;
+    int fate = kAlive;
+    if constexpr (kEst) {
+      // the move, then the warp's estimate at the vertices reached (all lanes, converged),
+      // then the scatter
+      int med_idx = 0;
+      if (alive)
+        fate = event_move<R, kQueue, kAdj, kExtras>(*scp, rp, ph, side, fl, cnt, s_hits, med_idx);
+      estimate_warp<R>(*scp, rp, ph, side, med_idx, alive && fate == kAlive, s_hits, s_est);
+      if (alive && fate == kAlive)
+        fate = event_scatter<R, kAdj, kExtras>(*scp, rp, ph, side, fl, cnt, med_idx);
+    } else if (alive) {
+      fate = event_step<R, kQueue, kAdj, kExtras>(*scp, rp, ph, side, fl, cnt, s_hits);
+    }
     if (alive) {
-      const int fate = event_step<R, kQueue, kAdj, kEst, kExtras>(*scp, rp, ph, side, fl, cnt, s_hits);
       if (fate != kAlive) {
         alive = false;
         cnt.draws += ph.rng.draw;
@@ -2249,15 +2359,20 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
   }
   if (kEst && rp.est_smem_doubles > 0) {      // the block's estimated grids into the tallies
     const Scene &sc = *scp;
+    const int copies = rp.est_per_warp ? (int)(blockDim.x >> 5) : 1;
     for (int si = 0; si < sc.n_sensors; ++si) {
       const int o = rp.est_smem[si];
       if (o < 0)
         continue;
       const Sensor &s = sc.sensors[si];
       const int n = (int)(8 * s.plane_stride);
-      for (int j = threadIdx.x; j < n; j += blockDim.x)
-        if (s_est[o + j] != 0.0)
-          atomicAdd(rp.tallies + s.tally_off + j, s_est[o + j]);
+      for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double v = 0.0;
+        for (int w = 0; w < copies; ++w)
+          v += s_est[w * rp.est_warp_doubles + o + j];
+        if (v != 0.0)
+          atomicAdd(rp.tallies + s.tally_off + j, v);
+      }
     }
   }
 }

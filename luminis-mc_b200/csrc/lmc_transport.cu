@@ -1051,6 +1051,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   // copy of the grid (one flush of non-zero cells per block), as long as they fit
   for (int i = 0; i < LMC_MAX_SENSORS; ++i)
     rp.est_smem[i] = -1;
+  size_t est_block_doubles = 0;          // the grids' shared copies, one per block
   if (est) {
     constexpr size_t kEstSmemDoubles = (40u << 10) / sizeof(double);
     size_t used = 0;
@@ -1064,8 +1065,9 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
       rp.est_smem[i] = (int)used;
       used += n;
     }
+    est_block_doubles = used;
     rp.est_smem_doubles = (int)used;
-    dyn_transport += used * sizeof(double);
+    rp.est_warp_doubles = (int)used;
   }
   if (adj && sw) {
     size_t total = 0;
@@ -1126,6 +1128,20 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio runs do not record an Absorption grid");
   const KernelFn tk = pick_transport(fp32, h->queued, three, adj != nullptr, sw, est, extras);
   const KernelFn tl = pick_tally(fp32, adj != nullptr, sw);
+  if (est_block_doubles) {
+    // one copy of the estimated grids per warp (plain adds) when that keeps as many
+    // blocks per SM as one shared copy per block (shared atomics); else the latter
+    const size_t shared_one = dyn_transport + est_block_doubles * sizeof(double);
+    const size_t per_warp = dyn_transport + (size_t)(block / 32) * est_block_doubles * sizeof(double);
+    int occ_one = 0, occ_warp = 0;
+    LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)std::max(shared_one, per_warp)));
+    LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_one, (const void *)tk, block, shared_one));
+    LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_warp, (const void *)tk, block, per_warp));
+    rp.est_per_warp = (occ_warp >= occ_one && occ_warp > 0) ? 1 : 0;
+    rp.est_smem_doubles = (int)(rp.est_per_warp ? (block / 32) * est_block_doubles : est_block_doubles);
+    dyn_transport += (size_t)rp.est_smem_doubles * sizeof(double);
+  }
   LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)dyn_transport));
   if (adj && !sw)
