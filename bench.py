@@ -68,9 +68,13 @@ def parse():
     ap.add_argument("--block-size", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--batch-photons", type=int, default=0)
+    ap.add_argument("--stage-tables", action="store_true",
+                    help="binary32 amplitude tables staged in shared memory (1-D bulk copies)")
+    ap.add_argument("--no-replay", action="store_true",
+                    help="keep every photon's reverse-path history instead of replaying CBS hits")
     ap.add_argument("--variant-steps", type=int, default=2,
                     help="timed steps of the FP64 and FP32+adjoint variants (0: skip them)")
-    ap.add_argument("--variants", default="fp64,differentiable,sweep,estimator,f2",
+    ap.add_argument("--variants", default="fp64,differentiable,sweep,estimator,f2,long_paths",
                     help="comma-separated subset of the variant arms to measure")
     ap.add_argument("--estimator-photons", type=int, default=1_000_000,
                     help="photons of the estimator-mode variant")
@@ -95,7 +99,9 @@ def config_block(spec, args, n_gpus):
             "l2": "flushed between steps (256 MiB write)", "parallelism": f"photon-range x{n_gpus}",
             "seed": spec["seed"], "block_size": args.block_size or 256,
             "blocks_per_sm": args.blocks_per_sm or "auto",
-            "batch_photons": args.batch_photons or (32 << 20)}
+            "batch_photons": args.batch_photons or (32 << 20),
+            "cbs_history": "tracked per event" if args.no_replay else "replayed for CBS-grid hits",
+            "amplitude_tables": "shared memory (bulk copies)" if args.stage_tables else "global via L1"}
 
 
 # ------------------------------------------------------------------------- clocks
@@ -276,7 +282,8 @@ def run_ours(args):
         flush.zero_()
         st, _ = run.run(P, seed, begin=(k * world * P) + base, precision=args.precision,
                         stream=stream.cuda_stream, block_size=args.block_size,
-                        blocks_per_sm=args.blocks_per_sm, batch_photons=args.batch_photons)
+                        blocks_per_sm=args.blocks_per_sm, batch_photons=args.batch_photons,
+                        stage_tables=args.stage_tables, no_replay=args.no_replay)
         return st
 
     for k in range(args.warmup):
@@ -308,7 +315,8 @@ def run_ours(args):
     achieved_tflops = events * FLOP_PER_EVENT / (transport_ms * 1e-3) / 1e12
     per_photon = TRAFFIC_BYTES_PER_PHOTON.get(spec["name"]) if args.precision == "fp32" else None
     traffic = per_photon * P / max(1, transport_launches // args.steps) if per_photon else None
-    launches = 2 * transport_launches     # one transport + one tally kernel per batch
+    # one transport, one CBS replay (when the scene replays) and one tally kernel per batch
+    launches = 2 * transport_launches + sum(s.get("replay_launches", 0) for s in stats)
 
     variants = {}
     if args.variant_steps > 0:
@@ -397,6 +405,8 @@ def run_ours(args):
                                            "frac": traffic / (transport_ms / max(1, transport_launches)) / 1e6
                                            / HBM_PEAK_GBS[0], "peak_source": HBM_PEAK_GBS[1]}
                                           if traffic else None)},
+                "replayed_per_photon": sum(s.get("replayed", 0) for s in stats) / max(1, photons_done),
+                "arms": headline_arms(value, e2e, variants),
                 "variants": variants,
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches}
         print(json.dumps(line), flush=True)
@@ -404,6 +414,22 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def headline_arms(value, e2e, variants):
+    """The three arms of the headline metric side by side: binary32 transport (this
+    line), binary64 throughout (the like-for-like arm of the reference's binary64 CPU
+    path) and binary32 with likelihood-ratio derivatives; device photons/s and the
+    end-to-end photons/s of each through its public API."""
+    def arm(rec, workload):
+        if not rec:
+            return None
+        return {"value": rec.get("value"), "e2e": (rec.get("e2e") or {}).get("value"),
+                "unit": "photons/s", "workload": workload}
+    return {"fp32": {"value": value, "e2e": (e2e or {}).get("value"), "unit": "photons/s",
+                     "workload": "bilayer_rgd_mie"},
+            "fp64": arm(variants.get("fp64"), "bilayer_rgd_mie"),
+            "fp32_adjoint": arm(variants.get("fp32_adjoint"), "bilayer_hg (differentiable)")}
 
 
 def measure_variants(args, spec, local, stream, flush, world, rank, dist):
@@ -433,6 +459,39 @@ def measure_variants(args, spec, local, stream, flush, world, rank, dist):
         out.update(measure_estimator(args, local, stream, flush, world, rank, max_ms))
     if "f2" in sel:
         out.update(measure_f2(args, local, stream, flush, world, rank, max_ms))
+    if "long_paths" in sel:
+        out.update(measure_long_paths(args, local, stream, flush, world, rank, max_ms))
+    return out
+
+
+def measure_long_paths(args, local, stream, flush, world, rank, max_ms):
+    """The precision-stress workload (mie_long_paths: mu_s = 100/mm, mu_a = 1e-4/mm,
+    ~1.1e4 events per photon, FarFieldCBS 400 bins to 20 mrad, 256 x 256 speckle grid),
+    linear and circular polarisation, in three arms: binary32 transport with the CBS
+    phase in binary64, the same with the phase in binary32, and binary64 throughout.
+    photons/s and scattering events/s from device time."""
+    import luminis_mc_b200 as lm
+    from luminis_mc_b200 import workloads as W
+    from luminis_mc_b200.device import DeviceRun
+
+    out = {}
+    P = 2_000_000
+    for circ in (False, True):
+        spec = W.mie_long_paths(P, 12345, circular=circ)
+        cfg, _, keep = W.build(lm, spec)
+        rec = {"workload": spec["name"], "photons": P, "unit": "photons/s"}
+        for key, prec, phase in (("fp32", "fp32", "fp64"), ("fp32_phase32", "fp32", "fp32"),
+                                 ("fp64", "fp64", "fp64")):
+            run = DeviceRun(cfg, device=f"cuda:{local}")
+            run.run(P // 20, 7, precision=prec, stream=stream.cuda_stream, cbs_phase=phase)
+            flush.zero_()
+            st, _ = run.run(P, 12345, begin=(1 + rank) * P, precision=prec, stream=stream.cuda_stream,
+                            cbs_phase=phase)
+            run.close()
+            ms = max_ms(st["kernel_ms"])
+            rec[key] = {"value": P * world / (ms * 1e-3), "events_per_s": st["events"] * world / (ms * 1e-3),
+                        "events_per_photon": st["events"] / P}
+        out[f"long_paths_{'circular' if circ else 'linear'}"] = rec
     return out
 
 
@@ -485,7 +544,9 @@ def measure_f2(args, local, stream, flush, world, rank, max_ms):
 
 
 def measure_fp64(args, spec, local, stream, flush, world, rank, max_ms):
-    """FP64 throughout on the headline workload."""
+    """FP64 throughout on the headline workload, device time and end to end."""
+    import torch
+
     import luminis_mc_b200 as lm
     from luminis_mc_b200 import workloads as W
     from luminis_mc_b200.device import DeviceRun
@@ -502,13 +563,38 @@ def measure_fp64(args, spec, local, stream, flush, world, rank, max_ms):
             ms += st["kernel_ms"]
     run.close()
     ms = max_ms(ms)
-    return {"fp64": {"value": P * world * args.variant_steps / (ms * 1e-3), "unit": "photons/s",
-                     "workload": spec["name"], "steps": args.variant_steps}}
+    rec = {"value": P * world * args.variant_steps / (ms * 1e-3), "unit": "photons/s",
+           "workload": spec["name"], "steps": args.variant_steps}
+    if not args.no_e2e:
+        # end to end through the public API in FP64: the like-for-like arm of the
+        # reference's all-binary64 CPU path
+        cfg2, _, keep2 = W.build(lm, spec)
+        cfg2.seed = int(spec["seed"]) + 90
+        lm.run_simulation_parallel(cfg2, precision="fp64")          # untimed first call
+        wall = []
+        for k in range(2):
+            lm.release_gpu_cache()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            cfg2.seed = int(spec["seed"]) + 91 + k
+            lm.run_simulation_parallel(cfg2, precision="fp64")
+            torch.cuda.synchronize()
+            wall.append((time.perf_counter() - t0) * 1e3)
+        lm.release_gpu_cache()
+        worst = max_ms(max(wall))
+        rec["e2e"] = {"value": P * world / (worst * 1e-3), "unit": "photons/s",
+                      "path": "luminis_mc_b200.run_simulation_parallel(config, precision='fp64') "
+                              "with numpy tallies",
+                      "calls_ms": [round(x, 2) for x in wall]}
+    return {"fp64": rec}
 
 
 def measure_differentiable(args, local, stream, flush, world, rank, max_ms):
     """FP32 on the differentiable workload, without and with the likelihood-ratio
     derivatives (HG bilayer, 1e7 photons, radial fluence profile, CBS cone)."""
+    import numpy as np
+    import torch
+
     import luminis_mc_b200 as lm
     from luminis_mc_b200 import workloads as W
     from luminis_mc_b200.adjoint import AdjointTransport
@@ -541,12 +627,31 @@ def measure_differentiable(args, local, stream, flush, world, rank, max_ms):
                           stream=stream.cuda_stream)
         if k >= 1:
             ms += st["kernel_ms"]
-    tr.close()
     ms = max_ms(ms)
     out["fp32_adjoint"] = {"value": PA * world * args.variant_steps / (ms * 1e-3),
                            "unit": "photons/s", "workload": "bilayer_hg (differentiable)",
                            "parameters": 8, "outputs": "total + 100 radial bins + CBS S0 cone",
                            "steps": args.variant_steps}
+    if not args.no_e2e:
+        # end to end through the autograd function: parameters from a host tensor (scene
+        # tables re-uploaded), forward on the GPU, outputs to the host, backward
+        # (J^T g on the GPU) and the gradient to the host
+        from luminis_mc_b200.adjoint import lr_transport
+        wall = []
+        for k in range(3):
+            theta = torch.tensor(tr.parameters(), dtype=torch.float64, requires_grad=True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            y = lr_transport(theta, tr, PA, 2024 + 31 * k, precision="fp32")
+            y.sum().backward()
+            g = theta.grad.numpy().copy()
+            wall.append((time.perf_counter() - t0) * 1e3)
+        worst = max_ms(max(wall[1:]))           # the first call is untimed
+        out["fp32_adjoint"]["e2e"] = {
+            "value": PA * world / (worst * 1e-3), "unit": "photons/s",
+            "path": "luminis_mc_b200.adjoint.lr_transport(theta) forward + backward, host tensors",
+            "calls_ms": [round(x, 2) for x in wall[1:]], "grad_finite": bool(np.isfinite(g).all())}
+    tr.close()
 
     return out
 
@@ -689,10 +794,11 @@ def measure_estimator(args, local, stream, flush, world, rank, max_ms):
 
 
 def precision_report(args):
-    """Per sensor: FP32 transport (u24 stream) against FP64 transport on the same u24
-    numbers (stream_format=1), i.e. precision error alone, next to the Monte Carlo
-    noise of the same tally (FP64 on two independent seeds).  One JSON line per
-    workload."""
+    """Per sensor: FP32 transport (u24 stream), with the CBS phase in binary64 and in
+    binary32, against FP64 transport on the same u24 numbers (stream_format=1), i.e.
+    precision error alone, next to the Monte Carlo noise of the same tally (FP64 on two
+    independent seeds).  The long-path workloads run --photons photons (1e7 by
+    default).  One JSON line per workload."""
     import numpy as np
     import torch
 
@@ -701,38 +807,46 @@ def precision_report(args):
     from luminis_mc_b200.device import DeviceRun
 
     torch.cuda.set_device(0)
+    n3 = args.photons or 10_000_000
     cases = [("mie_cbs_small", W.mie_cbs_small(1_000_000, 12345)),
              ("bilayer_rgd_mie", W.bilayer_rgd_mie(10_000_000, 12345)),
-             ("mie_long_paths_linear", W.mie_long_paths(200_000, 12345)),
-             ("mie_long_paths_circular", W.mie_long_paths(200_000, 12345, circular=True))]
+             ("mie_long_paths_linear", W.mie_long_paths(n3, 12345)),
+             ("mie_long_paths_circular", W.mie_long_paths(n3, 12345, circular=True))]
+    # arms: binary32 transport with the CBS phase in binary64 (the default) and in
+    # binary32; binary64 on the same u24 numbers (the oracle of both); binary64 on another
+    # seed (the Monte Carlo noise of the same tally)
+    arms = (("fp32", "fp32", 0, 0, "fp64"), ("fp32_phase32", "fp32", 0, 0, "fp32"),
+            ("fp64", "fp64", 1, 0, "fp64"), ("fp64_other_seed", "fp64", 1, 1, "fp64"))
     for name, spec in cases:
         cfg, _, keep = W.build(lm, spec)
         n, seed = int(spec["n_photons"]), int(spec["seed"])
         res = {}
-        for key, prec, fmt, sd in (("fp32", "fp32", 0, seed), ("fp64", "fp64", 1, seed),
-                                   ("fp64_other_seed", "fp64", 1, seed + 1)):
+        for key, prec, fmt, dseed, phase in arms:
             run = DeviceRun(cfg)
-            st, _ = run.run(n, sd, precision=prec, stream_format=fmt)
-            res[key] = ([t.copy() for t in run.host_tallies()], st)
+            st, _ = run.run(n, seed + dseed, precision=prec, stream_format=fmt, cbs_phase=phase,
+                            max_events=spec["max_events"])
+            res[key] = ([t.copy() for t in run.host_tallies()], st, st["kernel_ms"])
             run.close()
         sensors = []
         for i, s in enumerate(spec["sensors"]):
-            a, b, c = res["fp32"][0][i], res["fp64"][0][i], res["fp64_other_seed"][0][i]
+            b, c = res["fp64"][0][i], res["fp64_other_seed"][0][i]
             comps = []
             for q in range(b.shape[0]):
                 bq = b[q].ravel()
                 scale = float(np.abs(bq).max()) or 1.0
                 l2 = float(np.linalg.norm(bq)) or 1.0
-                comps.append({
-                    "max_abs_err_of_max": float(np.abs(a[q].ravel() - bq).max()) / scale,
-                    "rel_l2_err": float(np.linalg.norm(a[q].ravel() - bq)) / l2,
-                    "rel_l2_mc_noise": float(np.linalg.norm(c[q].ravel() - bq)) / l2,
-                    "total_rel_err": float(abs(a[q].sum() - bq.sum()) / (abs(bq.sum()) or 1.0))})
+                comp = {"rel_l2_mc_noise": float(np.linalg.norm(c[q].ravel() - bq)) / l2}
+                for key in ("fp32", "fp32_phase32"):
+                    aq = res[key][0][i][q].ravel()
+                    comp[key] = {"max_abs_err_of_max": float(np.abs(aq - bq).max()) / scale,
+                                 "rel_l2_err": float(np.linalg.norm(aq - bq)) / l2,
+                                 "total_rel_err": float(abs(aq.sum() - bq.sum()) / (abs(bq.sum()) or 1.0))}
+                comps.append(comp)
             sensors.append({"sensor": s["kind"], "components": comps})
         line = {"workload": name, "photons": n, "seed": seed,
-                "events_fp32": res["fp32"][1]["events"], "events_fp64": res["fp64"][1]["events"],
-                "hits_fp32": res["fp32"][1]["hits"][:len(spec["sensors"])],
-                "hits_fp64": res["fp64"][1]["hits"][:len(spec["sensors"])],
+                "events": {k: res[k][1]["events"] for k in res},
+                "hits": {k: res[k][1]["hits"][:len(spec["sensors"])] for k in res},
+                "photons_per_s": {k: n / (res[k][2] * 1e-3) for k in res},
                 "sensors": sensors}
         print(json.dumps(line), flush=True)
 

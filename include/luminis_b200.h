@@ -211,6 +211,15 @@ typedef struct lmc_run_opts {
                                    run on the FP32 run's numbers: precision alone)      */
   int host_tallies_zero;        /* lmc_run_host only: the caller's host tallies are all zero,
                                    so the device copy is cleared instead of uploaded     */
+  int cbs_phase;                /* FarFieldCBS geometric phase k (s_out + s_in).(r_n - r_1):
+                                   0 in binary64 (default), 1 in binary32 (precision study) */
+  int stage_tables;             /* binary32 transport: copy every medium's amplitude table
+                                   into each block's shared memory (1-D bulk copies) when
+                                   that keeps the blocks per SM; 0 reads them through L1  */
+  int no_replay;                /* 1: the transport keeps every photon's reverse-path history
+                                   instead of replaying the photons a FarFieldCBS grid reads
+                                   (replay is used by queued runs without records,
+                                   likelihood-ratio outputs or estimator sensors)         */
 } lmc_run_opts;
 
 /* Final state of one photon, written when opts.records is set (the same layout as
@@ -236,6 +245,8 @@ typedef struct lmc_stats {
   float kernel_ms;                  /* whole run on the device (all launches), CUDA events */
   float transport_ms;               /* sum of the transport kernel launches alone       */
   uint32_t transport_launches;      /* transport kernel launches (queue batches)        */
+  uint32_t replay_launches;         /* CBS replay kernel launches (0: no replay)        */
+  uint64_t replayed;                /* photons whose reverse path the replay rebuilt    */
 } lmc_stats;
 
 typedef struct lmc_handle lmc_handle;

@@ -25,6 +25,7 @@ struct Medium {
   double mu_s;                           // scattering coefficient (likelihood-ratio scores)
   float mu_s_f, pad_s;
   double I_norm;                         // int (|S1|^2 + |S2|^2) sin(theta), the estimator's p(Omega)
+  const float4 *amp_stage;               // the block's shared-memory copy of amp_f (null: none)
 };
 
 // A layer with its transport coefficients (Layer::mu_attenuation, mu_scattering,
@@ -113,8 +114,10 @@ struct __align__(16) Scene {
 struct Scratch {
   unsigned long long next_photon;        // reset per batch
   unsigned long long queue_count;        // reset per batch
+  unsigned long long replay_count;       // reset per batch: entries of RunParams::replay_list
   unsigned long long photons, events, steps, detected, escaped, stack, roulette, cap, draws;
   unsigned long long hits[LMC_MAX_SENSORS];
+  unsigned long long replayed;           // CBS replays over the run's batches
   unsigned int error_flags;
   unsigned int pad;
 };
@@ -155,6 +158,8 @@ enum ErrorFlag : unsigned int {
   kErrNonFiniteWeight = 1u << 0,   // a photon ended with a NaN/inf weight
   kErrAborted = 1u << 1,           // a photon was dropped: non-finite state (see kError)
   kErrQueueOverflow = 1u << 2,     // more hits than the queue holds (tallies incomplete)
+  kErrReplay = 1u << 3,            // a replayed history did not reach its recorded hit
+  kErrStaging = 1u << 4,           // a table copy into shared memory did not complete in time
 };
 
 // Likelihood-ratio output layout of one scene of a sweep: its block of (1 + K) rows of
@@ -198,6 +203,15 @@ struct RunParams {
   int est_smem[LMC_MAX_SENSORS];
   int est_smem_doubles;
   int est_per_warp, est_warp_doubles;
+  // CBS replay: the transport keeps no reverse-path history (track_reverse 0 in its
+  // launch); hits a FarFieldCBS grid will read append their queue slot to replay_list,
+  // and the replay kernel rebuilds those photons' histories from their streams
+  int cbs_replay;
+  int cbs_phase_f32;                     // the CBS geometric phase in binary32 (precision study)
+  uint32_t *replay_list;
+  // amplitude tables staged per block: every medium's amp_f, one after another, copied
+  // by cp.async.bulk into dynamic shared memory at byte stage_off (0 bytes: not staged)
+  unsigned int stage_bytes, stage_off;
 };
 
 }  // namespace dev

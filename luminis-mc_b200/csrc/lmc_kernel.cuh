@@ -275,14 +275,16 @@ template <typename R> struct Photon {
 // warps share an SM.  Lives in dynamic shared memory (the binary64 layout exceeds
 // the 48 KB static limit).
 template <typename R> struct Side {
+  uint32_t ring[kRing][kBlock];  // the photon's generated Philox words (see RngT)
+  int first_med[kBlock];
+  // the reverse-path history from here on (a launch that replays it instead allocates
+  // only the members above: side_slim_bytes)
   R first[12][kBlock];         // r_1 (3), then P1 rows m_1, n_1, s_1 (9)
   R last[6][kBlock];           // S2, S1 (re, im) and cos, sin(phi) of the newest scatter
   R ang[4][kBlock];            // cos, sin theta and cos, sin phi of the newest scatter:
                                // P_{n-1} = A^T P_n when a hit needs it (prev_frame)
   R rn[3][kBlock];             // position of the newest scatter (r_n)
   R T[8][kBlock];              // matrix_T_raw: normalised interior Jones product (re, im)
-  uint32_t ring[kRing][kBlock];  // the photon's generated Philox words (see RngT)
-  int first_med[kBlock];
 };
 
 // Dynamic shared memory of a transport block: the Side arrays, then (kAdj) the
@@ -291,6 +293,12 @@ template <typename R> struct Side {
 template <typename R> __host__ __device__ constexpr size_t side_bytes()
 {
   return (sizeof(Side<R>) + 15) & ~size_t(15);
+}
+// The ring and the first species alone: a transport launch without reverse-path
+// bookkeeping (rp.track_reverse == 0) touches nothing else of Side.
+template <typename R> __host__ __device__ constexpr size_t side_slim_bytes()
+{
+  return (sizeof(uint32_t) * kRing * kBlock + sizeof(int) * kBlock + 15) & ~size_t(15);
 }
 
 struct Counters {
@@ -533,15 +541,17 @@ template <> __device__ __forceinline__ void amplitudes<float>(const Medium &m, f
 {
   const float pos = theta * m.amp_inv_dx_f;
   const int last = m.amp_n - 1;
+  const float4 *st = m.amp_stage;        // the block's shared copy, when staged
+  auto node = [&](int k) { return st ? st[k] : __ldg(m.amp_f + k); };
   float4 a;
   if (pos <= 0.0f) {
-    a = __ldg(m.amp_f);
+    a = node(0);
   } else if (pos >= (float)last) {
-    a = __ldg(m.amp_f + last);
+    a = node(last);
   } else {
     const int i = (int)pos;
     const float t = pos - (float)i;
-    const float4 y0 = __ldg(m.amp_f + i), y1 = __ldg(m.amp_f + i + 1);
+    const float4 y0 = node(i), y1 = node(i + 1);
     a = make_float4(y0.x + t * (y1.x - y0.x), y0.y + t * (y1.y - y0.y), y0.z + t * (y1.z - y0.z),
                     y0.w + t * (y1.w - y0.w));
   }
@@ -877,15 +887,28 @@ __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor 
     if (rec) {                     // photon.polarization_reverse, kept for the replay check
       rec->Er[0] = Rm.re; rec->Er[1] = Rm.im; rec->Er[2] = Rn.re; rec->Er[3] = Rn.im;
     }
-    // CBS geometric phase exp(i k (s_out + s_in).(r_n - r_1)) in binary64
+    // CBS geometric phase exp(i k (s_out + s_in).(r_n - r_1)) in binary64, or all in
+    // binary32 when the run asks for it (precision study)
     const Laser &L = sc.laser;
-    const double qx = ((double)sx + L.dir[0]) * L.k, qy = ((double)sy + L.dir[1]) * L.k,
-                 qz = ((double)sz + L.dir[2]) * L.k;
-    const double arg = qx * ((double)h.rn[0] - (double)h.r1[0]) +
-                       qy * ((double)h.rn[1] - (double)h.r1[1]) +
-                       qz * ((double)h.rn[2] - (double)h.r1[2]);
     double sp, cp;
-    sincos(arg, &sp, &cp);
+    if (rp.cbs_phase_f32) {
+      const float kf = (float)L.k;
+      const float qx = ((float)sx + (float)L.dir[0]) * kf, qy = ((float)sy + (float)L.dir[1]) * kf,
+                  qz = ((float)sz + (float)L.dir[2]) * kf;
+      const float arg = qx * ((float)h.rn[0] - (float)h.r1[0]) + qy * ((float)h.rn[1] - (float)h.r1[1]) +
+                        qz * ((float)h.rn[2] - (float)h.r1[2]);
+      float spf, cpf;
+      sincosf(arg, &spf, &cpf);
+      sp = spf;
+      cp = cpf;
+    } else {
+      const double qx = ((double)sx + L.dir[0]) * L.k, qy = ((double)sy + L.dir[1]) * L.k,
+                   qz = ((double)sz + L.dir[2]) * L.k;
+      const double arg = qx * ((double)h.rn[0] - (double)h.r1[0]) +
+                         qy * ((double)h.rn[1] - (double)h.r1[1]) +
+                         qz * ((double)h.rn[2] - (double)h.r1[2]);
+      sincos(arg, &sp, &cp);
+    }
     const Cx<R> pp = {R(cp), R(sp)};
     const Cx<R> Rm2 = cmul(cscale(Rm, w_sqrt), pp), Rn2 = cmul(cscale(Rn, w_sqrt), pp);
     Erx = cadd(cscale(Rm2, h.P[0]), cscale(Rn2, h.P[3]));
@@ -1707,6 +1730,31 @@ __device__ __forceinline__ void fill_hit(const Photon<R> &ph, const Side<R> &sid
     h.T[q] = {side.T[2 * q][tid], side.T[2 * q + 1][tid]};
 }
 
+// Whether a hit's FarFieldCBS sensors will read its reverse-path fields: from the
+// second scattering event on (src/detector.cpp:1290) and when the exit direction falls
+// in one of their grids (the binning of hit_farfield, src/detector.cpp:1271-1281),
+// widened by a bin on every side so that no hit a grid bins is missed.
+template <typename R>
+__device__ __forceinline__ bool needs_reverse(const Scene &sc, unsigned mask, const Photon<R> &ph)
+{
+  const unsigned m = mask & sc.cbs_mask;
+  if (!m || ph.events < 2)
+    return false;
+  const R theta = exit_theta(ph.P[6], ph.P[7], ph.P[8]);
+  R phi = m_atan2(ph.P[7], ph.P[6]);
+  if (phi < R(0))
+    phi += R(6.283185307179586);
+  for (int si = 0; si < sc.n_sensors; ++si) {
+    if (!(m & (1u << si)))
+      continue;
+    const Sensor &s = sc.sensors[si];
+    const int it = (int)(theta / R(s.dtheta)), jp = (int)(phi / R(s.dphi));
+    if (it >= -1 && it <= s.N_theta && jp >= -1 && jp <= s.N_phi)
+      return true;
+  }
+  return false;
+}
+
 // Append a hit to the queue (warp-aggregated slot).  Only the fields the
 // sensors in `mask` read are written.
 template <typename R, bool kAdj>
@@ -1750,7 +1798,14 @@ __device__ __forceinline__ void enqueue_hit(const Scene &sc, const RunParams &rp
   r[(kQE + 1) * C + slot] = ph.Em.im;
   r[(kQE + 2) * C + slot] = ph.En.re;
   r[(kQE + 3) * C + slot] = ph.En.im;
-  if (mask & sc.cbs_mask) {
+  if ((mask & sc.cbs_mask) && rp.cbs_replay) {
+    // no history kept: the replay kernel rebuilds it for the hits a grid will read
+    if (needs_reverse<R>(sc, mask, ph)) {
+      const unsigned long long k = atomicAdd(&rp.scratch->replay_count, 1ull);
+      if (k < C)
+        rp.replay_list[k] = (uint32_t)slot;
+    }
+  } else if (mask & sc.cbs_mask) {
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       r[(kQR1 + j) * C + slot] = side.first[j][tid];
@@ -1846,16 +1901,18 @@ __device__ void init_photon(const Scene &sc, const RunParams &rp, Photon<R> &ph,
   ph.scene = 0;
   ph.layer = layer_index_at<R>(sc, ph.pz);
   ph.last_med = 0;
-  const int tid = threadIdx.x;                              // r_1 = r_n = launch, P1 = P0
-  side.rn[0][tid] = ph.px; side.rn[1][tid] = ph.py; side.rn[2][tid] = ph.pz;
+  const int tid = threadIdx.x;
+  side.first_med[tid] = 0;
+  if (!rp.track_reverse)                                    // no history in this launch
+    return;
+  side.rn[0][tid] = ph.px; side.rn[1][tid] = ph.py; side.rn[2][tid] = ph.pz;   // r_1 = r_n = launch
 #pragma unroll
   for (int q = 0; q < 8; ++q)
     side.T[q][tid] = R(q == 0 || q == 6 ? 1 : 0);
   side.first[0][tid] = ph.px; side.first[1][tid] = ph.py; side.first[2][tid] = ph.pz;
 #pragma unroll
   for (int j = 0; j < 9; ++j)
-    side.first[3 + j][tid] = ph.P[j];
-  side.first_med[tid] = 0;
+    side.first[3 + j][tid] = ph.P[j];                       // P1 = P0
 }
 
 enum Fate { kAlive = 0, kDetected = 1, kEscaped = 2, kStack = 3, kRoulette = 4, kCap = 5, kError = 6 };
@@ -2226,6 +2283,49 @@ __device__ __forceinline__ void load_scene(unsigned char *s_raw, const Scene *g_
     dst[i] = src[i];
 }
 
+// Amplitude tables into shared memory (1-D bulk copies by the tensor memory accelerator,
+// completion counted on an mbarrier; the source is this GPU's own table arena).  Thread
+// 0 issues one cp.async.bulk per medium -- sizes and both addresses are multiples of 16
+// bytes, which the arena's 256-byte alignment and 16-byte table entries guarantee --
+// and waits with a bounded number of tries; the block's scene copy then points each
+// medium at its staged table.  A copy that does not complete in time raises kErrStaging
+// and leaves the scene on the global tables.
+__device__ __forceinline__ void stage_amplitudes(Scene &sc, const RunParams &rp, unsigned char *s_dyn,
+                                                 unsigned long long *mbar)
+{
+  if (threadIdx.x == 0) {
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(mbar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(rp.stage_bytes)
+                 : "memory");
+    unsigned off = rp.stage_off;
+    for (int m = 0; m < sc.n_media; ++m) {
+      const unsigned bytes = (unsigned)sc.media[m].amp_n * 16u;
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(s_dyn + off);
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                   ::"r"(dst), "l"(sc.media[m].amp_f), "r"(bytes), "r"(bar) : "memory");
+      off += bytes;
+    }
+    bool done = false;
+    for (int tries = 0; tries < (1 << 22) && !done; ++tries) {
+      unsigned ok;
+      asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+                   " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(bar) : "memory");
+      done = ok != 0;
+    }
+    if (done) {
+      off = rp.stage_off;
+      for (int m = 0; m < sc.n_media; ++m) {
+        sc.media[m].amp_stage = reinterpret_cast<const float4 *>(s_dyn + off);
+        off += (unsigned)sc.media[m].amp_n * 16u;
+      }
+    } else {
+      atomicOr(&rp.scratch->error_flags, (unsigned)kErrStaging);
+    }
+  }
+}
+
 // kMinBlocks > 1 asks the compiler to fit that many 256-thread blocks per SM
 // (register cap 65536 / (256 kMinBlocks)); lmc_run picks the variant.
 
@@ -2269,6 +2369,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
     for (int j = threadIdx.x; j < rp.est_smem_doubles; j += blockDim.x)
       s_est[j] = 0.0;
   __syncthreads();
+  if (!kSweep && sizeof(R) == 4 && rp.stage_bytes) {
+    __shared__ __align__(8) unsigned long long s_mbar;
+    stage_amplitudes(*reinterpret_cast<Scene *>(s_raw), rp, s_dyn, &s_mbar);
+    __syncthreads();
+  }
   const Scene *scp = kSweep ? g_scene : reinterpret_cast<const Scene *>(s_raw);
   const unsigned lane = threadIdx.x & 31u;
   Counters cnt = {0, 0, 0};
@@ -2374,6 +2479,86 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
           atomicAdd(rp.tallies + s.tally_off + j, v);
       }
     }
+  }
+}
+
+// CBS replay kernel: for every hit on the replay list, re-run the photon from its
+// launch -- the same stream (seed, photon index), the same transport code -- through its
+// recorded number of scattering events with the reverse-path bookkeeping on, and write
+// the CBS fields (r_1, r_n, P_1, P_{n-1}, the interior product T, the first and last
+// species) into its queue entry, where the tally kernel reads them.  The replay must
+// reach the recorded hit state: the frame and Jones vector after the last event are
+// compared with the entry's, and a replay that does not match, or whose photon ends
+// early, raises kErrReplay.  Each thread takes list entries in turn.
+template <typename R, bool kSweep = false, bool kExtras = false>
+__global__ void __launch_bounds__(kBlock, 2) cbs_replay_kernel(const Scene *__restrict__ g_scene, RunParams rp)
+{
+  __shared__ __align__(16) unsigned char s_raw[kSweep ? 16 : sizeof(Scene)];
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  Side<R> &side = *reinterpret_cast<Side<R> *>(s_dyn);
+  if (!kSweep)
+    load_scene(s_raw, g_scene);
+  __syncthreads();
+  const Queue &q = rp.queue;
+  const unsigned long long C = q.cap;
+  const unsigned long long listed = *(volatile unsigned long long *)&rp.scratch->replay_count;
+  const unsigned long long n = listed < C ? listed : C;
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    atomicAdd(&rp.scratch->replayed, n);
+  rp.track_reverse = 1;
+  Photon<R> ph;
+  ph.rng.ring = &side.ring[0][threadIdx.x];
+  Flight<R> fl;
+  fl.score = nullptr;
+  Counters cnt = {0, 0, 0};
+  R *r = static_cast<R *>(q.r);
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long slot = rp.replay_list[i];
+    const unsigned scene = kSweep ? q.u32[kQScene * C + slot] : 0u;
+    const Scene &sc = kSweep ? g_scene[scene] : *reinterpret_cast<const Scene *>(s_raw);
+    const unsigned long long index =
+        ((unsigned long long)q.u32[kQPhotonHi * C + slot] << 32) | q.u32[kQPhotonLo * C + slot];
+    const uint32_t target = q.u32[kQEvents * C + slot];
+    init_photon<R>(sc, rp, ph, side, index);
+    bool ok = true;
+    while (ok && ph.events < target) {
+      int med = 0;
+      int fate = event_move<R, true, false, kExtras, false>(sc, rp, ph, side, fl, cnt, nullptr, med);
+      if (fate == kAlive)
+        fate = event_scatter<R, false, kExtras, false>(sc, rp, ph, side, fl, cnt, med);
+      ok = fate == kAlive;
+    }
+    // the frame and Jones vector of the hit are those after the last scatter
+    R dev = R(0);
+#pragma unroll
+    for (int j = 0; j < 9; ++j)
+      dev = fmax(dev, fabs(ph.P[j] - r[(kQP + j) * C + slot]));
+    dev = fmax(dev, fabs(ph.Em.re - r[(kQE + 0) * C + slot]));
+    dev = fmax(dev, fabs(ph.Em.im - r[(kQE + 1) * C + slot]));
+    dev = fmax(dev, fabs(ph.En.re - r[(kQE + 2) * C + slot]));
+    dev = fmax(dev, fabs(ph.En.im - r[(kQE + 3) * C + slot]));
+    if (!ok || ph.events != target || !(dev <= R(1e-3))) {
+      atomicOr(&rp.scratch->error_flags, (unsigned)kErrReplay);
+      continue;
+    }
+    const int tid = threadIdx.x;
+    q.u32[kQMedia * C + slot] = (uint32_t)side.first_med[tid] | ((uint32_t)ph.last_med << 16);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      r[(kQR1 + j) * C + slot] = side.first[j][tid];
+      r[(kQRn + j) * C + slot] = side.rn[j][tid];
+    }
+    R pn1[9];
+    prev_frame<R>(ph, side, pn1);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      r[(kQP1 + j) * C + slot] = side.first[3 + j][tid];
+      r[(kQPn1 + j) * C + slot] = pn1[j];
+    }
+#pragma unroll
+    for (int qd = 0; qd < 8; ++qd)
+      r[(kQT + qd) * C + slot] = side.T[qd][tid];
   }
 }
 

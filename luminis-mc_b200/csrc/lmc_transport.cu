@@ -978,6 +978,16 @@ static KernelFn pick_tally(bool fp32, bool adj, bool sw)
   return fp32 ? tally_kernel<float> : tally_kernel<double>;
 }
 
+static KernelFn pick_replay(bool fp32, bool sw, bool extras)
+{
+  using namespace lmc::dev;
+  if (extras)
+    return fp32 ? (sw ? cbs_replay_kernel<float, true, true> : cbs_replay_kernel<float, false, true>)
+                : (sw ? cbs_replay_kernel<double, true, true> : cbs_replay_kernel<double, false, true>);
+  return fp32 ? (sw ? cbs_replay_kernel<float, true> : cbs_replay_kernel<float, false>)
+              : (sw ? cbs_replay_kernel<double, true> : cbs_replay_kernel<double, false>);
+}
+
 // Whether any of a scene's layers draws species or records absorption.
 static bool scene_extras(const lmc::dev::Scene &sc)
 {
@@ -1036,6 +1046,9 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   if (opts->stream_format != 0 && opts->stream_format != 1)
     return fail(LMC_ERR_INVALID, "stream_format must be 0 or 1");
   rp.stream_u24 = (!fp32 && opts->stream_format == 1) ? 1 : 0;
+  if (opts->cbs_phase != 0 && opts->cbs_phase != 1)
+    return fail(LMC_ERR_INVALID, "cbs_phase must be 0 (binary64) or 1 (binary32)");
+  rp.cbs_phase_f32 = opts->cbs_phase;
   if (sw) {
     rp.n_scenes = h->n_scenes;
     rp.sweep_prefix = h->d_prefix;
@@ -1128,6 +1141,29 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio runs do not record an Absorption grid");
   const KernelFn tk = pick_transport(fp32, h->queued, three, adj != nullptr, sw, est, extras);
   const KernelFn tl = pick_tally(fp32, adj != nullptr, sw);
+  // CBS replay: queued runs without likelihood-ratio outputs, estimator or records keep
+  // no reverse-path history in the transport; the replay kernel rebuilds it for the
+  // hits that FarFieldCBS grids read
+  bool any_cbs = false;
+  for (int k = 0; k < h->n_scenes; ++k)
+    any_cbs = any_cbs || (sw ? h->scenes[k] : h->scene).cbs_mask != 0;
+  const bool replay = h->queued && !adj && !est && !opts->records && !opts->no_replay &&
+                      opts->track_reverse_paths && any_cbs;
+  rp.cbs_replay = replay ? 1 : 0;
+  if (replay) {                          // no history: the ring and first species only
+    rp.track_reverse = 0;
+    dyn_transport = fp32 ? dev::side_slim_bytes<float>() : dev::side_slim_bytes<double>();
+  }
+  const KernelFn tr = replay ? pick_replay(fp32, sw, extras) : nullptr;
+  const size_t dyn_replay = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
+  int replay_grid = 0;
+  if (replay) {
+    LMC_CUDA(cudaFuncSetAttribute((const void *)tr, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)dyn_replay));
+    int per = 0;
+    LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)tr, dev::kBlock, dyn_replay));
+    replay_grid = h->sm_count * std::max(per, 1);
+  }
   if (est_block_doubles) {
     // one copy of the estimated grids per warp (plain adds) when that keeps as many
     // blocks per SM as one shared copy per block (shared atomics); else the latter
@@ -1141,6 +1177,24 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     rp.est_per_warp = (occ_warp >= occ_one && occ_warp > 0) ? 1 : 0;
     rp.est_smem_doubles = (int)(rp.est_per_warp ? (block / 32) * est_block_doubles : est_block_doubles);
     dyn_transport += (size_t)rp.est_smem_doubles * sizeof(double);
+  }
+  if (opts->stage_tables && fp32 && !sw) {
+    // every medium's binary32 amplitude table in the block's shared memory, after the
+    // other dynamic arrays -- as long as that keeps the blocks per SM
+    size_t bytes = 0;
+    for (int m = 0; m < h->scene.n_media; ++m)
+      bytes += (size_t)h->scene.media[m].amp_n * sizeof(float4);
+    const size_t off = (dyn_transport + 15) & ~size_t(15);
+    int occ0 = 0, occ1 = 0;
+    LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(off + bytes)));
+    LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, (const void *)tk, block, dyn_transport));
+    LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, (const void *)tk, block, off + bytes));
+    if (bytes > 0 && occ1 >= occ0 && occ1 > 0) {
+      rp.stage_bytes = (unsigned)bytes;
+      rp.stage_off = (unsigned)off;
+      dyn_transport = off + bytes;
+    }
   }
   LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)dyn_transport));
@@ -1161,7 +1215,8 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     const unsigned long long planes = std::max(1, h->max_planes);
     const unsigned long long cap = batch * planes + batch / 16 + 1024;
     const size_t need = (size_t)cap * (dev::kQU32Fields * 4 + dev::kQF64Fields * 8 +
-                                       (dev::kQRFields + (size_t)rp.adj_K) * rbytes) + 3 * 256;
+                                       (dev::kQRFields + (size_t)rp.adj_K) * rbytes) +
+                        (replay ? (size_t)cap * sizeof(uint32_t) : 0) + 4 * 256;
     if (h->queue_bytes < need) {
       cudaFree(h->d_queue);
       h->d_queue = nullptr;
@@ -1180,6 +1235,8 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     rp.queue.f64 = reinterpret_cast<double *>(q + o);
     o += align((size_t)cap * dev::kQF64Fields * 8);
     rp.queue.r = q + o;
+    o += align((size_t)cap * (dev::kQRFields + (size_t)rp.adj_K) * rbytes);
+    rp.replay_list = replay ? reinterpret_cast<uint32_t *>(q + o) : nullptr;
   }
   if (stats && n_photons > 0) {           // one event pair per transport launch
     const size_t need_ev = 2 * (size_t)((n_photons + batch - 1) / batch);
@@ -1197,7 +1254,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     rp.n_photons = nb;
     rp.records = records ? records + done : nullptr;   // the kernels index from photon_begin
     // reset the work counter and the queue fill of this batch
-    LMC_CUDA(cudaMemsetAsync(h->d_scratch, 0, 2 * sizeof(unsigned long long), stream));
+    LMC_CUDA(cudaMemsetAsync(h->d_scratch, 0, 3 * sizeof(unsigned long long), stream));
     const int grid = (int)std::max<unsigned long long>(
         1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * per_sm,
                                            (nb + block - 1) / block));
@@ -1206,6 +1263,10 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
       LMC_CUDA(cudaEventRecord(h->kev[pair], stream));
     tk<<<grid, block, dyn_transport, stream>>>(h->d_scene, rp);
     LMC_CUDA(cudaGetLastError());
+    if (replay) {                        // part of the transport (timed with it)
+      tr<<<replay_grid, dev::kBlock, dyn_replay, stream>>>(h->d_scene, rp);
+      LMC_CUDA(cudaGetLastError());
+    }
     if (stats)
       LMC_CUDA(cudaEventRecord(h->kev[pair + 1], stream));
     if (h->queued && h->tally_doubles > 0) {
@@ -1240,6 +1301,8 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     }
     stats->transport_ms = (float)tms;
     stats->transport_launches = (uint32_t)launches;
+    stats->replay_launches = replay ? (uint32_t)launches : 0u;
+    stats->replayed = sc.replayed;
     if (sc.error_flags)
       return fail(LMC_ERR_KERNEL, "transport kernel raised error flags " + std::to_string(sc.error_flags));
   }
@@ -1951,7 +2014,7 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     rp.photon_begin = photon_begin + done;
     rp.n_photons = nb;
     rp.records = records ? records + done : nullptr;   // the kernels index from photon_begin
-    LMC_CUDA(cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned long long), stream));
+    LMC_CUDA(cudaMemsetAsync(d_counters, 0, 3 * sizeof(unsigned long long), stream));
     const int grid = (int)std::max<unsigned long long>(
         1ull, std::min<unsigned long long>((unsigned long long)sm_count * per_sm, (nb + block - 1) / block));
     tk<<<grid, block, dyn_transport, stream>>>(d_scene, rp);

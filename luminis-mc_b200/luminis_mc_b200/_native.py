@@ -101,7 +101,8 @@ class RunOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("max_events", C.c_int), ("track_reverse_paths", C.c_int),
                 ("block_size", C.c_int), ("blocks_per_sm", C.c_int), ("records", C.c_void_p),
                 ("stream", C.c_void_p), ("batch_photons", C.c_uint64),
-                ("stream_format", C.c_int), ("host_tallies_zero", C.c_int)]
+                ("stream_format", C.c_int), ("host_tallies_zero", C.c_int),
+                ("cbs_phase", C.c_int), ("stage_tables", C.c_int), ("no_replay", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -110,7 +111,8 @@ class Stats(C.Structure):
                 ("roulette", C.c_uint64), ("cap", C.c_uint64), ("draws", C.c_uint64),
                 ("hits", C.c_uint64 * MAX_SENSORS), ("error_flags", C.c_uint32),
                 ("kernel_ms", C.c_float), ("transport_ms", C.c_float),
-                ("transport_launches", C.c_uint32)]
+                ("transport_launches", C.c_uint32), ("replay_launches", C.c_uint32),
+                ("replayed", C.c_uint64)]
 
     def as_dict(self) -> dict:
         d = {n: int(getattr(self, n)) for n in
@@ -120,6 +122,8 @@ class Stats(C.Structure):
         d["kernel_ms"] = float(self.kernel_ms)
         d["transport_ms"] = float(self.transport_ms)
         d["transport_launches"] = int(self.transport_launches)
+        d["replay_launches"] = int(self.replay_launches)
+        d["replayed"] = int(self.replayed)
         return d
 
 

@@ -262,7 +262,8 @@ class Transport:
 
     def opts(self, precision="fp32", max_events=None, track_reverse_paths=None, block_size=0,
              blocks_per_sm=0, records_ptr=None, stream=None, batch_photons=0,
-             stream_format=0, host_tallies_zero=False) -> N.RunOpts:
+             stream_format=0, host_tallies_zero=False, cbs_phase="fp64",
+             stage_tables=False, no_replay=False) -> N.RunOpts:
         if precision not in N.PRECISION:
             raise ValueError("precision must be 'fp32' or 'fp64'")
         c = self.config
@@ -278,6 +279,11 @@ class Transport:
         o.batch_photons = int(batch_photons)
         o.stream_format = int(stream_format)
         o.host_tallies_zero = int(bool(host_tallies_zero))
+        if cbs_phase not in ("fp64", "fp32"):
+            raise ValueError("cbs_phase must be 'fp64' or 'fp32'")
+        o.cbs_phase = 1 if cbs_phase == "fp32" else 0
+        o.stage_tables = int(bool(stage_tables))
+        o.no_replay = int(bool(no_replay))
         return o
 
     def run_host(self, tallies: np.ndarray, n_photons: int, seed: int, begin: int = 0,

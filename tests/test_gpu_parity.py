@@ -165,6 +165,30 @@ def test_records_over_several_batches(precision, cuda):
     b.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("make", [W.mie_cbs_small, W.bilayer_rgd_mie, W.mixture_bilayer],
+                         ids=["mie_cbs_small", "bilayer_rgd_mie", "mixture_bilayer"])
+def test_cbs_replay_equals_tracked_history(make, precision, cuda):
+    """By default a queued run keeps no reverse-path history in the transport and
+    replays the photons a FarFieldCBS grid reads; with no_replay every photon's history
+    is tracked event by event.  Both give the same tallies and counts: the replay
+    rebuilds exactly the history the tracked run keeps (same stream, same arithmetic)."""
+    spec = make(20000, 53)
+    cfg, _, keep = W.build(lm, spec)
+    a = DeviceRun(cfg)
+    sa, _ = a.run(20000, 53, precision=precision)                    # replayed
+    b = DeviceRun(cfg)
+    sb, _ = b.run(20000, 53, precision=precision, no_replay=True)    # tracked
+    assert sa["replay_launches"] > 0 and sa["replayed"] > 0
+    assert sb["replay_launches"] == 0
+    assert sa["error_flags"] == 0 and sb["error_flags"] == 0
+    for ga, gb in zip(a.host_tallies(), b.host_tallies()):
+        np.testing.assert_allclose(ga, gb, rtol=1e-12, atol=1e-12 * max(np.abs(gb).max(), 1e-300))
+    assert sa["hits"] == sb["hits"] and sa["events"] == sb["events"]
+    a.close()
+    b.close()
+
+
 def test_photon_ranges_compose(cuda):
     """Two runs over [0, n/2) and [n/2, n) tally the same as one run over [0, n)."""
     spec = W.mie_cbs_small(4000, 99)
