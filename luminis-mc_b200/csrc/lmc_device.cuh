@@ -212,6 +212,9 @@ struct RunParams {
   // amplitude tables staged per block: every medium's amp_f, one after another, copied
   // by cp.async.bulk into dynamic shared memory at byte stage_off (0 bytes: not staged)
   unsigned int stage_bytes, stage_off;
+  // bytes of dynamic shared memory before the likelihood-ratio scores / estimated grids:
+  // the whole Side, or only its ring and first species when the run replays CBS hits
+  unsigned int side_off, side_pad;
 };
 
 }  // namespace dev

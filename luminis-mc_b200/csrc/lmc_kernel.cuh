@@ -2357,14 +2357,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
   extern __shared__ __align__(16) unsigned char s_dyn[];
   Side<R> &side = *reinterpret_cast<Side<R> *>(s_dyn);
   Flight<R> fl;
-  fl.score = reinterpret_cast<R *>(s_dyn + side_bytes<R>()) + threadIdx.x;
+  fl.score = reinterpret_cast<R *>(s_dyn + rp.side_off) + threadIdx.x;
   if (!kSweep)
     load_scene(s_raw, g_scene);
   if (threadIdx.x < LMC_MAX_SENSORS)
     s_hits[threadIdx.x] = 0;
   if (threadIdx.x < 7)
     s_fate[threadIdx.x] = 0;
-  double *s_est = reinterpret_cast<double *>(s_dyn + side_bytes<R>());
+  double *s_est = reinterpret_cast<double *>(s_dyn + rp.side_off);
   if (kEst)
     for (int j = threadIdx.x; j < rp.est_smem_doubles; j += blockDim.x)
       s_est[j] = 0.0;

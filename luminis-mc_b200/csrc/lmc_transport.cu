@@ -1113,7 +1113,6 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     rp.adj_n_out = total;
     rp.adj_K = kmax;
     rp.adj_radial_sensor = -1;           // per scene in adj_scenes, added globally
-    dyn_transport += (size_t)rp.adj_K * dev::kBlock * rbytes;
   } else if (adj) {
     size_t n_out = 0;
     const lmc_status ls = adjoint_layout(h, adj, &n_out, rp.adj_cbs_off);
@@ -1127,7 +1126,6 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     rp.adj_radial_sensor = adj->radial_sensor;
     rp.adj_radial_bins = adj->radial_bins;
     rp.adj_radial_max = adj->radial_max;
-    dyn_transport += (size_t)rp.adj_K * dev::kBlock * rbytes;
     if (adj->radial_sensor >= 0)
       dyn_tally = (size_t)(1 + rp.adj_K) * (adj->radial_bins + 1) * sizeof(double);
   }
@@ -1141,19 +1139,23 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio runs do not record an Absorption grid");
   const KernelFn tk = pick_transport(fp32, h->queued, three, adj != nullptr, sw, est, extras);
   const KernelFn tl = pick_tally(fp32, adj != nullptr, sw);
-  // CBS replay: queued runs without likelihood-ratio outputs, estimator or records keep
-  // no reverse-path history in the transport; the replay kernel rebuilds it for the
-  // hits that FarFieldCBS grids read
+  // CBS replay: queued runs without an estimator or records keep no reverse-path
+  // history in the transport; the replay kernel rebuilds it for the hits that
+  // FarFieldCBS grids read (likelihood-ratio scores are carried apart from it)
   bool any_cbs = false;
   for (int k = 0; k < h->n_scenes; ++k)
     any_cbs = any_cbs || (sw ? h->scenes[k] : h->scene).cbs_mask != 0;
-  const bool replay = h->queued && !adj && !est && !opts->records && !opts->no_replay &&
+  const bool replay = h->queued && !est && !opts->records && !opts->no_replay &&
                       opts->track_reverse_paths && any_cbs;
   rp.cbs_replay = replay ? 1 : 0;
   if (replay) {                          // no history: the ring and first species only
     rp.track_reverse = 0;
     dyn_transport = fp32 ? dev::side_slim_bytes<float>() : dev::side_slim_bytes<double>();
   }
+  // the likelihood-ratio scores (or the estimated grids below) follow the Side arrays
+  rp.side_off = (unsigned)dyn_transport;
+  if (adj)
+    dyn_transport += (size_t)rp.adj_K * dev::kBlock * rbytes;
   const KernelFn tr = replay ? pick_replay(fp32, sw, extras) : nullptr;
   const size_t dyn_replay = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
   int replay_grid = 0;
@@ -1169,12 +1171,20 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     // blocks per SM as one shared copy per block (shared atomics); else the latter
     const size_t shared_one = dyn_transport + est_block_doubles * sizeof(double);
     const size_t per_warp = dyn_transport + (size_t)(block / 32) * est_block_doubles * sizeof(double);
+    // the largest dynamic shared memory a block of this kernel may ask for
+    int optin = 0;
+    LMC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    cudaFuncAttributes fa;
+    LMC_CUDA(cudaFuncGetAttributes(&fa, (const void *)tk));
+    const size_t dyn_max = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
     int occ_one = 0, occ_warp = 0;
-    LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)std::max(shared_one, per_warp)));
-    LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_one, (const void *)tk, block, shared_one));
-    LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_warp, (const void *)tk, block, per_warp));
-    rp.est_per_warp = (occ_warp >= occ_one && occ_warp > 0) ? 1 : 0;
+    if (per_warp <= dyn_max) {
+      LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)std::max(shared_one, per_warp)));
+      LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_one, (const void *)tk, block, shared_one));
+      LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_warp, (const void *)tk, block, per_warp));
+    }
+    rp.est_per_warp = (per_warp <= dyn_max && occ_warp >= occ_one && occ_warp > 0) ? 1 : 0;
     rp.est_smem_doubles = (int)(rp.est_per_warp ? (block / 32) * est_block_doubles : est_block_doubles);
     dyn_transport += (size_t)rp.est_smem_doubles * sizeof(double);
   }
@@ -1185,11 +1195,17 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     for (int m = 0; m < h->scene.n_media; ++m)
       bytes += (size_t)h->scene.media[m].amp_n * sizeof(float4);
     const size_t off = (dyn_transport + 15) & ~size_t(15);
+    int optin = 0;
+    LMC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    cudaFuncAttributes fa;
+    LMC_CUDA(cudaFuncGetAttributes(&fa, (const void *)tk));
     int occ0 = 0, occ1 = 0;
-    LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(off + bytes)));
-    LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, (const void *)tk, block, dyn_transport));
-    LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, (const void *)tk, block, off + bytes));
+    if (off + bytes + fa.sharedSizeBytes <= (size_t)optin) {
+      LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(off + bytes)));
+      LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, (const void *)tk, block, dyn_transport));
+      LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, (const void *)tk, block, off + bytes));
+    }
     if (bytes > 0 && occ1 >= occ0 && occ1 > 0) {
       rp.stage_bytes = (unsigned)bytes;
       rp.stage_off = (unsigned)off;
@@ -1980,6 +1996,7 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
   const KernelFn tk = pick_transport(fp32, queued, three, false, false, false, scene_extras(sc));
   const KernelFn tl = pick_tally(fp32, false, false);
   const size_t dyn_transport = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
+  rp.side_off = (unsigned)dyn_transport;
   LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)dyn_transport));
   int per_sm = 0;
