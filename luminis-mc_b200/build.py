@@ -20,6 +20,7 @@ INCLUDE = os.path.join(REPO, "include")
 OUT_DIR = os.path.join(HERE, "luminis_mc_b200", "lib")
 OBJ_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libluminis_b200.so")
+CHECKED_LIB = os.path.join(OUT_DIR, "libluminis_b200_checked.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # Binary32 division and square root by the fast approximations, binary32 denormals
@@ -52,9 +53,15 @@ def _stale(target: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False,
+          bounds_check: bool = False) -> str:
+    """Build the library (bounds_check: the debug variant libluminis_b200_checked.so, whose
+    kernels check every table and tally index and report failed sites)."""
+    obj_dir = OBJ_DIR + ("_checked" if bounds_check else "")
+    lib = CHECKED_LIB if bounds_check else LIB
+    defines = ["-DLMC_BOUNDS_CHECK"] if bounds_check else []
     os.makedirs(OUT_DIR, exist_ok=True)
-    os.makedirs(OBJ_DIR, exist_ok=True)
+    os.makedirs(obj_dir, exist_ok=True)
     cu, cpp = _sources()
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(INCLUDE, "luminis_b200.h"))
@@ -72,21 +79,21 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
 
     for f in cu:
         src = os.path.join(CSRC, f)
-        obj = os.path.join(OBJ_DIR, f + ".o")
+        obj = os.path.join(obj_dir, f + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
             extra = ["-Xptxas", "-v"] if ptxas_info else []
-            run([nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", src, "-o", obj])
+            run([nvcc(), *ARCH, *NVCC_FLAGS, *defines, *extra, "-c", src, "-o", obj])
     cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc())), "include")   # NVTX headers
     for f in cpp:
         src = os.path.join(CSRC, f)
-        obj = os.path.join(OBJ_DIR, f + ".o")
+        obj = os.path.join(obj_dir, f + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
             run(["g++", *CXX_FLAGS, f"-I{cuda_inc}", "-c", src, "-o", obj])
-    if force or _stale(LIB, objs):
-        run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lpthread"])
-    return LIB
+    if force or _stale(lib, objs):
+        run([nvcc(), *ARCH, "-shared", "-o", lib, *objs, "-lpthread"])
+    return lib
 
 
 if __name__ == "__main__":
@@ -94,5 +101,7 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas-info", action="store_true")
+    ap.add_argument("--bounds-check", action="store_true",
+                    help="the debug variant libluminis_b200_checked.so")
     a = ap.parse_args()
-    print(build(a.force, a.verbose, a.ptxas_info))
+    print(build(a.force, a.verbose, a.ptxas_info, a.bounds_check))

@@ -10,6 +10,33 @@ namespace dev {
 
 constexpr int kGuideBuckets = 4096;     // inverse-CDF guide table size (power of two)
 
+// Bounds-checked builds (LMC_BOUNDS_CHECK, libluminis_b200_checked.so from
+// `build.py --bounds-check`): every table and tally index is checked before use.  A failed
+// check sets its site's bit in g_bounds_failed and the access is clamped (tables) or
+// skipped (tallies); the run then fails with LMC_ERR_KERNEL naming the sites.  Product
+// builds compile the checks out.
+enum BoundSite {
+  kBoundGuide = 0,            // guide-table bucket of an inverse-CDF search
+  kBoundCdf = 1,              // node index found by the search
+  kBoundAmp = 2,              // amplitude-table node of S(theta)
+  kBoundFarfield = 3,         // FarFieldCBS / far-field fluence cell
+  kBoundFluence = 4,          // PlanarFluence cell
+  kBoundField = 5,            // PlanarField cell
+  kBoundAbsorb = 6,           // Absorption grid cell
+  kBoundEst = 7,              // estimator-mode FarFieldCBS cell
+};
+#ifdef LMC_BOUNDS_CHECK
+static __device__ unsigned g_bounds_failed;
+__device__ __forceinline__ bool in_bounds(int site, bool ok)
+{
+  if (!ok)
+    atomicOr(&g_bounds_failed, 1u << site);
+  return ok;
+}
+#else
+__device__ __forceinline__ bool in_bounds(int, bool) { return true; }
+#endif
+
 // One medium as the kernel sees it.  Tables live in the handle's device arena.
 struct Medium {
   int theta_kind, theta_n, amp_n, pad;

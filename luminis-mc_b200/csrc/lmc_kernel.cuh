@@ -455,7 +455,9 @@ __device__ __forceinline__ bool find_next_interface(const Scene &sc, R zc, R zt,
 // std::lower_bound's range; the index found is the same.
 __device__ __forceinline__ double table_sample_f64(const Medium &m, double u)
 {
-  const int j = (int)(u * (double)kGuideBuckets);
+  int j = (int)(u * (double)kGuideBuckets);
+  if (!in_bounds(kBoundGuide, j >= 0 && j < kGuideBuckets))
+    j = j < 0 ? 0 : kGuideBuckets - 1;
   int lo = __ldg(m.guide_d + j), hi = __ldg(m.guide_d + j + 1);
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
@@ -464,6 +466,8 @@ __device__ __forceinline__ double table_sample_f64(const Medium &m, double u)
     else
       hi = mid;
   }
+  if (!in_bounds(kBoundCdf, lo >= 0 && lo < m.theta_n))
+    lo = lo < 0 ? 0 : m.theta_n - 1;
   if (lo == 0)
     return __ldg(m.th_val_d);
   const double c0 = __ldg(m.th_cdf_d + lo - 1), c1 = __ldg(m.th_cdf_d + lo);
@@ -479,7 +483,9 @@ __device__ __forceinline__ double table_sample_f64(const Medium &m, double u)
 __device__ __forceinline__ double table_sample_f32(const Medium &m, float u)
 {
   const double ud = u;
-  const int j = (int)(u * (float)kGuideBuckets);
+  int j = (int)(u * (float)kGuideBuckets);
+  if (!in_bounds(kBoundGuide, j >= 0 && j < kGuideBuckets))
+    j = j < 0 ? 0 : kGuideBuckets - 1;
   int lo = __ldg(m.guide_d + j), hi = __ldg(m.guide_d + j + 1);
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
@@ -488,6 +494,8 @@ __device__ __forceinline__ double table_sample_f32(const Medium &m, float u)
     else
       hi = mid;
   }
+  if (!in_bounds(kBoundCdf, lo >= 0 && lo < m.theta_n))
+    lo = lo < 0 ? 0 : m.theta_n - 1;
   if (lo == 0)
     return __ldg(m.th_val_d);
   const double c0 = __ldg(m.th_cdf_d + lo - 1);
@@ -549,7 +557,9 @@ template <> __device__ __forceinline__ void amplitudes<float>(const Medium &m, f
   } else if (pos >= (float)last) {
     a = node(last);
   } else {
-    const int i = (int)pos;
+    int i = (int)pos;
+    if (!in_bounds(kBoundAmp, i >= 0 && i < last))
+      i = i < 0 ? 0 : last - 1;
     const float t = pos - (float)i;
     const float4 y0 = node(i), y1 = node(i + 1);
     a = make_float4(y0.x + t * (y1.x - y0.x), y0.y + t * (y1.y - y0.y), y0.z + t * (y1.z - y0.z),
@@ -569,7 +579,9 @@ template <> __device__ __forceinline__ void amplitudes<double>(const Medium &m, 
   } else if (pos >= (double)last) {
     a = m.amp_d[last];
   } else {
-    const int i = (int)pos;
+    int i = (int)pos;
+    if (!in_bounds(kBoundAmp, i >= 0 && i < last))
+      i = i < 0 ? 0 : last - 1;
     const double t = pos - (double)i;
     const double4 y0 = m.amp_d[i], y1 = m.amp_d[i + 1];
     a = make_double4(y0.x + t * (y1.x - y0.x), y0.y + t * (y1.y - y0.y), y0.z + t * (y1.z - y0.z),
@@ -871,6 +883,8 @@ __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor 
   const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
   double *base = rp.tallies + s.tally_off;
   const unsigned long long P = s.plane_stride;
+  if (!in_bounds(kBoundFarfield, (unsigned long long)t_idx * tstride + cell < P))
+    return false;
   if (s.kind == LMC_SENSOR_FARFIELD_FLUENCE) {
     const double q0 = (double)(cnorm(Efx) + cnorm(Efy)), q1 = (double)(cnorm(Efx) - cnorm(Efy));
     const Cx<R> xy = cmul(Efx, Cx<R>{Efy.re, -Efy.im});
@@ -972,6 +986,8 @@ __device__ bool hit_fluence(const Scene &sc, const RunParams &rp, const Sensor &
   double *base = rp.tallies + s.tally_off;
   const unsigned long long cell = (unsigned long long)xi * s.N_y + yi;
   const unsigned long long tstride = (unsigned long long)s.N_x * s.N_y;
+  if (!in_bounds(kBoundFluence, (unsigned long long)(t_idx > 0 ? t_idx : 0) * tstride + cell < s.plane_stride))
+    return false;
   if (s.dt > 0)
     add4(base, s.plane_stride, t_idx * tstride + cell, q0, q1, q2, q3);
   add4(base, s.plane_stride, cell, q0, q1, q2, q3);
@@ -1006,6 +1022,8 @@ __device__ bool hit_field(const Scene &sc, const RunParams &rp, const Sensor &s,
   const double eyi = (double)h.Em.im * P1 + (double)h.En.im * P4;
   double *base = rp.tallies + s.tally_off;
   const unsigned long long off = ((unsigned long long)xi * s.N_y + yi) * 2;
+  if (!in_bounds(kBoundField, off + 1 < s.plane_stride))
+    return false;
   atomicAdd(base + off, (exr * pr - exi * pi) * w_sqrt);
   atomicAdd(base + off + 1, (exr * pi + exi * pr) * w_sqrt);
   atomicAdd(base + s.plane_stride + off, (eyr * pr - eyi * pi) * w_sqrt);
@@ -1491,6 +1509,8 @@ __device__ __forceinline__ void est_bin(const Scene &sc, const Sensor &s, const 
   const unsigned long long P = s.plane_stride;
   const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
   const unsigned long long cell = (unsigned long long)b;   // bins enumerate (theta, phi) row-major
+  if (!in_bounds(kBoundEst, (unsigned long long)(t_idx > 0 ? t_idx : 0) * tstride + cell < P))
+    return;
   tg.add4(P, cell, c0, c1, c2s, c3);
   tg.add4(P, 4 * P + cell, i0, i1, i2, i3);
   if (t_idx >= 1) {
@@ -1601,6 +1621,8 @@ __device__ __forceinline__ void est_bin_f32(const Scene &sc, const Sensor &s, co
   const unsigned long long PS = s.plane_stride;
   const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
   const unsigned long long cell = (unsigned long long)b;
+  if (!in_bounds(kBoundEst, (unsigned long long)(t_idx > 0 ? t_idx : 0) * tstride + cell < PS))
+    return;
   tg.add4(PS, cell, c0, c1, c2s, c3);
   tg.add4(PS, 4 * PS + cell, i0, i1, i2, i3);
   if (t_idx >= 1) {
@@ -1939,6 +1961,8 @@ __device__ __noinline__ void record_absorption(const AbsorbGrid &g, double *tall
   const unsigned long long cell = (unsigned long long)fr * (unsigned long long)g.n_z +
                                   (unsigned long long)fz;
   double *grid = tallies + g.off;
+  if (!in_bounds(kBoundAbsorb, cell < (unsigned long long)g.n_r * (unsigned long long)g.n_z))
+    return;
   atomicAdd(grid + cell, d_weight);
   if (g.d_t > 0.0) {
     const double fk = floor(t / g.d_t) + 1.0;
@@ -1964,6 +1988,8 @@ __device__ __forceinline__ void record_absorption_f32(const AbsorbGrid &g, doubl
   const unsigned long long cell = (unsigned long long)fr * (unsigned long long)g.n_z +
                                   (unsigned long long)fz;
   double *grid = tallies + g.off;
+  if (!in_bounds(kBoundAbsorb, cell < (unsigned long long)g.n_r * (unsigned long long)g.n_z))
+    return;
   atomicAdd(grid + cell, d_weight);
   if (g.d_t > 0.0) {
     const double fk = floor(t / g.d_t) + 1.0;

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -38,6 +39,28 @@ struct CudaCheck {
     if (e_ != cudaSuccess)                                                                  \
       return fail(LMC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
   } while (0)
+
+// Bounds-checked builds: the sites whose index checks failed during the run on `stream`
+// (the flag word is cleared for the next run).  Product builds have no checks: LMC_OK.
+lmc_status bounds_status(cudaStream_t stream)
+{
+#ifdef LMC_BOUNDS_CHECK
+  unsigned failed = 0;
+  LMC_CUDA(cudaMemcpyFromSymbolAsync(&failed, dev::g_bounds_failed, sizeof failed, 0,
+                                     cudaMemcpyDeviceToHost, stream));
+  LMC_CUDA(cudaStreamSynchronize(stream));
+  if (failed) {
+    const unsigned zero = 0;
+    LMC_CUDA(cudaMemcpyToSymbol(dev::g_bounds_failed, &zero, sizeof zero));
+    char msg[96];
+    std::snprintf(msg, sizeof msg, "bounds check failed at sites 0x%x (lmc::dev::BoundSite bits)", failed);
+    return fail(LMC_ERR_KERNEL, msg);
+  }
+#else
+  (void)stream;
+#endif
+  return LMC_OK;
+}
 
 }  // namespace
 
@@ -1322,7 +1345,7 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     if (sc.error_flags)
       return fail(LMC_ERR_KERNEL, "transport kernel raised error flags " + std::to_string(sc.error_flags));
   }
-  return LMC_OK;
+  return bounds_status(stream);
 }
 
 lmc_status lmc_run(lmc_handle *h, uint64_t seed, uint64_t photon_begin, uint64_t n_photons,
@@ -2059,5 +2082,5 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
   }
   if (c.error_flags)
     return fail(LMC_ERR_KERNEL, "transport kernel raised error flags " + std::to_string(c.error_flags));
-  return LMC_OK;
+  return bounds_status(stream);
 }

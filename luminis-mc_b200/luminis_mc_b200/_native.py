@@ -9,7 +9,10 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libluminis_b200.so")
+# LUMINIS_B200_LIB names another build of the library, e.g. the bounds-checked
+# lib/libluminis_b200_checked.so (luminis-mc_b200/build.py --bounds-check)
+LIB_PATH = os.environ.get("LUMINIS_B200_LIB") or os.path.join(HERE, "lib", "libluminis_b200.so")
+CHECKED_LIB_PATH = os.path.join(HERE, "lib", "libluminis_b200_checked.so")
 
 MAX_LAYERS, MAX_MEDIA, MAX_SENSORS = 16, 16, 8
 MAX_SPECIES, MAX_MIX_ENTRIES = 8, 32

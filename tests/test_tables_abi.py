@@ -27,6 +27,16 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(L, name), name
 
 
+def test_checked_library_exports_the_same_symbols():
+    """The bounds-checked debug build (build.py --bounds-check) is a drop-in for the
+    product library: it loads and exports every declared entry point."""
+    import ctypes
+    assert os.path.exists(N.CHECKED_LIB_PATH), "build the checked library (build.py --bounds-check)"
+    L = ctypes.CDLL(N.CHECKED_LIB_PATH)
+    for name in N.EXPORTED:
+        assert hasattr(L, name), name
+
+
 def test_struct_layouts_match_ctypes():
     src = r"""
 #include <stdio.h>
