@@ -1310,7 +1310,9 @@ template <typename T> struct EstV {
   __device__ __forceinline__ bool multi() const { return (ids >> 24) & 1; }
 };
 
-template <typename T> __device__ __forceinline__ void est_bcast(EstV<T> &v, int src, bool timed)
+// Every lane takes the vertex of lane src (its own source; lanes may differ): the
+// fields the bin loop reads, opath and the launch time only for a time-resolved grid.
+template <typename T> __device__ __forceinline__ void est_fetch(EstV<T> &v, int src, bool timed)
 {
 #pragma unroll
   for (int j = 0; j < 9; ++j) {
@@ -1631,11 +1633,31 @@ __device__ __forceinline__ void est_bin_f32(const Scene &sc, const Sensor &s, co
   }
 }
 
+// The lane of the (k+1)-th set bit of mask (k < popc(mask)): the smallest b with
+// popc(mask & bits 0..b) > k, by binary search on b.
+__device__ __forceinline__ int nth_set_lane(unsigned mask, int k)
+{
+  int lo = 0, hi = 31;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    const unsigned upto = (mid == 31) ? 0xffffffffu : ((2u << mid) - 1u);
+    if (__popc(mask & upto) > k)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return lo;
+}
+
 // run_estimators (src/detector.cpp:274-281, called at src/simulation.cpp:419-426) for
 // the whole warp: `at` marks the lanes whose photon is at a vertex in medium med_idx.
-// Every lane of the warp calls it (converged).  Vertices are estimated in binary64 by
-// binary64 transport and in binary32 (CBS phase and tallies binary64) by binary32
-// transport.
+// Every lane of the warp calls it (converged).  The (vertex, bin) pairs of the warp's
+// vertices are numbered vertex-major and lane j takes pairs j, j + 32, ...: in each step
+// a lane fetches the vertex of its own pair from the lane that prepared it (a shuffle
+// whose source differs from lane to lane).  For a grid of 32 bins or more the 32 pairs
+// of a step fall in 32 different bins, so a warp's private grid copy takes plain adds;
+// a smaller grid adds atomically.  Vertices are estimated in binary64 by binary64
+// transport and in binary32 (CBS phase and tallies binary64) by binary32 transport.
 template <typename R>
 __device__ __noinline__ void estimate_warp(const Scene &sc, const RunParams &rp, const Photon<R> &ph,
                                            const Side<R> &side, int med_idx, bool at,
@@ -1653,17 +1675,26 @@ __device__ __noinline__ void estimate_warp(const Scene &sc, const RunParams &rp,
     if (lane == 0 && counted)
       atomicAdd(s_hits + si, (unsigned long long)__popc(counted));
     const bool reach = want && est_reachable(sc, (double)v.pos[2], v.layer());
-    const EstTarget tg = est_target(rp, s, si, s_est);
+    const unsigned verts = __ballot_sync(kFull, reach);
+    if (!verts)
+      continue;
+    EstTarget tg = est_target(rp, s, si, s_est);
     const int nb = s.est_n;
+    if (nb < 32)
+      tg.atomic = true;                  // two pairs of a step may share a bin
     const bool timed = s.dt > 0;
-    for (unsigned pend = __ballot_sync(kFull, reach); pend; pend &= pend - 1u) {
+    const int pairs = __popc(verts) * nb;
+    for (int p0 = 0; p0 < pairs; p0 += 32) {
+      const int p = p0 + (int)lane;
+      const int k = p < pairs ? p / nb : 0;               // the vertex of this lane's pair
+      const int src = nth_set_lane(verts, k);             // its preparing lane
       EstV<T> w = v;
-      est_bcast(w, __ffs(pend) - 1, timed);
-      for (int b = (int)lane; b < nb; b += 32) {
+      est_fetch(w, src, timed);
+      if (p < pairs) {
         if constexpr (sizeof(T) == 4)
-          est_bin_f32(sc, s, w, b, tg);
+          est_bin_f32(sc, s, w, p - k * nb, tg);
         else
-          est_bin(sc, s, w, b, tg);
+          est_bin(sc, s, w, p - k * nb, tg);
       }
     }
   }

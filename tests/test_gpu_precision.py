@@ -63,4 +63,14 @@ def test_fp32_is_unbiased_against_fp64_on_long_paths(circular, cuda):
     for i, s in enumerate(spec["sensors"]):
         res = S.compare(m32[i][0], m32[i][1], R, N, m64[i][0], m64[i][1], R, N,
                         max_rse=None if s["kind"] == "planar_field" else 0.25)
-        S.assert_agree(res, f"{what}/{s['kind']}", t2_range=(0.3, 1.8))
+        S.assert_agree(res, f"{what}/{s['kind']}", max_abs_t=max_t_over(res["n_tested"]),
+                       t2_range=(0.3, 1.8))
+
+
+def max_t_over(n_bins, df=2 * R - 2, false_alarm=1e-3):
+    """The bar on the largest |t| over n_bins Welch statistics of 16 + 16 replicas:
+    the Student-t quantile at which all bins together exceed it with probability
+    false_alarm (8.2 over the 262,144 speckle bins, 5.8 over 400 cone bins).  A fixed
+    bar of 6 would fail about one run in six on the speckle grid: 6.28 was measured."""
+    from scipy import stats
+    return max(6.0, float(stats.t.ppf(1.0 - false_alarm / (2.0 * max(n_bins, 1)), df)))
