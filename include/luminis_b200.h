@@ -218,8 +218,8 @@ typedef struct lmc_run_opts {
                                    that keeps the blocks per SM; 0 reads them through L1  */
   int no_replay;                /* 1: the transport keeps every photon's reverse-path history
                                    instead of replaying the photons a FarFieldCBS grid reads
-                                   (replay is used by queued runs without records,
-                                   likelihood-ratio outputs or estimator sensors)         */
+                                   (replay is used by queued runs without records or
+                                   estimator sensors, likelihood-ratio runs included)     */
 } lmc_run_opts;
 
 /* Final state of one photon, written when opts.records is set (the same layout as
