@@ -144,10 +144,10 @@ template <int kStride> struct RngT {
 };
 using Rng = RngT<kBlock>;
 
-// One copy of the ten rounds (a call keeps the event loop small enough for the
-// instruction cache).
-__device__ __noinline__ uint4 philox_block(uint32_t block, uint32_t p_lo, uint32_t p_hi,
-                                           uint32_t key0, uint32_t key1)
+// The ten rounds of one block, inlined where the ring is filled: at the once-per-event
+// prefetch and at a draw that finds the ring dry.
+__device__ __forceinline__ uint4 philox_block(uint32_t block, uint32_t p_lo, uint32_t p_hi,
+                                              uint32_t key0, uint32_t key1)
 {
   uint32_t c0 = block, c1 = 0u, c2 = p_lo, c3 = p_hi;
   uint32_t k0 = key0, k1 = key1;
@@ -642,6 +642,23 @@ __device__ __forceinline__ float exit_theta(float sx, float sy, float sz)
   return atan2f(sqrtf(sx * sx + sy * sy), -sz);
 }
 
+// The exit direction as the sensors' angular tests read it.  Binary32 transport's
+// direction drifts off unit length as a random walk of its roundings (|s| - 1 ~ 6e-8
+// sqrt(events): ~6e-6 after 1e4 events), and a cosine test on a narrow cone (1 - cos 20
+// mrad = 2e-4) turns that into lost hits at both edges (3.7 % of a 20 mrad cone's hits
+// at 1.1e4 events per photon), so binary32 divides by |s| in binary64.  Binary64 keeps the
+// reference's components as they are (|s| - 1 ~ 1e-15).
+__device__ __forceinline__ void exit_dir(double sx, double sy, double sz, double *d)
+{
+  d[0] = sx; d[1] = sy; d[2] = sz;
+}
+__device__ __forceinline__ void exit_dir(float sx, float sy, float sz, double *d)
+{
+  const double x = sx, y = sy, z = sz;
+  const double inv = 1.0 / sqrt(x * x + y * y + z * z);
+  d[0] = x * inv; d[1] = y * inv; d[2] = z * inv;
+}
+
 // ---------------------------------------------------------------- source
 // Laser::emit_photon's random part (src/laser.cpp:11-28, :42-75, :77-99): launch
 // x, y and emission time, drawn from the photon's stream starting at draw 0.
@@ -1111,8 +1128,9 @@ __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData
     else if (s.kind == LMC_SENSOR_STATISTICS) {
       const double arrival = (s.dt > 0 || (s.stat->set & LMC_STAT_TIME))
                                  ? hit_launch_time<R>(sc, rp, h) + h.opath : 0.0;
-      hit_statistics(s, rp.tallies, arrival, h.events, (double)h.P[6], (double)h.P[7],
-                     (double)h.P[8], h.pen, h.w);
+      double d[3];
+      exit_dir(h.P[6], h.P[7], h.P[8], d);
+      hit_statistics(s, rp.tallies, arrival, h.events, d[0], d[1], d[2], h.pen, h.w);
       counted = true;
     }
     else
@@ -1294,13 +1312,14 @@ __device__ __forceinline__ EstTarget est_target(const RunParams &rp, const Senso
 
 // A vertex as the estimate reads it, in the estimate's precision T (binary64 for
 // binary64 transport, binary32 for binary32 transport, whose positions are binary32
-// already).  Small, because every lane holds its own vertex and the one broadcast.
+// already).  Small, because every lane holds its own vertex and the one broadcast:
+// r_1 and the frame after the first scatter stay in the source lane's Side column in
+// shared memory, where the bin reads them.
 template <typename T> struct EstV {
-  T P[9], P1[9];                // frame at the vertex; frame after the first scatter
+  T P[9];                       // frame at the vertex
   Cx<T> Em, En;                 // Jones vector
   Cx<T> pre_m, pre_n;           // reverse path through stages A + B (from the 2nd vertex)
   T pos[3];                     // vertex
-  T dr[3];                      // r_n - r_1 (CBS phase), formed in binary64
   T wgt;                        // binary64: w mu_s / mu_t; binary32: that / (pi I_norm)
   double opath, t_launch;       // broadcast only for a time-resolved grid
   int ids;                      // medium | first medium << 8 | layer << 16 | multi << 24
@@ -1317,7 +1336,6 @@ template <typename T> __device__ __forceinline__ void est_fetch(EstV<T> &v, int 
 #pragma unroll
   for (int j = 0; j < 9; ++j) {
     v.P[j] = __shfl_sync(kFull, v.P[j], src);
-    v.P1[j] = __shfl_sync(kFull, v.P1[j], src);
   }
   v.Em.re = __shfl_sync(kFull, v.Em.re, src);
   v.Em.im = __shfl_sync(kFull, v.Em.im, src);
@@ -1328,10 +1346,8 @@ template <typename T> __device__ __forceinline__ void est_fetch(EstV<T> &v, int 
   v.pre_n.re = __shfl_sync(kFull, v.pre_n.re, src);
   v.pre_n.im = __shfl_sync(kFull, v.pre_n.im, src);
 #pragma unroll
-  for (int j = 0; j < 3; ++j) {
+  for (int j = 0; j < 3; ++j)
     v.pos[j] = __shfl_sync(kFull, v.pos[j], src);
-    v.dr[j] = __shfl_sync(kFull, v.dr[j], src);
-  }
   v.wgt = __shfl_sync(kFull, v.wgt, src);
   v.ids = __shfl_sync(kFull, v.ids, src);
   if (timed) {
@@ -1363,14 +1379,9 @@ __device__ __forceinline__ bool est_prepare(const Scene &sc, const RunParams &rp
   const int tid = threadIdx.x;
   const double px = ph.px, py = ph.py, pz = ph.pz;
   v.pos[0] = (T)px; v.pos[1] = (T)py; v.pos[2] = (T)pz;
-  v.dr[0] = (T)(px - (double)side.first[0][tid]);
-  v.dr[1] = (T)(py - (double)side.first[1][tid]);
-  v.dr[2] = (T)(pz - (double)side.first[2][tid]);
 #pragma unroll
-  for (int j = 0; j < 9; ++j) {
+  for (int j = 0; j < 9; ++j)
     v.P[j] = (T)ph.P[j];
-    v.P1[j] = (T)side.first[3 + j][tid];
-  }
   v.Em = {(T)ph.Em.re, (T)ph.Em.im};
   v.En = {(T)ph.En.re, (T)ph.En.im};
   v.opath = ph.opath;
@@ -1414,10 +1425,23 @@ __device__ __forceinline__ bool est_reachable(const Scene &sc, double z, int lay
   return !(mu * z > 47.0);
 }
 
+// r_1 and the frame after the first scatter of the vertex prepared by thread st,
+// from its Side column; r_n - r_1 (CBS phase) formed in binary64.
+template <typename T>
+__device__ __forceinline__ void est_first(const Side<T> &side, int st, const T *pos, T *P1, T *dr)
+{
+#pragma unroll
+  for (int j = 0; j < 9; ++j)
+    P1[j] = side.first[3 + j][st];
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    dr[j] = (T)((double)pos[j] - (double)side.first[j][st]);
+}
+
 // One bin of one vertex, binary64 (FarFieldCBSSensor::process_estimation,
-// src/detector.cpp:1384-1560, per bin).
+// src/detector.cpp:1384-1560, per bin); src_t: the thread that prepared the vertex.
 __device__ __forceinline__ void est_bin(const Scene &sc, const Sensor &s, const EstV<double> &v, int b,
-                                        const EstTarget &tg)
+                                        const Side<double> &side, int src_t, const EstTarget &tg)
 {
   const Laser &L = sc.laser;
   const Medium &med = sc.media[v.med()];
@@ -1487,10 +1511,12 @@ __device__ __forceinline__ void est_bin(const Scene &sc, const Sensor &s, const 
   if (v.multi()) {
     const V3<double> s_in = v3<double>(L.dir[0], L.dir[1], L.dir[2]);
     Cx<double> Rm, Rn;
-    est_suffix(sc, v.P1, Pe, v.first_med(), v.pre_m, v.pre_n, Rm, Rn);
+    double P1[9], dr[3];
+    est_first(side, src_t, v.pos, P1, dr);
+    est_suffix(sc, P1, Pe, v.first_med(), v.pre_m, v.pre_n, Rm, Rn);
     const double qx = (s_out.x + s_in.x) * L.k, qy = (s_out.y + s_in.y) * L.k,
                  qz = (s_out.z + s_in.z) * L.k;
-    const double arg = qx * v.dr[0] + qy * v.dr[1] + qz * v.dr[2];
+    const double arg = qx * dr[0] + qy * dr[1] + qz * dr[2];
     double sp_, cp_;
     sincos(arg, &sp_, &cp_);
     const Cx<double> pp = {cp_, sp_};
@@ -1527,7 +1553,7 @@ __device__ __forceinline__ void est_bin(const Scene &sc, const Sensor &s, const 
 // and Stokes values, accumulated in binary64.  The CBS phase q . (r_n - r_1) uses the
 // table's q = k (s_out + s_in), formed in binary64, and r_n - r_1 formed in binary64.
 __device__ __forceinline__ void est_bin_f32(const Scene &sc, const Sensor &s, const EstV<float> &v, int b,
-                                            const EstTarget &tg)
+                                            const Side<float> &side, int src_t, const EstTarget &tg)
 {
   const Medium &med = sc.media[v.med()];
   const float4 *bf = reinterpret_cast<const float4 *>(s.est_bins + s.est_n);
@@ -1600,9 +1626,11 @@ __device__ __forceinline__ void est_bin_f32(const Scene &sc, const Sensor &s, co
   Cx<float> Erx = {0.f, 0.f}, Ery = {0.f, 0.f};
   if (v.multi()) {
     Cx<float> Rm, Rn;
-    est_suffix<float>(sc, v.P1, Pe, v.first_med(), v.pre_m, v.pre_n, Rm, Rn);
+    float P1[9], dr[3];
+    est_first(side, src_t, v.pos, P1, dr);
+    est_suffix<float>(sc, P1, Pe, v.first_med(), v.pre_m, v.pre_n, Rm, Rn);
     const float4 q = bf[2 * b + 1];
-    const float arg = q.x * v.dr[0] + q.y * v.dr[1] + q.z * v.dr[2];
+    const float arg = q.x * dr[0] + q.y * dr[1] + q.z * dr[2];
     float sp_, cp_;
     sincosf(arg, &sp_, &cp_);
     const Cx<float> pp = {cp_ * amp, sp_ * amp};
@@ -1684,6 +1712,7 @@ __device__ __noinline__ void estimate_warp(const Scene &sc, const RunParams &rp,
       tg.atomic = true;                  // two pairs of a step may share a bin
     const bool timed = s.dt > 0;
     const int pairs = __popc(verts) * nb;
+    __syncwarp();                        // the lanes' Side columns, read across the warp
     for (int p0 = 0; p0 < pairs; p0 += 32) {
       const int p = p0 + (int)lane;
       const int k = p < pairs ? p / nb : 0;               // the vertex of this lane's pair
@@ -1691,10 +1720,11 @@ __device__ __noinline__ void estimate_warp(const Scene &sc, const RunParams &rp,
       EstV<T> w = v;
       est_fetch(w, src, timed);
       if (p < pairs) {
+        const int st = (int)(threadIdx.x & ~31u) + src;
         if constexpr (sizeof(T) == 4)
-          est_bin_f32(sc, s, w, p - k * nb, tg);
+          est_bin_f32(sc, s, w, p - k * nb, side, st, tg);
         else
-          est_bin(sc, s, w, p - k * nb, tg);
+          est_bin(sc, s, w, p - k * nb, side, st, tg);
       }
     }
   }
@@ -1710,7 +1740,9 @@ __device__ __forceinline__ bool check_conditions(const Sensor &s, double hx, dou
   if (s.f_events && ((int)ph.events < s.events_min || (int)ph.events > s.events_max))
     return false;
   if (s.f_theta) {
-    const double ct = -1.0 * (double)ph.P[8];
+    double d[3];
+    exit_dir(ph.P[6], ph.P[7], ph.P[8], d);
+    const double ct = -1.0 * d[2];
     if (ct < s.cos_min || ct > s.cos_max)
       return false;
   }
@@ -2006,7 +2038,7 @@ __device__ __noinline__ void record_absorption(const AbsorbGrid &g, double *tall
 // The same deposit for the binary32 transport: the cell from the binary32 position by
 // reciprocal multiplies instead of binary64 divisions.  The position itself carries
 // binary32 rounding (~1e-7 relative), so the bin edges are no blurrier than the position.
-// Short enough to inline without spills (80 registers, 3 blocks per SM kept).
+// Short enough to inline into the binary32 transport.
 __device__ __forceinline__ void record_absorption_f32(const AbsorbGrid &g, double *tallies, float x,
                                                    float y, float z, double t, double d_weight)
 {
@@ -2165,7 +2197,7 @@ __device__ __forceinline__ int event_scatter(const Scene &sc, const RunParams &r
     if (ph.rng.filled >= (ph.rng.draw + 2u * kSpec) * wpd) {
       bool acc = false;
       uint32_t take = 2u * kSpec;
-#pragma unroll
+#pragma unroll 1                  // rolled: a smaller event loop for the instruction cache
       for (int t = 0; t < kSpec; ++t) {
         const R u1 = peek_uniform<R>(ph.rng, rp, 2u * t);
         const R u2 = peek_uniform<R>(ph.rng, rp, 2u * t + 1u);

@@ -962,7 +962,7 @@ static lmc_status sweep_adjoint_layout(const lmc_handle *h, const lmc_adjoint_op
 using KernelFn = void (*)(const lmc::dev::Scene *, lmc::dev::RunParams);
 
 template <bool E>
-static KernelFn pick_transport_e(bool fp32, bool queued, bool three, bool adj, bool sw, bool est)
+static KernelFn pick_transport_e(bool fp32, bool queued, bool wide, bool adj, bool sw, bool est)
 {
   using namespace lmc::dev;
   if (est)
@@ -976,17 +976,17 @@ static KernelFn pick_transport_e(bool fp32, bool queued, bool three, bool adj, b
   if (adj)
     return fp32 ? transport_kernel<float, true, 3, true> : transport_kernel<double, true, 1, true>;
   if (fp32)
-    return queued ? (three ? transport_kernel<float, true, 3, false, false, false, E>
+    return queued ? (wide ? transport_kernel<float, true, 4, false, false, false, E>
                            : transport_kernel<float, true, 2, false, false, false, E>)
                   : transport_kernel<float, false, 1, false, false, false, E>;
   return queued ? transport_kernel<double, true, 2, false, false, false, E>
                 : transport_kernel<double, false, 1, false, false, false, E>;
 }
 
-static KernelFn pick_transport(bool fp32, bool queued, bool three, bool adj, bool sw, bool est, bool extras)
+static KernelFn pick_transport(bool fp32, bool queued, bool wide, bool adj, bool sw, bool est, bool extras)
 {
-  return extras ? pick_transport_e<true>(fp32, queued, three, adj, sw, est)
-                : pick_transport_e<false>(fp32, queued, three, adj, sw, est);
+  return extras ? pick_transport_e<true>(fp32, queued, wide, adj, sw, est)
+                : pick_transport_e<false>(fp32, queued, wide, adj, sw, est);
 }
 
 static KernelFn pick_tally(bool fp32, bool adj, bool sw)
@@ -1152,15 +1152,15 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     if (adj->radial_sensor >= 0)
       dyn_tally = (size_t)(1 + rp.adj_K) * (adj->radial_bins + 1) * sizeof(double);
   }
-  // binary32 queued transport: a 3-block (<=85 registers, the default) and a
+  // binary32 queued transport: a 4-block (<=64 registers, the default) and a
   // 2-block (<=128 registers) variant; blocks_per_sm == 1 or 2 selects the latter
-  const bool three = fp32 && h->queued && !adj && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
+  const bool wide = fp32 && h->queued && !adj && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
   bool extras = false;
   for (int k = 0; k < h->n_scenes; ++k)
     extras = extras || scene_extras(sw ? h->scenes[k] : h->scene);
   if (adj && extras)                     // (MixtureLayers are refused by the layout already)
     return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio runs do not record an Absorption grid");
-  const KernelFn tk = pick_transport(fp32, h->queued, three, adj != nullptr, sw, est, extras);
+  const KernelFn tk = pick_transport(fp32, h->queued, wide, adj != nullptr, sw, est, extras);
   const KernelFn tl = pick_tally(fp32, adj != nullptr, sw);
   // CBS replay: queued runs without an estimator or records keep no reverse-path
   // history in the transport; the replay kernel rebuilds it for the hits that
@@ -2015,8 +2015,8 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
   if (block % 32 != 0 || block > dev::kBlock)
     return fail(LMC_ERR_INVALID, "block_size must be a multiple of 32 and at most 256");
   // the kernels lmc_run picks for the same scene and options
-  const bool three = fp32 && queued && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
-  const KernelFn tk = pick_transport(fp32, queued, three, false, false, false, scene_extras(sc));
+  const bool wide = fp32 && queued && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
+  const KernelFn tk = pick_transport(fp32, queued, wide, false, false, false, scene_extras(sc));
   const KernelFn tl = pick_tally(fp32, false, false);
   const size_t dyn_transport = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
   rp.side_off = (unsigned)dyn_transport;
