@@ -47,10 +47,10 @@ def _hbm_peak():
 
 HBM_PEAK_GBS = _hbm_peak()
 # DRAM bytes (read + write) per photon of one FP32 transport launch on bilayer_rgd_mie
-# with CBS replay: 2.12 MB read + 133.11 MB written for a 2 M-photon launch in one ncu
+# with CBS replay: 2.41 MB read + 138.82 MB written for a 2 M-photon launch in one ncu
 # capture of the transport kernel; the traffic is the hit queue, so it grows with the
 # photons.
-TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": (2.120192e6 + 133.112832e6) / 2e6}
+TRAFFIC_BYTES_PER_PHOTON = {"bilayer_rgd_mie": (2.405120e6 + 138.818048e6) / 2e6}
 
 
 def parse():
