@@ -32,6 +32,13 @@ sys.path.insert(0, os.path.join(REPO, "luminis-mc_b200"))
 sys.path.insert(0, REPO)
 
 FLOP_PER_EVENT = 300        # FP32 flops per scattering event (add/mul = 1, FMA = 2)
+# FP32 flops of one (vertex, bin) pair of the estimator-mode FarFieldCBS, counted from the
+# reference's per-bin arithmetic (FarFieldCBSSensor::process_estimation,
+# src/detector.cpp:1384-1560) for a vertex from the second event on: the exit frame and
+# forward field (~185), the reverse path's last stage and its normalisation (~205), the
+# CBS phase and reverse field (~30), the Stokes values and their accumulation (~62);
+# plus ~13 SFU operations (exp, sqrt, atan2, sincos) not counted.
+FLOP_PER_EST_PAIR = 480
 METRIC = "photons/s"
 
 
@@ -772,6 +779,8 @@ def measure_estimator(args, local, stream, flush, world, rank, max_ms):
     espec["sensors"] = [dict(espec["sensors"][0], estimator=True)]
     ecfg, _, ekeep = W.build(lm, espec)
     PE = int(espec["n_photons"])
+    from luminis_mc_b200 import _native as N
+    n_bins = int(round(espec["sensors"][0]["theta_max"] / espec["sensors"][0]["d_theta"]))
     for prec in ("fp64", "fp32"):
         run = DeviceRun(ecfg, device=f"cuda:{local}")
         run.run(20_000, 4242, precision=prec, stream=stream.cuda_stream)
@@ -782,6 +791,16 @@ def measure_estimator(args, local, stream, flush, world, rank, max_ms):
         out[f"estimator_{prec}"] = {"value": PE * world / (ms * 1e-3), "unit": "photons/s",
                                     "workload": "mie_cbs_small, FarFieldCBS 100x1 in estimator mode",
                                     "photons": PE}
+        if prec == "fp32":
+            # every estimated vertex (the sensor's hit count) against every bin of the grid
+            pairs = st["hits"][0] * n_bins
+            peak, _ = N.probe_fp32_peak(200000)
+            achieved = pairs * FLOP_PER_EST_PAIR / (st["transport_ms"] * 1e-3) / 1e12
+            out["estimator_fp32"]["roofline"] = {
+                "bound": "fp32-issue", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "flop_per_pair": FLOP_PER_EST_PAIR, "pairs": pairs,
+                "kernel": "transport_kernel (estimator mode)", "ms": st["transport_ms"],
+                "peak_source": "measured: FFMA probe (lmc_probe_fp32_peak) on this GPU"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             rate, n, dt = reference_sample(espec, 6.0, os.cpu_count() or 1)
