@@ -476,10 +476,11 @@ def measure_long_paths(args, local, stream, flush, world, rank, max_ms):
     """The precision-stress workload (mie_long_paths: mu_s = 100/mm, mu_a = 1e-4/mm,
     ~1.1e4 events per photon, FarFieldCBS 400 bins to 20 mrad, 256 x 256 speckle grid),
     linear and circular polarisation, binary32 and binary64 transport, 1e7 photons per
-    run.  photons/s and scattering events/s from device time.  Each run ends with the few
-    photons whose paths reach MAX_EVENTS (1e6 events; ~4e-4 of them) running alone for a
-    few seconds, one event after another: at 2e6 photons that tail is most of the run
-    (~0.32 M photons/s in either precision), at 1e7 the bulk of the work hides most of it."""
+    run.  photons/s and scattering events/s from device time.  5.5e-3 of the photons reach
+    MAX_EVENTS (1e6 events) and carry half of all events; a run ends with the last of them
+    running on a nearly idle GPU, one event after another, for a few seconds: at 2e6
+    photons that tail is most of the run (~0.32 M photons/s in either precision), at 1e7
+    the bulk of the work hides most of it."""
     import luminis_mc_b200 as lm
     from luminis_mc_b200 import workloads as W
     from luminis_mc_b200.device import DeviceRun
