@@ -254,6 +254,19 @@ def probe_fp32_peak(iters: int = 200000) -> tuple[float, float]:
     return t.value, ms.value
 
 
+# cudaStreamLegacy: the legacy default stream, on which torch's default stream runs.  In
+# lmc_run_opts.stream a NULL handle selects the lmc handle's own (non-blocking) stream, which
+# torch's default-stream work does not wait for.
+CUDA_STREAM_LEGACY = 1
+
+
+def launch_stream(stream):
+    """The cudaStream_t to put in lmc_run_opts.stream for a Python caller: a stream handle
+    (torch's `Stream.cuda_stream`) as given; None, or torch's default-stream handle 0, the
+    legacy default stream, so that the run is ordered with torch's default-stream work."""
+    return CUDA_STREAM_LEGACY if not stream else stream
+
+
 def last_error() -> str:
     buf = C.create_string_buffer(1024)
     lib().lmc_last_error(buf, 1024)

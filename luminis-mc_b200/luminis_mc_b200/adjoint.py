@@ -112,7 +112,7 @@ class AdjointTransport:
             o.precision = N.PRECISION[precision]
             o.max_events = int(self.config.MAX_EVENTS)
             o.track_reverse_paths = int(bool(self.config.track_reverse_paths))
-            o.stream = stream
+            o.stream = N.launch_stream(stream)
             st = N.Stats()
             torch.cuda.synchronize(self.device)
             N.check(N.lib().lmc_run_adjoint(self._handle, int(seed) & (2 ** 64 - 1), int(begin),

@@ -275,7 +275,7 @@ class Transport:
         o.block_size = int(block_size)
         o.blocks_per_sm = int(blocks_per_sm)
         o.records = records_ptr
-        o.stream = stream
+        o.stream = N.launch_stream(stream)
         o.batch_photons = int(batch_photons)
         o.stream_format = int(stream_format)
         o.host_tallies_zero = int(bool(host_tallies_zero))

@@ -73,7 +73,7 @@ class SweepRun:
         o.precision = N.PRECISION[precision]
         o.max_events = int(c.MAX_EVENTS if max_events is None else max_events)
         o.track_reverse_paths = int(any(bool(cfg.track_reverse_paths) for cfg in self.configs))
-        o.stream = stream
+        o.stream = N.launch_stream(stream)
         for key, value in self.launch.items():
             setattr(o, key, value)
         return o

@@ -169,3 +169,12 @@ def test_build_mie_sweep_refuses_other_specs():
     mismatch["media"][0]["radius"] *= 2
     with pytest.raises(ValueError, match="same particle"):
         W.build_mie_sweep(lm, [mismatch])
+
+
+def test_python_default_stream_maps_to_the_legacy_stream():
+    """A NULL lmc_run_opts.stream selects the handle's own non-blocking stream; the Python
+    layer passes the legacy default stream for None and for torch's default-stream handle 0
+    (so runs are ordered with torch's default-stream work) and other handles as given."""
+    assert N.launch_stream(None) == N.CUDA_STREAM_LEGACY == 1
+    assert N.launch_stream(0) == N.CUDA_STREAM_LEGACY
+    assert N.launch_stream(12345) == 12345
