@@ -35,9 +35,8 @@ def test_run_is_ordered_with_torch_work(stream, cuda):
         if stream == "created":
             s = torch.cuda.Stream()
             t.run_device(buf.data_ptr(), N_PHOTONS, 1, 0, want_stats=False, stream=s.cuda_stream)
-            with torch.cuda.stream(s):
-                early = buf.sum()
-            got = float(early.item())
+            with torch.cuda.stream(s):                  # the sum and its read-back on s
+                got = float(buf.sum().item())
         else:
             t.run_device(buf.data_ptr(), N_PHOTONS, 1, 0, want_stats=False, stream=stream)
             got = float(buf.sum().item())          # torch's default stream, no synchronise
