@@ -142,6 +142,7 @@ struct Scratch {
   unsigned long long next_photon;        // reset per batch
   unsigned long long queue_count;        // reset per batch
   unsigned long long replay_count;       // reset per batch: entries of RunParams::replay_list
+  unsigned long long replay_next;        // reset per batch: the replay kernel's next list entry
   unsigned long long photons, events, steps, detected, escaped, stack, roulette, cap, draws;
   unsigned long long hits[LMC_MAX_SENSORS];
   unsigned long long replayed;           // CBS replays over the run's batches

@@ -2590,9 +2590,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_kernel(const Sce
 // species) into its queue entry, where the tally kernel reads them.  The replay must
 // reach the recorded hit state: the frame and Jones vector after the last event are
 // compared with the entry's, and a replay that does not match, or whose photon ends
-// early, raises kErrReplay.  Each thread takes list entries in turn.
+// early, raises kErrReplay.  Persistent like the transport: each loop iteration advances
+// every busy lane by one event, and a lane whose replay is finished takes the next list
+// entry from a shared counter (warp-aggregated), so a warp never waits for the longest
+// of 32 replays that were handed out together.
 template <typename R, bool kSweep = false, bool kExtras = false>
-__global__ void __launch_bounds__(kBlock, 2) cbs_replay_kernel(const Scene *__restrict__ g_scene, RunParams rp)
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 3 : 2)
+    cbs_replay_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
   __shared__ __align__(16) unsigned char s_raw[kSweep ? 16 : sizeof(Scene)];
   extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -2607,29 +2611,58 @@ __global__ void __launch_bounds__(kBlock, 2) cbs_replay_kernel(const Scene *__re
   if (blockIdx.x == 0 && threadIdx.x == 0)
     atomicAdd(&rp.scratch->replayed, n);
   rp.track_reverse = 1;
+  const unsigned lane = threadIdx.x & 31u;
+  const int tid = threadIdx.x;
   Photon<R> ph;
   ph.rng.ring = &side.ring[0][threadIdx.x];
   Flight<R> fl;
   fl.score = nullptr;
   Counters cnt = {0, 0, 0};
   R *r = static_cast<R *>(q.r);
-  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
-       i += (unsigned long long)gridDim.x * blockDim.x) {
-    const unsigned long long slot = rp.replay_list[i];
-    const unsigned scene = kSweep ? q.u32[kQScene * C + slot] : 0u;
-    const Scene &sc = kSweep ? g_scene[scene] : *reinterpret_cast<const Scene *>(s_raw);
-    const unsigned long long index =
-        ((unsigned long long)q.u32[kQPhotonHi * C + slot] << 32) | q.u32[kQPhotonLo * C + slot];
-    const uint32_t target = q.u32[kQEvents * C + slot];
-    init_photon<R>(sc, rp, ph, side, index);
-    bool ok = true;
-    while (ok && ph.events < target) {
-      int med = 0;
-      int fate = event_move<R, true, false, kExtras, false>(sc, rp, ph, side, fl, cnt, nullptr, med);
-      if (fate == kAlive)
-        fate = event_scatter<R, false, kExtras, false>(sc, rp, ph, side, fl, cnt, med);
-      ok = fate == kAlive;
+  const Scene *scp = kSweep ? g_scene : reinterpret_cast<const Scene *>(s_raw);
+  unsigned long long slot = 0;
+  uint32_t target = 0;
+  bool busy = false, done = false;
+  for (;;) {
+    const unsigned need = __ballot_sync(kFull, !busy && !done);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if ((int)lane == leader)
+        base = atomicAdd(&rp.scratch->replay_next, (unsigned long long)__popc(need));
+      base = __shfl_sync(kFull, base, leader);
+      if (!busy && !done) {
+        const unsigned long long i = base + __popc(need & ((1u << lane) - 1u));
+        if (i < n) {
+          slot = rp.replay_list[i];
+          if (kSweep)
+            scp = g_scene + q.u32[kQScene * C + slot];
+          const unsigned long long index =
+              ((unsigned long long)q.u32[kQPhotonHi * C + slot] << 32) | q.u32[kQPhotonLo * C + slot];
+          target = q.u32[kQEvents * C + slot];
+          init_photon<R>(*scp, rp, ph, side, index);
+          busy = true;
+        } else {
+          done = true;
+        }
+      }
     }
+    if (__all_sync(kFull, done))
+      break;
+    if (!busy)
+      continue;
+    if (ph.events < target) {                    // one more event of this replay
+      int med = 0;
+      int fate = event_move<R, true, false, kExtras, false>(*scp, rp, ph, side, fl, cnt, nullptr, med);
+      if (fate == kAlive)
+        fate = event_scatter<R, false, kExtras, false>(*scp, rp, ph, side, fl, cnt, med);
+      if (fate != kAlive) {                      // ended before its recorded hit
+        atomicOr(&rp.scratch->error_flags, (unsigned)kErrReplay);
+        busy = false;
+      }
+      continue;
+    }
+    busy = false;
     // the frame and Jones vector of the hit are those after the last scatter
     R dev = R(0);
 #pragma unroll
@@ -2639,11 +2672,10 @@ __global__ void __launch_bounds__(kBlock, 2) cbs_replay_kernel(const Scene *__re
     dev = fmax(dev, fabs(ph.Em.im - r[(kQE + 1) * C + slot]));
     dev = fmax(dev, fabs(ph.En.re - r[(kQE + 2) * C + slot]));
     dev = fmax(dev, fabs(ph.En.im - r[(kQE + 3) * C + slot]));
-    if (!ok || ph.events != target || !(dev <= R(1e-3))) {
+    if (ph.events != target || !(dev <= R(1e-3))) {
       atomicOr(&rp.scratch->error_flags, (unsigned)kErrReplay);
       continue;
     }
-    const int tid = threadIdx.x;
     q.u32[kQMedia * C + slot] = (uint32_t)side.first_med[tid] | ((uint32_t)ph.last_med << 16);
 #pragma unroll
     for (int j = 0; j < 3; ++j) {

@@ -1292,8 +1292,8 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
     rp.photon_begin = photon_begin + done;
     rp.n_photons = nb;
     rp.records = records ? records + done : nullptr;   // the kernels index from photon_begin
-    // reset the work counter and the queue fill of this batch
-    LMC_CUDA(cudaMemsetAsync(h->d_scratch, 0, 3 * sizeof(unsigned long long), stream));
+    // reset the work counters (transport, replay) and the queue fills of this batch
+    LMC_CUDA(cudaMemsetAsync(h->d_scratch, 0, 4 * sizeof(unsigned long long), stream));
     const int grid = (int)std::max<unsigned long long>(
         1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * per_sm,
                                            (nb + block - 1) / block));
@@ -2054,7 +2054,7 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     rp.photon_begin = photon_begin + done;
     rp.n_photons = nb;
     rp.records = records ? records + done : nullptr;   // the kernels index from photon_begin
-    LMC_CUDA(cudaMemsetAsync(d_counters, 0, 3 * sizeof(unsigned long long), stream));
+    LMC_CUDA(cudaMemsetAsync(d_counters, 0, 4 * sizeof(unsigned long long), stream));
     const int grid = (int)std::max<unsigned long long>(
         1ull, std::min<unsigned long long>((unsigned long long)sm_count * per_sm, (nb + block - 1) / block));
     tk<<<grid, block, dyn_transport, stream>>>(d_scene, rp);
