@@ -80,6 +80,9 @@ def parse():
                     help="binary32 amplitude tables staged in shared memory (1-D bulk copies)")
     ap.add_argument("--no-replay", action="store_true",
                     help="keep every photon's reverse-path history instead of replaying CBS hits")
+    ap.add_argument("--tally-mode", default="default",
+                    choices=["default", "global", "warp", "shared"],
+                    help="how the hit-queue tally kernel adds into the sensor grids")
     ap.add_argument("--variant-steps", type=int, default=2,
                     help="timed steps of the FP64 and FP32+adjoint variants (0: skip them)")
     ap.add_argument("--variants", default="fp64,differentiable,sweep,estimator,f2,long_paths",
@@ -109,7 +112,8 @@ def config_block(spec, args, n_gpus):
             "blocks_per_sm": args.blocks_per_sm or "auto",
             "batch_photons": args.batch_photons or (32 << 20),
             "cbs_history": "tracked per event" if args.no_replay else "replayed for CBS-grid hits",
-            "amplitude_tables": "shared memory (bulk copies)" if args.stage_tables else "global via L1"}
+            "amplitude_tables": "shared memory (bulk copies)" if args.stage_tables else "global via L1",
+            "tally_mode": args.tally_mode}
 
 
 # ------------------------------------------------------------------------- clocks
@@ -291,7 +295,8 @@ def run_ours(args):
         st, _ = run.run(P, seed, begin=(k * world * P) + base, precision=args.precision,
                         stream=stream.cuda_stream, block_size=args.block_size,
                         blocks_per_sm=args.blocks_per_sm, batch_photons=args.batch_photons,
-                        stage_tables=args.stage_tables, no_replay=args.no_replay)
+                        stage_tables=args.stage_tables, no_replay=args.no_replay,
+                        tally_mode=args.tally_mode)
         return st
 
     for k in range(args.warmup):
@@ -677,6 +682,7 @@ def measure_sweep(args, local, stream, flush, world, rank, max_ms):
     from luminis_mc_b200.adjoint import AdjointTransport
 
     out = {}
+    from luminis_mc_b200 import _native as N
     from luminis_mc_b200.sweep import SweepRun
     from luminis_mc_b200.simulation import Transport
     _, _, _, counts = W.mie_sweep_parameters()
@@ -766,7 +772,9 @@ def measure_sweep(args, local, stream, flush, world, rank, max_ms):
         "gradients": "CBS S0 coherent + incoherent grids and d/d(mu_a, mu_s, mfp, g) per medium",
         "launch_shape": {"picked_by": "lmc_autotune on a 2e7-photon scaled copy of the sweep",
                          **{k: tuned[k] for k in ("block_size", "blocks_per_sm", "batch_photons",
-                                                  "n_tried")}},
+                                                  "n_tried")},
+                         "tally_mode": {v: k for k, v in N.TALLY_MODES.items()}.get(
+                             tuned["tally_mode"], tuned["tally_mode"])},
         "workload": "256 single-layer Mie media, FarFieldCBS 100x1 each, seeded draws "
                     "(numpy default_rng(2026))",
         "tables": {"species": len(particles), "host_s": round(sorted(host_s)[1], 4),

@@ -198,6 +198,24 @@ typedef enum lmc_precision {
   LMC_PRECISION_FP64 = 1        /* fp64 throughout (strict per-photon replay)          */
 } lmc_precision;
 
+/* How the hit-queue tally kernel adds hits into the direct-hit sensor grids
+ * (lmc_run_opts.tally_mode).  The reference adds into per-thread sensor copies merged
+ * after the run (src/simulation.cpp:131-139, 229-236); on the GPU every mode gives the same sums
+ * up to the order of binary64 additions. */
+typedef enum lmc_tally_mode {
+  LMC_TALLY_DEFAULT = 0,        /* the library's choice: LMC_TALLY_GLOBAL                */
+  LMC_TALLY_GLOBAL = 1,         /* one global atomic add per Stokes value per hit          */
+  LMC_TALLY_WARP = 2,           /* lanes of a warp adding into the same grid cell combine
+                                   their values first (match + shuffles): one global
+                                   atomic per distinct cell and Stokes value               */
+  LMC_TALLY_SHARED = 3          /* every block of the tally kernel keeps a private copy of
+                                   the PlanarFluence / FarFieldCBS / FarFieldFluence grids
+                                   that fit in its shared memory (smallest first), adds
+                                   into it with shared atomics and adds it into the
+                                   tallies once at its end; the other grids as GLOBAL.
+                                   Single-scene handles only (a sweep: LMC_ERR_INVALID)  */
+} lmc_tally_mode;
+
 typedef struct lmc_run_opts {
   int precision;                /* lmc_precision                                       */
   int max_events;               /* SimConfig::MAX_EVENTS                               */
@@ -220,6 +238,8 @@ typedef struct lmc_run_opts {
                                    instead of replaying the photons a FarFieldCBS grid reads
                                    (replay is used by queued runs without records or
                                    estimator sensors, likelihood-ratio runs included)     */
+  int tally_mode;               /* lmc_tally_mode of the hit-queue tally kernel (queued
+                                   runs; inline runs add with global atomics)             */
 } lmc_run_opts;
 
 /* Final state of one photon, written when opts.records is set (the same layout as
@@ -346,15 +366,18 @@ typedef struct lmc_tune_result {
   uint64_t batch_photons;       /* photons per hit-queue batch                         */
   double photons_per_s;         /* the shape's rate on the sample (device time)        */
   uint64_t sample_photons;      /* photons of the sample                               */
-  int n_tried, pad;
+  int n_tried;
+  int tally_mode;               /* lmc_tally_mode picked (queued runs; else the options') */
 } lmc_tune_result;
 
 /* Times candidate launch shapes -- threads per block (256, 128), resident blocks per SM
  * (as many as fit, 2, 1: the persistent grid, hence photons per thread) and photons per
  * hit-queue batch (32 Mi, 8 Mi) -- on a sample of about sample_photons photons (a
- * sweep: every scene's count scaled down, restored afterwards) with the rest of `opts`,
- * and returns the fastest; copy its fields into lmc_run_opts for the real runs.  Runs
- * into a scratch tally buffer (allocates it); synchronous. */
+ * sweep: every scene's count scaled down, restored afterwards) with the rest of `opts`;
+ * then, at the fastest shape, the tally modes (LMC_TALLY_GLOBAL, _WARP and, for a
+ * single scene, _SHARED) of hit-queue runs.  Returns the fastest; copy its fields into
+ * lmc_run_opts for the real runs.  Runs into a scratch tally buffer (allocates it);
+ * synchronous. */
 LMC_API lmc_status lmc_autotune(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts,
                                 uint64_t sample_photons, lmc_tune_result *out);
 

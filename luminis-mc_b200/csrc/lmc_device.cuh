@@ -243,6 +243,12 @@ struct RunParams {
   // bytes of dynamic shared memory before the likelihood-ratio scores / estimated grids:
   // the whole Side, or only its ring and first species when the run replays CBS hits
   unsigned int side_off, side_pad;
+  // tally kernel, LMC_TALLY_SHARED: sensor i's grid has a block-private copy at
+  // tally_smem[i] doubles into the block's private area (-1: global atomics), of
+  // tally_smem_n[i] doubles; the area holds tally_smem_doubles
+  int tally_smem[LMC_MAX_SENSORS];
+  int tally_smem_n[LMC_MAX_SENSORS];
+  int tally_smem_doubles, tally_pad;
 };
 
 }  // namespace dev

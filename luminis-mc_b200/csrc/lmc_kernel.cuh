@@ -798,13 +798,58 @@ __device__ void reverse_field(const Scene &sc, const HitData<R> &h, Cx<R> &Om, C
 }
 
 // ------------------------------------------------------------------- tallies
+// Tally modes of the hit-queue tally kernel (lmc_tally_mode less one): every add a
+// global atomic; lanes of a warp adding into one cell combined first; block-private
+// shared-memory grids for the sensors the run privatises.
+constexpr int kTallyGlobal = 0, kTallyWarp = 1, kTallyShared = 2;
+
+// The four Stokes values of one cell: planes base, base + stride, ... at `off`.
+// kTallyWarp: the lanes of the warp that reach this call together group by cell
+// (__match_any_sync on the address); the lowest lane of each group pulls its peers'
+// values one lane at a time by shuffles and issues the group's four atomics.  When no
+// two lanes share a cell (the common case) that costs one match and one vote.
+template <int kT = kTallyGlobal>
 __device__ __forceinline__ void add4(double *base, unsigned long long stride, unsigned long long off,
                                      double a, double b, double c, double d)
 {
-  atomicAdd(base + off, a);
-  atomicAdd(base + stride + off, b);
-  atomicAdd(base + 2 * stride + off, c);
-  atomicAdd(base + 3 * stride + off, d);
+  double *const p = base + off;
+  if (kT == kTallyWarp) {
+    const unsigned act = __activemask();
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned peers = __match_any_sync(act, (unsigned long long)p);
+    const bool lead = (unsigned)(__ffs(peers) - 1) == lane;
+    if (__any_sync(act, peers != (1u << lane))) {
+      double sa = a, sb = b, sc = c, sd = d;
+      unsigned pend = lead ? (peers & ~(1u << lane)) : 0u;
+      while (__any_sync(act, pend != 0u)) {
+        const int src = pend ? __ffs(pend) - 1 : (int)lane;
+        const double ta = __shfl_sync(act, a, src), tb = __shfl_sync(act, b, src);
+        const double tc = __shfl_sync(act, c, src), td = __shfl_sync(act, d, src);
+        if (pend) {
+          sa += ta; sb += tb; sc += tc; sd += td;
+          pend &= pend - 1u;
+        }
+      }
+      a = sa; b = sb; c = sc; d = sd;
+    }
+    if (!lead)
+      return;
+  }
+  atomicAdd(p, a);
+  atomicAdd(p + stride, b);
+  atomicAdd(p + 2 * stride, c);
+  atomicAdd(p + 3 * stride, d);
+}
+
+// Where sensor si's adds go: its block-private copy in shared memory (kTallyShared,
+// when the run privatised it; the generic-address atomics then resolve to shared
+// memory), else the tally buffer.
+template <int kT>
+__device__ __forceinline__ double *tally_base(const RunParams &rp, const Sensor &s, int si, double *priv)
+{
+  if (kT == kTallyShared && rp.tally_smem[si] >= 0)
+    return priv + rp.tally_smem[si];
+  return rp.tallies + s.tally_off;
 }
 
 __device__ __forceinline__ int time_bin(const Sensor &s, double arrival)
@@ -874,9 +919,10 @@ __device__ __forceinline__ void adj_add_radial(const AdjView &A, double *s_rad, 
 // FarFieldCBSSensor::process_hit (src/detector.cpp:1231-1310) and the far-field
 // fluence sensor (same binning, reverse field zero).  exp(i k L) multiplies E_f
 // and E_r alike and cancels in every Stokes parameter, so it is not formed.
-template <typename R, bool kAdj>
+template <typename R, bool kAdj, int kT = kTallyGlobal>
 __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor &s,
-                             const HitData<R> &h, lmc_record *rec, int si, const R *hs, const AdjView *A)
+                             const HitData<R> &h, lmc_record *rec, int si, const R *hs, const AdjView *A,
+                             double *priv = nullptr)
 {
   const double t_launch = (s.dt > 0) ? hit_launch_time<R>(sc, rp, h) : 0.0;
   const int t_idx = time_bin(s, t_launch + h.opath);
@@ -898,7 +944,7 @@ __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor 
   const Cx<R> Efy = cadd(cscale(Em, h.P[1]), cscale(En, h.P[4]));
   const unsigned long long cell = ((unsigned long long)it) * s.N_phi + jp;
   const unsigned long long tstride = (unsigned long long)s.N_theta * s.N_phi;
-  double *base = rp.tallies + s.tally_off;
+  double *base = tally_base<kT>(rp, s, si, priv);
   const unsigned long long P = s.plane_stride;
   if (!in_bounds(kBoundFarfield, (unsigned long long)t_idx * tstride + cell < P))
     return false;
@@ -906,9 +952,9 @@ __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor 
     const double q0 = (double)(cnorm(Efx) + cnorm(Efy)), q1 = (double)(cnorm(Efx) - cnorm(Efy));
     const Cx<R> xy = cmul(Efx, Cx<R>{Efy.re, -Efy.im});
     const double q2 = 2.0 * (double)xy.re, q3 = 2.0 * (double)xy.im;
-    add4(base, P, cell, q0, q1, q2, q3);
+    add4<kT>(base, P, cell, q0, q1, q2, q3);
     if (t_idx >= 1)
-      add4(base, P, t_idx * tstride + cell, q0, q1, q2, q3);
+      add4<kT>(base, P, t_idx * tstride + cell, q0, q1, q2, q3);
     return true;
   }
   Cx<R> Erx = {R(0), R(0)}, Ery = {R(0), R(0)};
@@ -956,11 +1002,11 @@ __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor 
   const double i1 = (double)(cnorm(Efx) - cnorm(Efy) + cnorm(Erx) - cnorm(Ery));
   const double i2 = 2.0 * ((double)f_xy.re + (double)r_xy.re);
   const double i3 = 2.0 * ((double)f_xy.im + (double)r_xy.im);
-  add4(base, P, cell, c0, c1, c2, c3);
-  add4(base + 4 * P, P, cell, i0, i1, i2, i3);
+  add4<kT>(base, P, cell, c0, c1, c2, c3);
+  add4<kT>(base + 4 * P, P, cell, i0, i1, i2, i3);
   if (t_idx >= 1) {
-    add4(base, P, t_idx * tstride + cell, c0, c1, c2, c3);
-    add4(base + 4 * P, P, t_idx * tstride + cell, i0, i1, i2, i3);
+    add4<kT>(base, P, t_idx * tstride + cell, c0, c1, c2, c3);
+    add4<kT>(base + 4 * P, P, t_idx * tstride + cell, i0, i1, i2, i3);
   }
   if (kAdj && s.kind == LMC_SENSOR_FARFIELD_CBS) {     // S0 coherent, S0 incoherent
     const unsigned long long o = A->cbs_off[si];
@@ -976,9 +1022,9 @@ __device__ bool hit_farfield(const Scene &sc, const RunParams &rp, const Sensor 
 
 // PlanarFluenceSensor::process_hit (src/detector.cpp:780-841): lab-frame Stokes
 // with E_x negated; exp(i k L) cancels and is not formed.
-template <typename R, bool kAdj>
+template <typename R, bool kAdj, int kT = kTallyGlobal>
 __device__ bool hit_fluence(const Scene &sc, const RunParams &rp, const Sensor &s, const HitData<R> &h,
-                            int si, const R *hs, double *s_rad, const AdjView *A)
+                            int si, const R *hs, double *s_rad, const AdjView *A, double *priv = nullptr)
 {
   int t_idx = -1;
   if (s.dt > 0) {
@@ -1000,14 +1046,14 @@ __device__ bool hit_fluence(const Scene &sc, const RunParams &rp, const Sensor &
   const Cx<R> xy = cmul(Ex, Cx<R>{Ey.re, -Ey.im});
   const double q0 = (double)(cnorm(Ex) + cnorm(Ey)), q1 = (double)(cnorm(Ex) - cnorm(Ey));
   const double q2 = 2.0 * (double)xy.re, q3 = 2.0 * (double)xy.im;
-  double *base = rp.tallies + s.tally_off;
+  double *base = tally_base<kT>(rp, s, si, priv);
   const unsigned long long cell = (unsigned long long)xi * s.N_y + yi;
   const unsigned long long tstride = (unsigned long long)s.N_x * s.N_y;
   if (!in_bounds(kBoundFluence, (unsigned long long)(t_idx > 0 ? t_idx : 0) * tstride + cell < s.plane_stride))
     return false;
   if (s.dt > 0)
-    add4(base, s.plane_stride, t_idx * tstride + cell, q0, q1, q2, q3);
-  add4(base, s.plane_stride, cell, q0, q1, q2, q3);
+    add4<kT>(base, s.plane_stride, t_idx * tstride + cell, q0, q1, q2, q3);
+  add4<kT>(base, s.plane_stride, cell, q0, q1, q2, q3);
   if (kAdj && si == A->radial_sensor) {                // total S0 and its radial profile
     adj_add_radial<R>(*A, s_rad, 0, q0, hs);
     const double r = sqrt((double)h.hx * (double)h.hx + (double)h.hy * (double)h.hy);
@@ -1108,10 +1154,11 @@ __device__ __noinline__ void hit_statistics(const Sensor &s, double *tallies, do
 
 // process_hit of every sensor in `mask` (all on the plane of this hit), in
 // insertion order, as SensorsGroup::record_hit calls them (src/detector.cpp:244-265).
-template <typename R, bool kAdj>
+// kT: the tally kernel's mode (kTallyShared: priv is the block's private grid area).
+template <typename R, bool kAdj, int kT = kTallyGlobal>
 __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData<R> &h,
                              unsigned mask, unsigned long long *hits, const R *hs, double *s_rad,
-                             const AdjView *A)
+                             const AdjView *A, double *priv = nullptr)
 {
   lmc_record *rec = rp.records ? rp.records + ((((unsigned long long)h.p_hi << 32) | h.p_lo) -
                                                rp.photon_begin)
@@ -1122,7 +1169,7 @@ __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData
     const Sensor &s = sc.sensors[si];
     bool counted;
     if (s.kind == LMC_SENSOR_PLANAR_FLUENCE)
-      counted = hit_fluence<R, kAdj>(sc, rp, s, h, si, hs, s_rad, A);
+      counted = hit_fluence<R, kAdj, kT>(sc, rp, s, h, si, hs, s_rad, A, priv);
     else if (s.kind == LMC_SENSOR_PLANAR_FIELD)
       counted = hit_field<R>(sc, rp, s, h);
     else if (s.kind == LMC_SENSOR_STATISTICS) {
@@ -1134,7 +1181,7 @@ __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData
       counted = true;
     }
     else
-      counted = hit_farfield<R, kAdj>(sc, rp, s, h, rec, si, hs, A);
+      counted = hit_farfield<R, kAdj, kT>(sc, rp, s, h, rec, si, hs, A, priv);
     if (counted) {
       atomicAdd(hits + si, 1ull);
       if (rec) {
@@ -2700,9 +2747,14 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 3 : 2)
 // (1 + adj_K) * (adj_radial_bins + 1) doubles of dynamic shared memory.
 // kSweep: each entry carries its scene (an index into the g_scene array) and hit
 // counts go to rp.sweep_hits.
-template <typename R, bool kAdj = false, bool kSweep = false>
+// kT (lmc_tally_mode less one): kTallyWarp combines the adds of a warp's lanes into
+// one cell; kTallyShared (one scene) gives the block private copies of the grids
+// rp.tally_smem names, after the radial outputs in dynamic shared memory: zeroed
+// here, added to with shared atomics, and added into the tallies when the block ends.
+template <typename R, bool kAdj = false, bool kSweep = false, int kT = kTallyGlobal>
 __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
+  static_assert(!(kSweep && kT == kTallyShared), "private grids hold one scene");
   __shared__ __align__(16) unsigned char s_raw[kSweep ? 16 : sizeof(Scene)];
   __shared__ unsigned long long s_hits[LMC_MAX_SENSORS];
   extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -2716,6 +2768,10 @@ __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__
     s_hits[threadIdx.x] = 0;
   for (int j = threadIdx.x; j < rad_n; j += blockDim.x)
     s_rad[j] = 0.0;
+  double *const priv = (kT == kTallyShared) ? s_rad + rad_n : nullptr;
+  if (kT == kTallyShared)
+    for (int j = threadIdx.x; j < rp.tally_smem_doubles; j += blockDim.x)
+      priv[j] = 0.0;
   __syncthreads();
   const Scene &sc0 = *reinterpret_cast<const Scene *>(s_raw);
   const Queue &q = rp.queue;
@@ -2768,11 +2824,24 @@ __global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__
       for (int k = 0; k < A.K; ++k)
         hs[k] = r[(kQScore + k) * C + i];
     }
-    process_hits<R, kAdj>(sc, rp, h, mask,
-                          kSweep ? rp.sweep_hits + (unsigned long long)scene * LMC_MAX_SENSORS : s_hits,
-                          hs, rad_n ? s_rad : nullptr, kAdj ? &A : nullptr);
+    process_hits<R, kAdj, kT>(sc, rp, h, mask,
+                              kSweep ? rp.sweep_hits + (unsigned long long)scene * LMC_MAX_SENSORS : s_hits,
+                              hs, rad_n ? s_rad : nullptr, kAdj ? &A : nullptr, priv);
   }
   __syncthreads();
+  if (kT == kTallyShared) {              // the block's private grids into the tallies
+    for (int si = 0; si < sc0.n_sensors; ++si) {
+      const int o = rp.tally_smem[si];
+      if (o < 0)
+        continue;
+      double *dst = rp.tallies + sc0.sensors[si].tally_off;
+      for (int j = threadIdx.x; j < rp.tally_smem_n[si]; j += blockDim.x) {
+        const double v = priv[o + j];
+        if (v != 0.0)
+          atomicAdd(dst + j, v);
+      }
+    }
+  }
   if (threadIdx.x < LMC_MAX_SENSORS && s_hits[threadIdx.x])
     atomicAdd(&rp.scratch->hits[threadIdx.x], s_hits[threadIdx.x]);
   if (kAdj && rad_n) {                   // radial outputs sit at offset 0 of every row

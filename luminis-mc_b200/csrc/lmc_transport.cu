@@ -989,16 +989,107 @@ static KernelFn pick_transport(bool fp32, bool queued, bool wide, bool adj, bool
                 : pick_transport_e<false>(fp32, queued, wide, adj, sw, est);
 }
 
-static KernelFn pick_tally(bool fp32, bool adj, bool sw)
+template <int kT>
+static KernelFn pick_tally_t(bool fp32, bool adj, bool sw)
 {
   using namespace lmc::dev;
-  if (sw && adj)
-    return fp32 ? tally_kernel<float, true, true> : tally_kernel<double, true, true>;
-  if (sw)
-    return fp32 ? tally_kernel<float, false, true> : tally_kernel<double, false, true>;
-  if (adj)
-    return fp32 ? tally_kernel<float, true> : tally_kernel<double, true>;
-  return fp32 ? tally_kernel<float> : tally_kernel<double>;
+  if (sw) {
+    constexpr int kS = kT == kTallyShared ? kTallyGlobal : kT;   // (refused by tally_setup)
+    return adj ? (fp32 ? tally_kernel<float, true, true, kS> : tally_kernel<double, true, true, kS>)
+               : (fp32 ? tally_kernel<float, false, true, kS> : tally_kernel<double, false, true, kS>);
+  }
+  return adj ? (fp32 ? tally_kernel<float, true, false, kT> : tally_kernel<double, true, false, kT>)
+             : (fp32 ? tally_kernel<float, false, false, kT> : tally_kernel<double, false, false, kT>);
+}
+
+// kt: the device tally mode (dev::kTallyGlobal, kTallyWarp, kTallyShared).
+static KernelFn pick_tally(bool fp32, bool adj, bool sw, int kt = lmc::dev::kTallyGlobal)
+{
+  using namespace lmc::dev;
+  if (kt == kTallyWarp)
+    return pick_tally_t<kTallyWarp>(fp32, adj, sw);
+  if (kt == kTallyShared)
+    return pick_tally_t<kTallyShared>(fp32, adj, sw);
+  return pick_tally_t<kTallyGlobal>(fp32, adj, sw);
+}
+
+// The hit-queue tally kernel of a run under lmc_run_opts.tally_mode `mode`: the kernel,
+// its dynamic shared memory (dyn_tally: what it needs before the private grids) and
+// its grid.  LMC_TALLY_SHARED gives private copies to the direct-hit PlanarFluence,
+// FarFieldCBS and FarFieldFluence grids, smallest first, while they fit in the shared
+// memory a block may have beside the kernel's static arrays; their offsets go to rp.
+// Without any grid that fits the mode adds like LMC_TALLY_GLOBAL (and says so in kt).
+struct TallyLaunch {
+  KernelFn fn;
+  size_t dyn;
+  int grid_per_sm;                       // blocks per SM of the tally grid
+  int kt;                                // device mode used
+};
+
+static lmc_status tally_setup(int mode, bool sw, bool fp32, bool adj, const lmc::dev::Scene &sc,
+                              const size_t *sensor_count, int device, size_t dyn_tally,
+                              lmc::dev::RunParams &rp, TallyLaunch &out)
+{
+  using namespace lmc;
+  if (mode < LMC_TALLY_DEFAULT || mode > LMC_TALLY_SHARED)
+    return fail(LMC_ERR_INVALID, "tally_mode must be an lmc_tally_mode");
+  if (mode == LMC_TALLY_SHARED && sw)
+    return fail(LMC_ERR_INVALID, "tally_mode LMC_TALLY_SHARED needs a single-scene handle");
+  for (int i = 0; i < LMC_MAX_SENSORS; ++i) {
+    rp.tally_smem[i] = -1;
+    rp.tally_smem_n[i] = 0;
+  }
+  rp.tally_smem_doubles = 0;
+  int kt = mode == LMC_TALLY_WARP ? dev::kTallyWarp
+         : mode == LMC_TALLY_SHARED ? dev::kTallyShared : dev::kTallyGlobal;
+  out.dyn = dyn_tally;
+  out.grid_per_sm = 8;
+  if (kt == dev::kTallyShared) {
+    const KernelFn fn = pick_tally(fp32, adj, sw, kt);
+    int optin = 0;
+    LMC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    cudaFuncAttributes fa;
+    LMC_CUDA(cudaFuncGetAttributes(&fa, (const void *)fn));
+    const size_t room = (size_t)optin > fa.sharedSizeBytes + dyn_tally
+                            ? ((size_t)optin - fa.sharedSizeBytes - dyn_tally) / sizeof(double) : 0;
+    int order[LMC_MAX_SENSORS], n = 0;
+    for (int i = 0; i < sc.n_sensors; ++i) {
+      const dev::Sensor &s = sc.sensors[i];
+      const bool direct = s.kind == LMC_SENSOR_PLANAR_FLUENCE || s.kind == LMC_SENSOR_FARFIELD_FLUENCE ||
+                          (s.kind == LMC_SENSOR_FARFIELD_CBS && !s.estimator);
+      if (direct && sensor_count[i] > 0)
+        order[n++] = i;
+    }
+    std::stable_sort(order, order + n, [&](int a, int b) { return sensor_count[a] < sensor_count[b]; });
+    size_t used = 0;
+    for (int k = 0; k < n; ++k) {
+      const size_t c = sensor_count[order[k]];
+      if (used + c > room)
+        break;
+      rp.tally_smem[order[k]] = (int)used;
+      rp.tally_smem_n[order[k]] = (int)c;
+      used += c;
+    }
+    rp.tally_smem_doubles = (int)used;
+    if (used == 0) {
+      kt = dev::kTallyGlobal;
+    } else {
+      out.dyn = dyn_tally + used * sizeof(double);
+      LMC_CUDA(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)out.dyn));
+      int per = 0;
+      LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)fn, dev::kBlock, out.dyn));
+      if (per < 1)
+        return fail(LMC_ERR_CUDA, "tally kernel with private grids does not fit on an SM");
+      out.grid_per_sm = per;            // one pass of resident blocks: each adds its grids once
+    }
+  }
+  out.kt = kt;
+  out.fn = pick_tally(fp32, adj, sw, kt);
+  if (out.dyn > 0 && kt != dev::kTallyShared)
+    LMC_CUDA(cudaFuncSetAttribute((const void *)out.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)out.dyn));
+  return LMC_OK;
 }
 
 static KernelFn pick_replay(bool fp32, bool sw, bool extras)
@@ -1161,7 +1252,14 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   if (adj && extras)                     // (MixtureLayers are refused by the layout already)
     return fail(LMC_ERR_UNSUPPORTED, "likelihood-ratio runs do not record an Absorption grid");
   const KernelFn tk = pick_transport(fp32, h->queued, wide, adj != nullptr, sw, est, extras);
-  const KernelFn tl = pick_tally(fp32, adj != nullptr, sw);
+  TallyLaunch tl{};
+  if (h->queued && h->tally_doubles > 0) {
+    const lmc_status st = tally_setup(opts->tally_mode, sw, fp32, adj != nullptr,
+                                      sw ? h->scenes[0] : h->scene, h->sensor_count, h->device,
+                                      (adj && !sw) ? dyn_tally : 0, rp, tl);
+    if (st != LMC_OK)
+      return st;
+  }
   // CBS replay: queued runs without an estimator or records keep no reverse-path
   // history in the transport; the replay kernel rebuilds it for the hits that
   // FarFieldCBS grids read (likelihood-ratio scores are carried apart from it)
@@ -1237,9 +1335,6 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
   }
   LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)dyn_transport));
-  if (adj && !sw)
-    LMC_CUDA(cudaFuncSetAttribute((const void *)tl, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)dyn_tally));
   int per_sm = 0;
   LMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)tk, block, dyn_transport));
   if (opts->blocks_per_sm > 0)
@@ -1310,9 +1405,9 @@ static lmc_status run_impl(lmc_handle *h, uint64_t seed, uint64_t photon_begin, 
       LMC_CUDA(cudaEventRecord(h->kev[pair + 1], stream));
     if (h->queued && h->tally_doubles > 0) {
       const int tgrid = (int)std::max<unsigned long long>(
-          1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * 8,
+          1ull, std::min<unsigned long long>((unsigned long long)h->sm_count * tl.grid_per_sm,
                                              (rp.queue.cap + dev::kBlock - 1) / dev::kBlock));
-      tl<<<tgrid, dev::kBlock, (adj && !sw) ? dyn_tally : 0, stream>>>(h->d_scene, rp);
+      tl.fn<<<tgrid, dev::kBlock, tl.dyn, stream>>>(h->d_scene, rp);
       LMC_CUDA(cudaGetLastError());
     }
   }
@@ -1558,6 +1653,38 @@ lmc_status lmc_autotune(lmc_handle *h, uint64_t seed, const lmc_run_opts *opts, 
           best.photons_per_s = rate;
         }
       }
+  // the tally kernel's mode at that shape (hit-queue runs; a sweep's scenes share no
+  // private grid, so it has two modes)
+  best.tally_mode = opts->tally_mode;
+  if (result == LMC_OK && h->queued && h->tally_doubles > 0) {
+    const int modes[] = {LMC_TALLY_GLOBAL, LMC_TALLY_WARP, LMC_TALLY_SHARED};
+    double best_rate = 0.0;
+    for (int m : modes) {
+      if (m == LMC_TALLY_SHARED && h->sweep)
+        continue;
+      lmc_run_opts o = *opts;
+      o.block_size = best.block_size;
+      o.blocks_per_sm = best.blocks_per_sm;
+      o.batch_photons = best.batch_photons;
+      o.tally_mode = m;
+      o.records = nullptr;
+      lmc_stats st;
+      double ms = 0.0;
+      for (int rep = 0; rep < 2 && result == LMC_OK; ++rep) {
+        result = run_impl(h, seed, 0, n_sample, &o, nullptr, nullptr, d_t, &st);
+        ms = st.kernel_ms;
+      }
+      if (result != LMC_OK)
+        break;
+      ++tried;
+      const double rate = ms > 0 ? (double)n_sample / (ms * 1e-3) : 0.0;
+      if (rate > best_rate) {
+        best_rate = rate;
+        best.tally_mode = m;
+        best.photons_per_s = rate;
+      }
+    }
+  }
   cudaFree(d_t);
   if (h->sweep) {
     const lmc_status st = lmc_sweep_set_photons(h, counts.data());
@@ -2017,7 +2144,13 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
   // the kernels lmc_run picks for the same scene and options
   const bool wide = fp32 && queued && (opts->blocks_per_sm == 0 || opts->blocks_per_sm >= 3);
   const KernelFn tk = pick_transport(fp32, queued, wide, false, false, false, scene_extras(sc));
-  const KernelFn tl = pick_tally(fp32, false, false);
+  TallyLaunch tl{};
+  if (queued && s->n_sensors > 0) {
+    const lmc_status st = tally_setup(opts->tally_mode, false, fp32, false, sc, sensor_count, device,
+                                      0, rp, tl);
+    if (st != LMC_OK)
+      return st;
+  }
   const size_t dyn_transport = fp32 ? dev::side_bytes<float>() : dev::side_bytes<double>();
   rp.side_off = (unsigned)dyn_transport;
   LMC_CUDA(cudaFuncSetAttribute((const void *)tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2061,9 +2194,9 @@ extern "C" lmc_status lmc_run_noalloc(const lmc_scene *s, uint64_t seed, uint64_
     LMC_CUDA(cudaGetLastError());
     if (queued && s->n_sensors > 0) {
       const int tgrid = (int)std::max<unsigned long long>(
-          1ull, std::min<unsigned long long>((unsigned long long)sm_count * 8,
+          1ull, std::min<unsigned long long>((unsigned long long)sm_count * tl.grid_per_sm,
                                              (rp.queue.cap + dev::kBlock - 1) / dev::kBlock));
-      tl<<<tgrid, dev::kBlock, 0, stream>>>(d_scene, rp);
+      tl.fn<<<tgrid, dev::kBlock, tl.dyn, stream>>>(d_scene, rp);
       LMC_CUDA(cudaGetLastError());
     }
   }

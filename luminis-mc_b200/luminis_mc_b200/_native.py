@@ -25,6 +25,19 @@ STAT_EVENTS, STAT_THETA, STAT_PHI, STAT_DEPTH, STAT_TIME, STAT_WEIGHT = 1, 2, 4,
 PDF_RAYLEIGH, PDF_RD, PDF_RDEMC, PDF_DRAINE, PDF_MIE = 1, 3, 4, 5, 6
 AMP_RGD, AMP_MIE = 0, 1
 PRECISION = {"fp32": 0, "fp64": 1}
+# lmc_tally_mode: how the hit-queue tally kernel adds into the sensor grids
+TALLY_MODES = {"default": 0, "global": 1, "warp": 2, "shared": 3}
+
+
+def tally_mode_value(mode) -> int:
+    """lmc_tally_mode of a name in TALLY_MODES or of its integer value."""
+    if isinstance(mode, str):
+        if mode not in TALLY_MODES:
+            raise ValueError(f"tally_mode must be one of {sorted(TALLY_MODES)}")
+        return TALLY_MODES[mode]
+    if int(mode) not in TALLY_MODES.values():
+        raise ValueError(f"tally_mode must be one of {sorted(TALLY_MODES)}")
+    return int(mode)
 
 dptr = C.POINTER(C.c_double)
 
@@ -94,10 +107,10 @@ class SceneDesc(C.Structure):
 class TuneResult(C.Structure):
     _fields_ = [("block_size", C.c_int), ("blocks_per_sm", C.c_int),
                 ("batch_photons", C.c_uint64), ("photons_per_s", C.c_double),
-                ("sample_photons", C.c_uint64), ("n_tried", C.c_int), ("pad", C.c_int)]
+                ("sample_photons", C.c_uint64), ("n_tried", C.c_int), ("tally_mode", C.c_int)]
 
     def as_dict(self) -> dict:
-        return {n: getattr(self, n) for n, _ in self._fields_ if n != "pad"}
+        return {n: getattr(self, n) for n, _ in self._fields_}
 
 
 class RunOpts(C.Structure):
@@ -105,7 +118,8 @@ class RunOpts(C.Structure):
                 ("block_size", C.c_int), ("blocks_per_sm", C.c_int), ("records", C.c_void_p),
                 ("stream", C.c_void_p), ("batch_photons", C.c_uint64),
                 ("stream_format", C.c_int), ("host_tallies_zero", C.c_int),
-                ("cbs_phase", C.c_int), ("stage_tables", C.c_int), ("no_replay", C.c_int)]
+                ("cbs_phase", C.c_int), ("stage_tables", C.c_int), ("no_replay", C.c_int),
+                ("tally_mode", C.c_int)]
 
 
 class Stats(C.Structure):

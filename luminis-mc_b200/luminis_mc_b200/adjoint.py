@@ -101,8 +101,9 @@ class AdjointTransport:
         return out
 
     def run(self, n_photons: int, seed: int, precision: str = "fp32", begin: int = 0,
-            stream=None):
-        """(outputs [n_out], jacobian [n_params, n_out], stats), per photon, on the device."""
+            stream=None, tally_mode="default"):
+        """(outputs [n_out], jacobian [n_params, n_out], stats), per photon, on the device.
+        The run's sensor tallies stay in self.last_tallies (device, flat)."""
         torch = self.torch
         with torch.cuda.device(self.device):
             adj = torch.zeros((1 + self.n_params) * self.n_out, dtype=torch.float64,
@@ -113,12 +114,14 @@ class AdjointTransport:
             o.max_events = int(self.config.MAX_EVENTS)
             o.track_reverse_paths = int(bool(self.config.track_reverse_paths))
             o.stream = N.launch_stream(stream)
+            o.tally_mode = N.tally_mode_value(tally_mode)
             st = N.Stats()
             torch.cuda.synchronize(self.device)
             N.check(N.lib().lmc_run_adjoint(self._handle, int(seed) & (2 ** 64 - 1), int(begin),
                                             int(n_photons), C.byref(o), C.byref(self.opts),
                                             C.c_void_p(tallies.data_ptr()),
                                             C.c_void_p(adj.data_ptr()), C.byref(st)))
+        self.last_tallies = tallies
         adj = adj.view(1 + self.n_params, self.n_out) / float(max(n_photons, 1))
         return adj[0], adj[1:], st.as_dict()
 

@@ -263,7 +263,7 @@ class Transport:
     def opts(self, precision="fp32", max_events=None, track_reverse_paths=None, block_size=0,
              blocks_per_sm=0, records_ptr=None, stream=None, batch_photons=0,
              stream_format=0, host_tallies_zero=False, cbs_phase="fp64",
-             stage_tables=False, no_replay=False) -> N.RunOpts:
+             stage_tables=False, no_replay=False, tally_mode="default") -> N.RunOpts:
         if precision not in N.PRECISION:
             raise ValueError("precision must be 'fp32' or 'fp64'")
         c = self.config
@@ -284,6 +284,7 @@ class Transport:
         o.cbs_phase = 1 if cbs_phase == "fp32" else 0
         o.stage_tables = int(bool(stage_tables))
         o.no_replay = int(bool(no_replay))
+        o.tally_mode = N.tally_mode_value(tally_mode)
         return o
 
     def run_host(self, tallies: np.ndarray, n_photons: int, seed: int, begin: int = 0,
@@ -309,8 +310,8 @@ class Transport:
 
     def autotune(self, seed: int, precision: str = "fp32", sample_photons: int = 4_000_000,
                  **kw) -> dict:
-        """Launch shape (block_size, blocks_per_sm, batch_photons) that ran a sample of
-        this scene fastest (lmc_autotune); pass it to run_device / run_host."""
+        """Launch shape (block_size, blocks_per_sm, batch_photons) and tally_mode that ran
+        a sample of this scene fastest (lmc_autotune); pass them to run_device / run_host."""
         r = N.TuneResult()
         N.check(N.lib().lmc_autotune(self._h, int(seed) & (2 ** 64 - 1),
                                      C.byref(self.opts(precision=precision, **kw)),

@@ -79,9 +79,10 @@ class SweepRun:
         return o
 
     def autotune(self, seed: int, precision: str = "fp32", sample_photons: int = 10_000_000) -> dict:
-        """Pick the launch shape (threads per block, blocks per SM, photons per batch) by
-        timing candidates on a scaled-down copy of the sweep (lmc_autotune); later runs
-        use it.  Returns the chosen shape and its rate on the sample."""
+        """Pick the launch shape (threads per block, blocks per SM, photons per batch) and
+        the tally kernel's mode by timing candidates on a scaled-down copy of the sweep
+        (lmc_autotune); later runs use them.  Returns the choice and its rate on the
+        sample."""
         if self.photons is None:
             raise ValueError("set_photons() first")
         self.launch = {}
@@ -90,7 +91,7 @@ class SweepRun:
                                      C.byref(self.opts(precision)), int(sample_photons),
                                      C.byref(r)))
         self.launch = {"block_size": r.block_size, "blocks_per_sm": r.blocks_per_sm,
-                       "batch_photons": r.batch_photons}
+                       "batch_photons": r.batch_photons, "tally_mode": r.tally_mode}
         return r.as_dict()
 
     def run(self, seed: int, precision: str = "fp32", stream=None, want_stats: bool = True):
