@@ -2751,8 +2751,12 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 3 : 2)
 // one cell; kTallyShared (one scene) gives the block private copies of the grids
 // rp.tally_smem names, after the radial outputs in dynamic shared memory: zeroed
 // here, added to with shared atomics, and added into the tallies when the block ends.
+// Binary32 kernels (but a sweep's with likelihood-ratio scores) are held to 128
+// registers, so that two blocks (16 warps) fit per SM: the kernel waits mostly on its
+// queue reads, and at 154 registers one block per SM left 8 warps to hide them.
 template <typename R, bool kAdj = false, bool kSweep = false, int kT = kTallyGlobal>
-__global__ void __launch_bounds__(kBlock) tally_kernel(const Scene *__restrict__ g_scene, RunParams rp)
+__global__ void __launch_bounds__(kBlock, (sizeof(R) == 4 && !(kAdj && kSweep)) ? 2 : 1)
+    tally_kernel(const Scene *__restrict__ g_scene, RunParams rp)
 {
   static_assert(!(kSweep && kT == kTallyShared), "private grids hold one scene");
   __shared__ __align__(16) unsigned char s_raw[kSweep ? 16 : sizeof(Scene)];
