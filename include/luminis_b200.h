@@ -320,7 +320,8 @@ LMC_API size_t lmc_last_error(char *buf, size_t len);
  * LMC_ERR_INVALID with the size it needs); photons are processed in batches that
  * fit the remaining ~56 MiB hit queue, or of opts->batch_photons when that is
  * smaller.  opts->block_size and opts->blocks_per_sm pick the launch shape and the
- * kernel variant as they do for lmc_run.  The first call on each device looks up the
+ * kernel variant, and opts->tally_mode the tally kernel's mode, as they do for lmc_run
+ * (LMC_TALLY_SHARED's private grids are the kernel's shared memory, not an allocation).  The first call on each device looks up the
  * array's device address (cudaGetSymbolAddress), so make that first call before
  * any stream capture.  All calls on one device share the array: calls that
  * overlap in time -- from two threads, or on two streams -- race and corrupt each
