@@ -43,10 +43,13 @@ def test_struct_layouts_match_ctypes():
 #include <stddef.h>
 #include "luminis_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(lmc_scene), sizeof(lmc_medium_desc),
-         sizeof(lmc_sensor_desc), sizeof(lmc_laser_desc), sizeof(lmc_run_opts), sizeof(lmc_stats),
-         sizeof(lmc_record), offsetof(lmc_scene, sensors), offsetof(lmc_run_opts, batch_photons),
-         sizeof(lmc_mie_species));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(lmc_scene),
+         sizeof(lmc_medium_desc), sizeof(lmc_sensor_desc), sizeof(lmc_laser_desc),
+         sizeof(lmc_run_opts), sizeof(lmc_stats), sizeof(lmc_record), offsetof(lmc_scene, sensors),
+         offsetof(lmc_run_opts, batch_photons), sizeof(lmc_mie_species),
+         offsetof(lmc_run_opts, tally_mode), sizeof(lmc_tune_result),
+         offsetof(lmc_tune_result, tally_mode));
+  printf("%d %d %d %d\n", LMC_TALLY_DEFAULT, LMC_TALLY_GLOBAL, LMC_TALLY_WARP, LMC_TALLY_SHARED);
   return 0;
 }
 """
@@ -55,12 +58,26 @@ int main(void) {
         open(c, "w").write(src)
         exe = os.path.join(d, "t")
         subprocess.run(["gcc", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
-        got = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
+        lines = subprocess.run([exe], capture_output=True, text=True).stdout.splitlines()
+    got = list(map(int, lines[0].split()))
     want = [C.sizeof(N.SceneDesc), C.sizeof(N.MediumDesc), C.sizeof(N.SensorDesc),
             C.sizeof(N.LaserDesc), C.sizeof(N.RunOpts), C.sizeof(N.Stats),
             np.dtype(N.RECORD_FIELDS).itemsize, N.SceneDesc.sensors.offset,
-            N.RunOpts.batch_photons.offset, C.sizeof(N.MieSpecies)]
+            N.RunOpts.batch_photons.offset, C.sizeof(N.MieSpecies),
+            N.RunOpts.tally_mode.offset, C.sizeof(N.TuneResult), N.TuneResult.tally_mode.offset]
     assert got == want
+    # lmc_tally_mode values, as the Python layer names them
+    assert list(map(int, lines[1].split())) == [N.TALLY_MODES[k] for k in
+                                                 ("default", "global", "warp", "shared")]
+
+
+def test_tally_mode_names():
+    """Run options take a tally mode by name or value; anything else is a ValueError
+    before any call into the library."""
+    assert N.tally_mode_value("shared") == 3 and N.tally_mode_value(2) == 2
+    for bad in ("atomic", 4, -1):
+        with pytest.raises(ValueError, match="tally_mode"):
+            N.tally_mode_value(bad)
 
 
 PHASES = [
