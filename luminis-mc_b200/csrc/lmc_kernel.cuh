@@ -1182,15 +1182,21 @@ __device__ void process_hits(const Scene &sc, const RunParams &rp, const HitData
     }
     else
       counted = hit_farfield<R, kAdj, kT>(sc, rp, s, h, rec, si, hs, A, priv);
-    if (counted) {
-      atomicAdd(hits + si, 1ull);
-      if (rec) {
-        rec->hit[0] = h.hx;
-        rec->hit[1] = h.hy;
-        rec->hit[2] = h.hz;
-        atomicAdd(&rec->n_hits, 1);
-      }
+    if (counted && rec) {
+      rec->hit[0] = h.hx;
+      rec->hit[1] = h.hy;
+      rec->hit[2] = h.hz;
+      atomicAdd(&rec->n_hits, 1);
     }
+    // Sensor::hits: the lanes here that count into the same counter (a block's shared
+    // counters, or a sweep scene's) add their number in one atomic, from their lowest
+    // lane; one atomic per lane serialised the warp on a few shared addresses
+    const unsigned act = __activemask();
+    unsigned long long *const cp = hits + si;
+    const unsigned grp = __match_any_sync(act, (unsigned long long)cp);
+    const unsigned cnt = __ballot_sync(act, counted) & grp;
+    if ((threadIdx.x & 31u) == (unsigned)(__ffs(grp) - 1) && cnt)
+      atomicAdd(cp, (unsigned long long)__popc(cnt));
   }
 }
 
