@@ -191,13 +191,30 @@ class Rng:
 
 
 # ------------------------------------------------------------------------------ enums
-class LaserSource(enum.IntEnum):
+class _BoundEnum(enum.Enum):
+    """An enumeration with the semantics of the reference's bound C++ enums (pybind11,
+    python/python_module.cpp): members carry .name and .value, int() and operator.index
+    give the value and the hash is the value's, but a member is not an int, does not
+    compare equal to one and has no order.  Code that treats scalars and enums apart
+    (the reference's HDF5 writer stores an enum by its name) sees the same types."""
+
+    def __int__(self):
+        return self.value
+
+    def __index__(self):
+        return self.value
+
+    def __hash__(self):
+        return hash(self.value)
+
+
+class LaserSource(_BoundEnum):
     Point = 0
     Uniform = 1
     Gaussian = 2
 
 
-class TemporalProfile(enum.IntEnum):
+class TemporalProfile(_BoundEnum):
     Delta = 0
     Gaussian = 1
     TopHat = 2
@@ -206,13 +223,13 @@ class TemporalProfile(enum.IntEnum):
     CW = 5
 
 
-class CrossingDirection(enum.IntEnum):
+class CrossingDirection(_BoundEnum):
     Forward = 0
     Backward = 1
     Both = 2
 
 
-class LogLevel(enum.IntEnum):
+class LogLevel(_BoundEnum):
     debug = 0
     info = 1
     warn = 2
