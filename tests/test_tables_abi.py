@@ -90,6 +90,14 @@ PHASES = [
     {"kind": "rd", "wavelength": 0.633e-3, "radius": 0.2e-3, "nDiv": 500, "min": 0.0, "max": math.pi},
     {"kind": "rayleigh", "nDiv": 400, "min": -1.0, "max": 1.0},
     {"kind": "draine", "g": 0.7, "a": 0.5, "nDiv": 400, "min": -1.0, "max": 1.0},
+    # odd nDiv: SamplingTable::initialize (src/table.cpp:23-41) writes and reads pdf[nDiv]
+    # one past its nDiv-element vector; for odd nDiv that overwrites glibc's next chunk
+    # header and the reference aborts in free() before it returns.  The tables here are
+    # sized nDiv + 1 and follow the reference's arithmetic (the oracle's restatement); the
+    # reference itself returns them for even nDiv only.
+    {"kind": "mie", "wavelength": 0.633e-3, "radius": 0.5e-3, "n_particle": 1.59, "n_medium": 1.33,
+     "nDiv": 999, "min": 0.0, "max": math.pi},
+    {"kind": "rayleigh", "nDiv": 401, "min": -1.0, "max": 1.0},
 ]
 
 
