@@ -146,6 +146,34 @@ def test_sweep_modes(cuda):
     sw.close()
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_sweep_adjoint_warp_matches_global(precision, cuda):
+    """A sweep with each scene's gradients (the path the bench's sweep arm takes when the
+    autotuner picks warp-combined adds): outputs, Jacobians and tallies as with global
+    atomics."""
+    from tests.test_gpu_sweep import _specs
+    specs = _specs()[:3]
+    sw = SweepRun([W.build(lm, s)[0] for s in specs])
+    sw.set_photons([15000, 6000, 9000])
+    got = {}
+    for mode in ("global", "warp"):
+        sw.zero()
+        sw.launch = {"tally_mode": N.TALLY_MODES[mode]}
+        blocks, st = sw.run_adjoint(21, precision=precision)
+        got[mode] = ([(o.cpu().numpy(), j.cpu().numpy()) for o, j in blocks],
+                     [sw.host_tallies(k) for k in range(3)], st)
+    sw.close()
+    tol = RTOL_FP32 if precision == "fp32" else RTOL
+    (b0, t0, s0), (b1, t1, s1) = got["global"], got["warp"]
+    assert s1["events"] == s0["events"] and s1["photons"] == s0["photons"]
+    for (o0, j0), (o1, j1) in zip(b0, b1):
+        np.testing.assert_allclose(o1, o0, rtol=0, atol=tol * max(np.abs(o0).max(), 1e-300))
+        np.testing.assert_allclose(j1, j0, rtol=0, atol=tol * max(np.abs(j0).max(), 1e-300))
+    for a, b in zip(t1, t0):
+        for x, y in zip(a, b):
+            np.testing.assert_allclose(x, y, rtol=0, atol=tol * max(np.abs(y).max(), 1e-300))
+
+
 def test_autotune_reports_a_mode(cuda):
     from luminis_mc_b200.simulation import Transport
     t = Transport(W.build(lm, W.bilayer_rgd_mie(0, 1))[0])
