@@ -8,7 +8,7 @@ scene field first, returns LMC_ERR_INVALID with a message (ValueError in Python)
 only then touches the GPU.  So each fault below is injected into an otherwise valid C
 scene and must be refused on a machine without a GPU.  The unmodified scene must pass
 validation and fail only at the first CUDA call.  lmc_create_sweep names the faulty
-scene.
+scene, and lmc_run_noalloc refuses corrupt scenes and options the same way.
 """
 import ctypes as C
 import math
@@ -97,6 +97,26 @@ def test_sweep_names_the_faulty_scene():
     h = C.c_void_p()
     with pytest.raises(ValueError, match="scene 2: medium coefficients"):
         N.check(N.lib().lmc_create_sweep(arr, 3, C.byref(h)))
+
+
+@pytest.mark.parametrize("what,message", [("scene", "medium coefficients"),
+                                           ("precision", "unknown precision"),
+                                           ("max_events", "max_events"),
+                                           ("reverse_paths", "track_reverse_paths")])
+def test_noalloc_refuses_before_the_gpu(what, message):
+    sc, keep = _scene()
+    o = N.RunOpts()
+    o.precision, o.max_events, o.track_reverse_paths = N.PRECISION["fp32"], 1000, 1
+    if what == "scene":
+        sc.media[0].mu_s = NAN
+    elif what == "precision":
+        o.precision = 7
+    elif what == "max_events":
+        o.max_events = -1
+    else:
+        o.track_reverse_paths = 0           # the scene has a FarFieldCBS grid
+    with pytest.raises(ValueError, match=message):
+        N.check(N.lib().lmc_run_noalloc(C.byref(sc), 1, 0, 1000, C.byref(o), None, None))
 
 
 @pytest.mark.skipif(gpu_available(), reason="on a GPU machine the valid scene is created")
