@@ -2758,8 +2758,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 3 : 2)
 // rp.tally_smem names, after the radial outputs in dynamic shared memory: zeroed
 // here, added to with shared atomics, and added into the tallies when the block ends.
 // Binary32 kernels (but a sweep's with likelihood-ratio scores) are held to 128
-// registers, so that two blocks (16 warps) fit per SM: the kernel waits mostly on its
-// queue reads, and at 154 registers one block per SM left 8 warps to hide them.
+// registers, so that two blocks (16 warps) fit per SM: the kernel is latency-bound
+// (shared-memory, SFU and queue-read waits), and 154 registers left 8 warps per SM.
 template <typename R, bool kAdj = false, bool kSweep = false, int kT = kTallyGlobal>
 __global__ void __launch_bounds__(kBlock, (sizeof(R) == 4 && !(kAdj && kSweep)) ? 2 : 1)
     tally_kernel(const Scene *__restrict__ g_scene, RunParams rp)
